@@ -1,0 +1,222 @@
+/*
+ * pyomgpu.h -- C ABI of the B200 external-mode (barotropic) solver for pyOM2.
+ *
+ * Drop-in for the routines pyOM2's f2py module binds for this path
+ * (py_src/Makefile:15-47 builds them into ``pyOM_code``):
+ *
+ *   reference routine (file:line)                      replaced by
+ *   ---------------------------------------------------------------------------
+ *   make_coeff_streamfunction  solve_streamfct.f90:123  pyomgpu_ctx_create (operator kept, like the SAVE'd cf)
+ *   make_coeff_surf_press      solve_pressure.f90:87    pyomgpu_ctx_create (second operator)
+ *   make_inv_sfc               solve_streamfct.f90:381  pyomgpu_set_islands / pyomgpu_streamfunction_init
+ *   congrad_streamfunction     solve_streamfct.f90:153  pyomgpu_congrad_streamfunction
+ *   congrad_surf_press         solve_pressure.f90:137   pyomgpu_congrad_surf_press
+ *   apply_op                   solve_pressure.f90:254   pyomgpu_apply_op
+ *   dot_sfc/absmax_sfc         solve_streamfct.f90:331-362 (fused into the CG kernels)
+ *   dot_sfp/absmax_sfp         solve_pressure.f90:277-311  (fused into the CG kernels)
+ *   streamfunction_init        streamfct_init.f90:7     pyomgpu_streamfunction_init (+ _get_islands)
+ *   isleperim                  island_module.f90:7      pyomgpu_isleperim
+ *   line_integral              streamfct_init.f90:311   pyomgpu_line_integral
+ *   solve_streamfunction       solve_streamfct.f90:10   pyomgpu_solve_streamfunction
+ *   solve_pressure             solve_pressure.f90:10    pyomgpu_solve_pressure
+ *
+ * Array conventions: every 2-D field has the Fortran extents of
+ * main_module.f90 for one PE, (1-onx:nx+onx, 1-onx:ny+onx) with onx = 2, in
+ * Fortran (column-major) order, leading dimension nx+4 -- exactly the buffers
+ * f2py exposes.  3-D fields append nz, 4-D fields append (nz, 3) time levels.
+ * Island arrays boundary/line_dir are (nisle, max_boundary, 2) int32 in
+ * Fortran order with Fortran index values.
+ *
+ * Pointers marked "host or device" may point to either; the library detects
+ * host memory with cudaPointerGetAttributes and stages it through device
+ * buffers owned by the context.  Grid inputs to pyomgpu_ctx_create are host
+ * pointers.  The full-step entry points take device pointers.
+ *
+ * Errors never abort the process (the reference calls halt_stop,
+ * parallel_none.f90:51-59): every entry point returns a status code and
+ * pyomgpu_last_error() gives a message.  A context is used by one host thread
+ * at a time; all work is ordered on the stream passed in.
+ */
+#ifndef PYOMGPU_H
+#define PYOMGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pyomgpu_ctx pyomgpu_ctx;
+typedef void* pyomgpu_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+/* ---- status codes --------------------------------------------------------- */
+#define PYOMGPU_OK 0
+#define PYOMGPU_MAXITER 1   /* max iterations exceeded (solve_streamfct.f90:303) */
+#define PYOMGPU_DIVERGED 2  /* divergence test fired (solve_streamfct.f90:236) */
+#define PYOMGPU_NAN 3       /* estimated error is NaN (solve_streamfct.f90:322) */
+#define PYOMGPU_TIMEOUT 4   /* a device-side grid barrier wait ran out */
+#define PYOMGPU_SINGULAR 5  /* island system singular (DGESV info != 0, solve_streamfct.f90:82) */
+#define PYOMGPU_EINVAL -1
+#define PYOMGPU_ECUDA -2
+#define PYOMGPU_ENOMEM -3
+#define PYOMGPU_EISLAND -4 /* island labelling / perimeter tracing failed */
+#define PYOMGPU_ESTATE -5  /* call needs state the context does not have yet */
+
+/* operators held by a context */
+#define PYOMGPU_OP_STREAMFUNCTION 0 /* solve_streamfct.f90:123-148 */
+#define PYOMGPU_OP_SURF_PRESS 1     /* solve_pressure.f90:87-131 */
+
+/* arithmetic of pyomgpu_solve_rtol */
+#define PYOMGPU_PREC_F64 64 /* FP64 Jacobi-PCG */
+#define PYOMGPU_PREC_F32 32 /* FP32 PCG with FP64 dot products inside FP64 iterative refinement */
+
+/* Geometry and operator inputs: the main_module arrays the solve reads
+ * (main_module.f90:115-121,185-192).  All host pointers. */
+typedef struct pyomgpu_grid {
+  int32_t nx, ny;      /* interior points (serial: is_pe=1, ie_pe=nx) */
+  int32_t onx;         /* halo width; must be 2 */
+  int32_t enable_cyclic_x, enable_cyclic_y;
+  int32_t enable_free_surface; /* adds -maskT/(grav dt^2) to the surf_press diagonal */
+  double grav, dt_mom;         /* only for the free-surface diagonal */
+  const double *dxt, *dxu;     /* [nx+4] */
+  const double *dyt, *dyu;     /* [ny+4] */
+  const double *cost, *cosu;   /* [ny+4] */
+  const double *hur, *hvr;     /* streamfunction operator */
+  const double *hu, *hv;       /* surface-pressure operator (may be NULL if unused) */
+  const double *maskT_top;     /* maskT(:,:,nz) (surface pressure; may be NULL) */
+  const double *maskU_top, *maskV_top; /* maskU/maskV(:,:,nz) for island integrals (may be NULL) */
+} pyomgpu_grid;
+
+/* Island description as produced by streamfunction_init (streamfct_init.f90:87-93). */
+typedef struct pyomgpu_islands {
+  int32_t nisle;
+  int32_t max_boundary;
+  const int32_t* boundary;    /* (nisle, max_boundary, 2) host */
+  const int32_t* line_dir;    /* (nisle, max_boundary, 2) host */
+  const int32_t* nr_boundary; /* (nisle) host */
+} pyomgpu_islands;
+
+/* Result of one solve. */
+typedef struct pyomgpu_solve_info {
+  int32_t iterations;       /* congr_itts (inner iterations summed for refinement) */
+  int32_t converged;        /* the logical ``converged`` of congrad_streamfunction */
+  int32_t status;           /* PYOMGPU_* */
+  int32_t outer_iterations; /* refinement sweeps (pyomgpu_solve_rtol F32) */
+  double estimated_error;   /* the reference's estimated_error */
+  double rel_residual;      /* FP64 ||b-Ax||/||b|| over the unknowns (solve_rtol only) */
+  double device_ms;         /* device time of the solve, CUDA events on the stream */
+} pyomgpu_solve_info;
+
+/* Model arrays of one time step (all DEVICE pointers, Fortran layout). */
+typedef struct pyomgpu_state {
+  int32_t nz;
+  int32_t taum1, tau, taup1;    /* 1-based time levels */
+  int32_t congr_max_iterations;
+  int32_t congr_itts;           /* out */
+  double dt_mom, AB_eps, grav, rho_0, congr_epsilon;
+  const double *dzt, *dzw;      /* [nz] */
+  const double *maskT, *maskU, *maskV; /* (nx+4,ny+4,nz) */
+  const double* rho;            /* (nx+4,ny+4,nz,3) */
+  double *u, *v, *du, *dv;      /* (nx+4,ny+4,nz,3) */
+  const double *du_mix, *dv_mix;/* (nx+4,ny+4,nz) */
+  double* p_hydro;              /* (nx+4,ny+4,nz) */
+  double *psi, *dpsi;           /* (nx+4,ny+4,3) */
+  double* dpsin;                /* (nisle,3), streamfunction only */
+} pyomgpu_state;
+
+/* ---- library -------------------------------------------------------------- */
+int32_t pyomgpu_version(void);
+const char* pyomgpu_last_error(void);
+
+/* Create a context for one grid on the current CUDA device: builds the
+ * streamfunction operator (and the surface-pressure operator when hu/hv and
+ * maskT_top are given) in device memory.  make_coeff_* of the reference is
+ * run once and kept, like its SAVE'd cf (solve_streamfct.f90:172-180). */
+int32_t pyomgpu_ctx_create(const pyomgpu_grid* grid, pyomgpu_ctx** out);
+void pyomgpu_ctx_destroy(pyomgpu_ctx* ctx);
+
+/* Device-side time limit of every grid-barrier wait (default 2 s). */
+int32_t pyomgpu_set_sync_timeout(pyomgpu_ctx* ctx, double seconds);
+/* Failure-detection test hook: when enabled, the next solver launch waits at
+ * its first grid barrier for one block more than it launched, so every wait
+ * runs into the time limit and the call returns PYOMGPU_TIMEOUT (no fault, the
+ * context stays usable).  Cleared after that launch. */
+int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* ctx, int32_t enable);
+
+/* ---- islands (streamfct_init.f90, island_module.f90) ------------------------ */
+/* isleperim on a (imt,jmt) int map; map, nippts (>= mnisle entries) host.
+ * Limits default to the reference's (mnisle 1000, maxipp 20000, maxq 10000)
+ * when passed as 0. */
+int32_t pyomgpu_isleperim(const int32_t* kmt, int32_t imt, int32_t jmt, int32_t cyclic, int32_t mnisle,
+                          int32_t maxipp, int32_t maxq, int32_t* map, int32_t* nisle, int32_t* nippts);
+
+/* Island labels and perimeters of streamfunction_init (streamfct_init.f90:35-267)
+ * on the host, without the psin solves.  kbot is (nx+4, ny+4) host.  Call
+ * first with boundary == NULL to get nisle and max_boundary, then with arrays
+ * of (nisle, max_boundary, 2) / (nisle) entries. */
+int32_t pyomgpu_island_boundaries(int32_t nx, int32_t ny, int32_t cyclic_x, const int32_t* kbot, int32_t mnisle,
+                                  int32_t maxipp, int32_t maxq, int32_t* nisle, int32_t* max_boundary,
+                                  int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary);
+
+/* Whole of streamfunction_init: land map from kbot (host), island labels,
+ * perimeter tracing, one psin solve per island (batched on the GPU) and the
+ * line_psin matrix.  Results stay in the context; read them with
+ * pyomgpu_island_sizes / pyomgpu_get_islands. */
+int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* ctx, const int32_t* kbot, int32_t mnisle, int32_t maxipp,
+                                    int32_t maxq, double congr_epsilon, int32_t congr_max_iterations,
+                                    pyomgpu_stream stream);
+int32_t pyomgpu_island_sizes(pyomgpu_ctx* ctx, int32_t* nisle, int32_t* max_boundary);
+/* Copies out boundary/line_dir/nr_boundary (host), psin (host or device,
+ * (nx+4,ny+4,nisle)), line_psin (host, (nisle,nisle)) and the psin iteration
+ * counts (host, nisle; may be NULL). */
+int32_t pyomgpu_get_islands(pyomgpu_ctx* ctx, int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary,
+                            double* psin, double* line_psin, int32_t* psin_iterations, pyomgpu_stream stream);
+/* Import islands computed elsewhere (e.g. by the Fortran streamfunction_init):
+ * builds Z (make_inv_sfc).  psin (host or device) and line_psin (host) may be
+ * NULL when only congrad_streamfunction is needed. */
+int32_t pyomgpu_set_islands(pyomgpu_ctx* ctx, const pyomgpu_islands* isl, const double* psin,
+                            const double* line_psin, pyomgpu_stream stream);
+
+/* ---- solvers ---------------------------------------------------------------- */
+/* congrad_streamfunction (solve_streamfct.f90:153-327): FP64 Jacobi-PCG with the
+ * reference's stopping estimate, divergence test and s.As guard.  forc is
+ * read, sol (in/out) is updated in place; both host or device. */
+int32_t pyomgpu_congrad_streamfunction(pyomgpu_ctx* ctx, const double* forc, double* sol, double congr_epsilon,
+                                       int32_t congr_max_iterations, pyomgpu_solve_info* info,
+                                       pyomgpu_stream stream);
+
+/* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
+ * products.  psi is psi(:,:,taup1), in/out, host or device. */
+int32_t pyomgpu_congrad_surf_press(pyomgpu_ctx* ctx, const double* forc, double* psi, double congr_epsilon,
+                                   int32_t congr_max_iterations, pyomgpu_solve_info* info, pyomgpu_stream stream);
+
+/* Solve A sol = forc (streamfunction operator, island perimeters Dirichlet)
+ * until the FP64 true relative residual ||forc - A sol||_2/||forc||_2 over the
+ * unknowns is <= rtol.  precision: PYOMGPU_PREC_F64 or PYOMGPU_PREC_F32.
+ * Measurement entry point of the ms/solve metric; not in the reference. */
+int32_t pyomgpu_solve_rtol(pyomgpu_ctx* ctx, const double* forc, double* sol, double rtol, int32_t precision,
+                           int32_t max_iterations, pyomgpu_solve_info* info, pyomgpu_stream stream);
+
+/* ---- operator utilities ------------------------------------------------------ */
+/* res = A p over the interior, zero halo (apply_op, solve_pressure.f90:254-274). */
+int32_t pyomgpu_apply_op(pyomgpu_ctx* ctx, int32_t op, const double* p, double* res, pyomgpu_stream stream);
+/* The Jacobi inverse Z of make_inv_sfc (solve_streamfct.f90:381-422), Fortran layout. */
+int32_t pyomgpu_get_inv_diag(pyomgpu_ctx* ctx, double* Z, pyomgpu_stream stream);
+/* line_integral (streamfct_init.f90:311-377) of island isle (1-based). */
+int32_t pyomgpu_line_integral(pyomgpu_ctx* ctx, int32_t isle, const double* uloc, const double* vloc, double* line,
+                              pyomgpu_stream stream);
+
+/* ---- one time step ------------------------------------------------------------ */
+/* solve_streamfunction (solve_streamfct.f90:10-120) on device-resident model
+ * arrays; islands must have been set up.  OBC (set_obc_streamfct) is not
+ * supported. */
+int32_t pyomgpu_solve_streamfunction(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_solve_info* info,
+                                     pyomgpu_stream stream);
+/* solve_pressure (solve_pressure.f90:10-82) on device-resident model arrays. */
+int32_t pyomgpu_solve_pressure(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_solve_info* info,
+                               pyomgpu_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,840 @@
+// C ABI (include/pyomgpu.h): context, island set-up and the solver entry
+// points.  Host orchestration only; every array operation runs on the GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pyomgpu.h"
+#include "cg_ref.cuh"
+#include "common.cuh"
+#include "islands.h"
+#include "kernels.cuh"
+
+using namespace pyomgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail(PYOMGPU_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,   \
+                                       cudaGetErrorString(e_));                                    \
+  } while (0)
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) return fail(PYOMGPU_ENOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  return 0;
+}
+
+}  // namespace
+
+struct pyomgpu_ctx {
+  int device = 0, nsm = 0;
+  Geo g{};
+  int nx = 0, ny = 0;
+  size_t n2 = 0;  // (nx+4)*(ny+4)
+  int free_surface = 0;
+  double grav = 0, dt_mom = 0;
+  std::vector<double> h_maskU, h_maskV;
+  // device grid copies
+  double *dxt = nullptr, *dxu = nullptr, *dyt = nullptr, *dyu = nullptr, *cost = nullptr, *cosu = nullptr;
+  double *hur = nullptr, *hvr = nullptr, *hu = nullptr, *hv = nullptr, *mT = nullptr, *mU = nullptr, *mV = nullptr;
+  OpBuf sf, sp;
+  bool have_sp = false;
+  // islands
+  bool have_islands = false, have_psin = false, have_line_psin = false, lu_singular = false;
+  IslandSet isl;
+  IslandDev idev;
+  std::vector<int> psin_iters;
+  std::vector<double> line_psin;
+  int *bnd_i = nullptr, *bnd_j = nullptr;
+  int nbnd = 0;
+  double* psin = nullptr;  // Fortran layout, nisle fields
+  double *lu = nullptr, *line_forc = nullptr, *line_psi0 = nullptr;
+  int* ipiv = nullptr;
+  // CG work
+  double *res = nullptr, *s0 = nullptr, *s1 = nullptr, *As = nullptr, *sol = nullptr;
+  double *stage_a = nullptr, *stage_b = nullptr, *fpx = nullptr, *fpy = nullptr, *forc = nullptr, *zeros = nullptr;
+  double *part = nullptr, *scal = nullptr;
+  SyncCtl* ctl = nullptr;
+  double* slots = nullptr;
+  CGResult* d_result = nullptr;
+  CGResult* h_result = nullptr;
+  double* h_scal = nullptr;
+  int max_blocks = 0;  // co-resident blocks of the CG kernels
+  double timeout_s = 2.0;
+  unsigned stall_next = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+  ~pyomgpu_ctx() {
+    void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
+                    sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,
+                    res, s0, s1, As, sol, stage_a, stage_b, fpx, fpy, forc, zeros, part, scal, ctl, slots, d_result,
+                    idev.seg_i, idev.seg_j, idev.seg_d, idev.seg_off};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+    if (h_result) cudaFreeHost(h_result);
+    if (h_scal) cudaFreeHost(h_scal);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+namespace {
+
+int upload(double** d, const double* h, size_t n) {
+  if (int rc = dalloc(d, n)) return rc;
+  if (h)
+    CK(cudaMemcpy(*d, h, n * sizeof(double), cudaMemcpyHostToDevice));
+  else
+    CK(cudaMemset(*d, 0, n * sizeof(double)));
+  return 0;
+}
+
+// Stage a Fortran-layout (nx+4, ny+4) array: device pointers pass through,
+// host pointers are copied into `stage`.
+int stage_in(pyomgpu_ctx* c, const double* user, double* stage, const double** out, cudaStream_t st) {
+  if (is_device_ptr(user)) {
+    *out = user;
+    return 0;
+  }
+  CK(cudaMemcpyAsync(stage, user, c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+  *out = stage;
+  return 0;
+}
+
+struct LaunchShape {
+  int grid, R, SX, SY;
+};
+
+LaunchShape cg_shape(const pyomgpu_ctx* c) {
+  LaunchShape s;
+  s.SX = (c->nx + 31) / 32;
+  const int maxwarps = c->max_blocks * (kCGThreads / 32);
+  int R = (int)std::ceil((double)s.SX * c->ny / std::max(1, maxwarps));
+  R = std::max(4, std::min(R, 256));
+  s.R = R;
+  s.SY = (c->ny + R - 1) / R;
+  const int strips = s.SX * s.SY;
+  s.grid = std::max(1, std::min(c->max_blocks, (strips + (kCGThreads / 32) - 1) / (kCGThreads / 32)));
+  return s;
+}
+
+// Runs the persistent CG kernel on c->sol (padded, already packed) with the
+// Fortran-layout device forcing.  Fills info (iterations, status, timing).
+int run_cg_ref(pyomgpu_ctx* c, bool surf_press, const double* forc_dev, double eps, int max_it, double rtol,
+               pyomgpu_solve_info* info, cudaStream_t st) {
+  const OpBuf& op = surf_press ? c->sp : c->sf;
+  const size_t bytes = c->g.size() * sizeof(double);
+  CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
+  CK(cudaMemsetAsync(c->res, 0, bytes, st));
+  CK(cudaMemsetAsync(c->s0, 0, bytes, st));
+  CK(cudaMemsetAsync(c->s1, 0, bytes, st));
+  LaunchShape sh = cg_shape(c);
+  CGRefParams P{};
+  P.g = c->g;
+  P.op = op.dev();
+  P.forc = forc_dev;
+  P.sol = c->sol;
+  P.res = c->res;
+  P.s[0] = c->s0;
+  P.s[1] = c->s1;
+  P.As = c->As;
+  P.eps = eps;
+  P.max_it = max_it;
+  P.rtol = rtol;
+  P.R = sh.R;
+  P.SX = sh.SX;
+  P.SY = sh.SY;
+  P.ctl = c->ctl;
+  P.slots = c->slots;
+  P.timeout_ns = (unsigned long long)(c->timeout_s * 1e9);
+  P.stall_extra = c->stall_next;
+  c->stall_next = 0;
+  P.out = c->d_result;
+  void* args[] = {&P};
+  CK(cudaEventRecord(c->e0, st));
+  CK(cudaLaunchCooperativeKernel(cg_ref_kernel_ptr(surf_press), dim3(sh.grid), dim3(kCGThreads), args, 0, st));
+  CK(cudaEventRecord(c->e1, st));
+  CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
+  int err = 0;
+  CK(cudaMemcpyAsync(c->h_scal, &c->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::memcpy(&err, c->h_scal, sizeof(int));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->e0, c->e1));
+  if (info) {
+    info->iterations = c->h_result->iterations;
+    info->converged = c->h_result->converged;
+    info->status = c->h_result->status;
+    info->outer_iterations = 1;
+    info->estimated_error = c->h_result->est;
+    info->rel_residual = -1.0;
+    info->device_ms = ms;
+    if (err) {
+      info->status = PYOMGPU_TIMEOUT;
+      info->converged = 0;
+    }
+  }
+  if (err) return fail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded %.3f s", c->timeout_s);
+  return c->h_result->status;
+}
+
+int rebuild_islands(pyomgpu_ctx* c) {
+  // Z of make_inv_sfc and the segment lists of line_integral from c->isl.
+  const IslandSet& I = c->isl;
+  std::vector<int> bi, bj;
+  std::vector<int> si, sj, sd, off((size_t)I.nisle + 1, 0);
+  for (int k = 1; k <= I.nisle; ++k) {
+    off[k - 1] = (int)si.size();
+    for (int n = 1; n <= I.nr_boundary[k - 1]; ++n) {
+      const size_t o = (size_t)(k - 1) + (size_t)(n - 1) * I.nisle;
+      const int i = I.boundary[o], j = I.boundary[o + (size_t)I.nisle * I.max_boundary];
+      bi.push_back(i);
+      bj.push_back(j);
+      if (i >= 0 && i <= c->nx && j >= 0 && j <= c->ny) {  // line_integral window (streamfct_init.f90:324-332)
+        const int d0 = I.line_dir[o], d1 = I.line_dir[o + (size_t)I.nisle * I.max_boundary];
+        int d;
+        if (d0 == 1 && d1 == 0)
+          d = 0;
+        else if (d0 == -1 && d1 == 0)
+          d = 1;
+        else if (d0 == 0 && d1 == 1)
+          d = 2;
+        else if (d0 == 0 && d1 == -1)
+          d = 3;
+        else
+          return fail(PYOMGPU_EISLAND, "missing line_dir in line integral (island %d point %d)", k, n);
+        si.push_back(i);
+        sj.push_back(j);
+        sd.push_back(d);
+      }
+    }
+  }
+  off[I.nisle] = (int)si.size();
+  for (int* p : {c->bnd_i, c->bnd_j, c->idev.seg_i, c->idev.seg_j, c->idev.seg_d, c->idev.seg_off})
+    if (p) cudaFree(p);
+  c->bnd_i = c->bnd_j = nullptr;
+  c->idev = IslandDev{};
+  c->nbnd = (int)bi.size();
+  if (int rc = dalloc(&c->bnd_i, bi.size())) return rc;
+  if (int rc = dalloc(&c->bnd_j, bj.size())) return rc;
+  if (!bi.empty()) {
+    CK(cudaMemcpy(c->bnd_i, bi.data(), bi.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->bnd_j, bj.data(), bj.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->idev.nisle = I.nisle;
+  if (int rc = dalloc(&c->idev.seg_i, si.size())) return rc;
+  if (int rc = dalloc(&c->idev.seg_j, sj.size())) return rc;
+  if (int rc = dalloc(&c->idev.seg_d, sd.size())) return rc;
+  if (int rc = dalloc(&c->idev.seg_off, off.size())) return rc;
+  if (!si.empty()) {
+    CK(cudaMemcpy(c->idev.seg_i, si.data(), si.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->idev.seg_j, sj.data(), sj.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->idev.seg_d, sd.data(), sd.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(c->idev.seg_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  launch_build_inv_diag(c->g, c->sf, c->bnd_i, c->bnd_j, c->nbnd, 0);
+  CK(cudaGetLastError());
+  CK(cudaDeviceSynchronize());
+  for (double* p : {c->line_forc, c->line_psi0})
+    if (p) cudaFree(p);
+  c->line_forc = c->line_psi0 = nullptr;
+  if (int rc = dalloc(&c->line_forc, (size_t)std::max(1, I.nisle))) return rc;
+  if (int rc = dalloc(&c->line_psi0, (size_t)std::max(1, I.nisle))) return rc;
+  c->have_islands = true;
+  return 0;
+}
+
+LineGeo line_geo(const pyomgpu_ctx* c) {
+  return LineGeo{c->dxu, c->dyu, c->cost, c->cosu, c->dxt, c->dyt, c->hur, c->hvr, c->mU, c->mV};
+}
+
+int factor_line_psin(pyomgpu_ctx* c) {
+  const int nisle = c->isl.nisle;
+  c->lu_singular = false;
+  if (nisle <= 1) return 0;
+  const int m = nisle - 1;
+  std::vector<double> a((size_t)m * m);
+  for (int col = 0; col < m; ++col)
+    for (int r = 0; r < m; ++r) a[(size_t)r + (size_t)col * m] = c->line_psin[(size_t)(r + 1) + (size_t)(col + 1) * nisle];
+  std::vector<int> ipiv;
+  const int info = lu_factor(m, a, ipiv);
+  c->lu_singular = info != 0;
+  for (double* p : {c->lu})
+    if (p) cudaFree(p);
+  if (c->ipiv) cudaFree(c->ipiv);
+  if (int rc = dalloc(&c->lu, a.size())) return rc;
+  if (int rc = dalloc(&c->ipiv, ipiv.size())) return rc;
+  CK(cudaMemcpy(c->lu, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->ipiv, ipiv.data(), ipiv.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// psin solves (streamfct_init.f90:272-287) and line_psin (:292-303).
+int psin_and_line_psin(pyomgpu_ctx* c, double eps, int max_it, cudaStream_t st) {
+  const int nisle = c->isl.nisle;
+  if (c->psin) cudaFree(c->psin);
+  c->psin = nullptr;
+  if (int rc = dalloc(&c->psin, c->n2 * (size_t)std::max(1, nisle))) return rc;
+  c->psin_iters.assign((size_t)nisle, 0);
+  int worst = 0;
+  std::vector<double> init(c->n2);
+  const IslandSet& I = c->isl;
+  for (int isle = 1; isle <= nisle; ++isle) {
+    std::fill(init.begin(), init.end(), 0.0);
+    for (int n = 1; n <= I.nr_boundary[isle - 1]; ++n) {
+      const size_t o = (size_t)(isle - 1) + (size_t)(n - 1) * nisle;
+      const int i = I.boundary[o], j = I.boundary[o + (size_t)nisle * I.max_boundary];
+      if (i >= -1 && i <= c->nx + 2 && j >= -1 && j <= c->ny + 2) init[fidx(c->nx, i, j)] = 1.0;
+    }
+    double* dst = c->psin + (size_t)(isle - 1) * c->n2;
+    CK(cudaMemcpyAsync(c->stage_b, init.data(), c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_pack(c->g, c->stage_b, c->sol, true, st);
+    pyomgpu_solve_info info{};
+    int rc = run_cg_ref(c, false, c->zeros, eps, max_it, 0.0, &info, st);
+    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    if (info.status == PYOMGPU_NAN) return fail(PYOMGPU_NAN, "psin solve of island %d: estimated error is NaN", isle);
+    worst = std::max(worst, info.status);
+    c->psin_iters[isle - 1] = info.iterations;
+    launch_unpack(c->g, c->sol, dst, true, false, false, st);
+  }
+  CK(cudaGetLastError());
+  c->have_psin = true;
+  // line_psin(n, isle) = line integral around island n of the velocity of psin(:,:,isle)
+  double* dout = nullptr;
+  if (int rc = dalloc(&dout, (size_t)nisle * nisle)) return rc;
+  launch_line_integral_psi(c->nx, c->ny, c->idev, line_geo(c), c->psin, c->n2, nisle, 0, nisle, dout, st);
+  c->line_psin.assign((size_t)nisle * nisle, 0.0);
+  cudaError_t e = cudaMemcpyAsync(c->line_psin.data(), dout, sizeof(double) * nisle * nisle, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail(PYOMGPU_ECUDA, "line_psin: %s", cudaGetErrorString(e));
+  c->have_line_psin = true;
+  if (int rc = factor_line_psin(c)) return rc;
+  return worst;
+}
+
+int island_error(int rc) {
+  switch (rc) {
+    case kIslMaxipp:
+      return fail(PYOMGPU_EISLAND, "maxipp too small (island_module.f90:256)");
+    case kIslQueue:
+      return fail(PYOMGPU_EISLAND, "queue fault in qpush (island_module.f90:310): raise maxq");
+    case kIslMnisle:
+      return fail(PYOMGPU_EISLAND, "mnisle too small (island_module.f90:86)");
+    case kIslMissing:
+      return fail(PYOMGPU_EISLAND, "cannot find island in map (streamfct_init.f90:81)");
+    case kIslNoStart:
+      return fail(PYOMGPU_EISLAND, "found no starting point for line integral (streamfct_init.f90:162)");
+    case kIslLostTrack:
+      return fail(PYOMGPU_EISLAND, "unknown situation or lost track (streamfct_init.f90:224)");
+    case kIslMaxBoundary:
+      return fail(PYOMGPU_EISLAND, "increase max_boundary (streamfct_init.f90:252)");
+    default:
+      return fail(PYOMGPU_EISLAND, "island map read outside the grid");
+  }
+}
+
+IslandLimits limits(int mnisle, int maxipp, int maxq) {
+  IslandLimits L;
+  if (mnisle > 0) L.mnisle = mnisle;
+  if (maxipp > 0) L.maxipp = maxipp;
+  if (maxq > 0) L.maxq = maxq;
+  return L;
+}
+
+StepDev step_dev(const pyomgpu_ctx* c, const pyomgpu_state* s) {
+  StepDev d{};
+  d.nx = c->nx;
+  d.ny = c->ny;
+  d.nz = s->nz;
+  d.cyclic_x = c->g.cyclic_x;
+  d.cyclic_y = c->g.cyclic_y;
+  d.taum1 = s->taum1;
+  d.tau = s->tau;
+  d.taup1 = s->taup1;
+  d.dt_mom = s->dt_mom;
+  d.AB_eps = s->AB_eps;
+  d.grav = s->grav;
+  d.rho_0 = s->rho_0;
+  d.dxt = c->dxt;
+  d.dxu = c->dxu;
+  d.dyt = c->dyt;
+  d.dyu = c->dyu;
+  d.cost = c->cost;
+  d.cosu = c->cosu;
+  d.dzt = s->dzt;
+  d.dzw = s->dzw;
+  d.hur = c->hur;
+  d.hvr = c->hvr;
+  d.maskT = s->maskT;
+  d.maskU = s->maskU;
+  d.maskV = s->maskV;
+  d.rho = s->rho;
+  d.du_mix = s->du_mix;
+  d.dv_mix = s->dv_mix;
+  d.u = s->u;
+  d.v = s->v;
+  d.du = s->du;
+  d.dv = s->dv;
+  d.p_hydro = s->p_hydro;
+  d.psi = s->psi;
+  d.dpsi = s->dpsi;
+  return d;
+}
+
+bool state_ok(const pyomgpu_state* s) {
+  const void* ptrs[] = {s->dzt, s->dzw, s->maskT, s->maskU, s->maskV, s->rho, s->u, s->v, s->du, s->dv,
+                        s->du_mix, s->dv_mix, s->p_hydro, s->psi, s->dpsi};
+  for (const void* p : ptrs)
+    if (!is_device_ptr(p)) return false;
+  return s->nz >= 1 && s->tau >= 1 && s->tau <= 3 && s->taup1 >= 1 && s->taup1 <= 3 && s->taum1 >= 1 &&
+         s->taum1 <= 3;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int32_t pyomgpu_version(void) { return 1; }
+
+const char* pyomgpu_last_error(void) { return g_last_error.c_str(); }
+
+int32_t pyomgpu_ctx_create(const pyomgpu_grid* gr, pyomgpu_ctx** out) {
+  if (!gr || !out) return fail(PYOMGPU_EINVAL, "null argument");
+  *out = nullptr;
+  if (gr->onx != 2) return fail(PYOMGPU_EINVAL, "onx must be 2 (got %d)", gr->onx);
+  if (gr->nx < 4 || gr->ny < 4) return fail(PYOMGPU_EINVAL, "grid must be at least 4x4 (got %dx%d)", gr->nx, gr->ny);
+  if (!gr->dxt || !gr->dxu || !gr->dyt || !gr->dyu || !gr->cost || !gr->cosu || !gr->hur || !gr->hvr)
+    return fail(PYOMGPU_EINVAL, "missing grid array");
+  auto* c = new pyomgpu_ctx();
+  auto bail = [&](int rc) {
+    delete c;
+    return rc;
+  };
+  CK(cudaGetDevice(&c->device));
+  CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
+  c->nx = gr->nx;
+  c->ny = gr->ny;
+  c->n2 = (size_t)(c->nx + 4) * (c->ny + 4);
+  c->g.nx = c->nx;
+  c->g.ny = c->ny;
+  c->g.pitch = ((c->nx + 4 + kXOff) + 31) / 32 * 32;
+  c->g.cyclic_x = gr->enable_cyclic_x ? 1 : 0;
+  c->g.cyclic_y = gr->enable_cyclic_y ? 1 : 0;
+  c->free_surface = gr->enable_free_surface;
+  c->grav = gr->grav;
+  c->dt_mom = gr->dt_mom;
+  const size_t X = c->nx + 4, Y = c->ny + 4, n2 = c->n2;
+  int rc;
+  if ((rc = upload(&c->dxt, gr->dxt, X)) || (rc = upload(&c->dxu, gr->dxu, X)) || (rc = upload(&c->dyt, gr->dyt, Y)) ||
+      (rc = upload(&c->dyu, gr->dyu, Y)) || (rc = upload(&c->cost, gr->cost, Y)) ||
+      (rc = upload(&c->cosu, gr->cosu, Y)) || (rc = upload(&c->hur, gr->hur, n2)) ||
+      (rc = upload(&c->hvr, gr->hvr, n2)) || (rc = upload(&c->mU, gr->maskU_top, n2)) ||
+      (rc = upload(&c->mV, gr->maskV_top, n2)))
+    return bail(rc);
+  c->have_sp = gr->hu && gr->hv && gr->maskT_top;
+  if (c->have_sp) {
+    if ((rc = upload(&c->hu, gr->hu, n2)) || (rc = upload(&c->hv, gr->hv, n2)) || (rc = upload(&c->mT, gr->maskT_top, n2)))
+      return bail(rc);
+  }
+  const size_t P = c->g.size();
+  for (OpBuf* op : {&c->sf, &c->sp}) {
+    if (op == &c->sp && !c->have_sp) break;
+    if ((rc = dalloc(&op->FX, P)) || (rc = dalloc(&op->FY, P)) || (rc = dalloc(&op->W, P)) ||
+        (rc = dalloc(&op->ax, X)) || (rc = dalloc(&op->bx, Y)) || (rc = dalloc(&op->by, Y)))
+      return bail(rc);
+    if (cudaMemset(op->FX, 0, P * 8) || cudaMemset(op->FY, 0, P * 8) || cudaMemset(op->W, 0, P * 8))
+      return bail(fail(PYOMGPU_ECUDA, "memset"));
+  }
+  GridDev gd{c->nx, c->ny, c->dxt, c->dxu, c->dyt, c->dyu, c->cost, c->cosu, c->hur, c->hvr, c->hu, c->hv, c->mT};
+  launch_build_op_streamfunction(gd, c->g, c->sf, 0);
+  launch_build_inv_diag(c->g, c->sf, nullptr, nullptr, 0, 0);
+  if (c->have_sp) {
+    launch_build_op_surf_press(gd, c->g, c->sp, 0);
+    c->sp.dcoef = c->free_surface ? -1.0 / (c->grav * (c->dt_mom * c->dt_mom)) : 0.0;
+  }
+  if ((rc = dalloc(&c->res, P)) || (rc = dalloc(&c->s0, P)) || (rc = dalloc(&c->s1, P)) || (rc = dalloc(&c->As, P)) ||
+      (rc = dalloc(&c->sol, P)) || (rc = dalloc(&c->stage_a, n2)) || (rc = dalloc(&c->stage_b, n2)) ||
+      (rc = dalloc(&c->fpx, n2)) || (rc = dalloc(&c->fpy, n2)) || (rc = dalloc(&c->forc, n2)) ||
+      (rc = dalloc(&c->zeros, n2)) || (rc = dalloc(&c->part, 2 * 4096)) || (rc = dalloc(&c->scal, 16)))
+    return bail(rc);
+  if (cudaMemset(c->zeros, 0, n2 * 8) || cudaMemset(c->sol, 0, P * 8) || cudaMemset(c->As, 0, P * 8))
+    return bail(fail(PYOMGPU_ECUDA, "memset"));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_ref_kernel_ptr(false), kCGThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    return bail(fail(PYOMGPU_ECUDA, "occupancy query failed"));
+  int per_sm2 = per_sm;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, cg_ref_kernel_ptr(true), kCGThreads, 0);
+  c->max_blocks = std::min(per_sm, std::max(1, per_sm2)) * c->nsm;
+  if ((rc = dalloc((double**)&c->ctl, 2)) || (rc = dalloc(&c->slots, (size_t)2 * c->max_blocks * 4)) ||
+      (rc = dalloc((double**)&c->d_result, 4)))
+    return bail(rc);
+  if (cudaMallocHost((void**)&c->h_result, sizeof(CGResult)) != cudaSuccess ||
+      cudaMallocHost((void**)&c->h_scal, 64) != cudaSuccess)
+    return bail(fail(PYOMGPU_ENOMEM, "cudaMallocHost"));
+  if (cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess)
+    return bail(fail(PYOMGPU_ECUDA, "event create"));
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return bail(fail(PYOMGPU_ECUDA, "ctx build: %s", cudaGetErrorString(e)));
+  *out = c;
+  return PYOMGPU_OK;
+}
+
+void pyomgpu_ctx_destroy(pyomgpu_ctx* c) { delete c; }
+
+int32_t pyomgpu_set_sync_timeout(pyomgpu_ctx* c, double seconds) {
+  if (!c || !(seconds > 0)) return fail(PYOMGPU_EINVAL, "bad timeout");
+  c->timeout_s = seconds;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* c, int32_t enable) {
+  if (!c) return fail(PYOMGPU_EINVAL, "null context");
+  c->stall_next = enable ? 1u : 0u;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_island_boundaries(int32_t nx, int32_t ny, int32_t cyclic_x, const int32_t* kbot, int32_t mnisle,
+                                  int32_t maxipp, int32_t maxq, int32_t* nisle, int32_t* max_boundary,
+                                  int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary) {
+  if (!kbot || !nisle || !max_boundary || nx < 4 || ny < 4) return fail(PYOMGPU_EINVAL, "bad arguments");
+  IslandLimits L = limits(mnisle, maxipp, maxq);
+  std::vector<int> allmap;
+  int n = 0, mb = 0;
+  int rc = island_map(nx, ny, cyclic_x != 0, kbot, L, allmap, &n, &mb);
+  if (rc) return island_error(rc);
+  if (!boundary) {
+    *nisle = n;
+    *max_boundary = mb;
+    return PYOMGPU_OK;
+  }
+  if (*nisle != n || *max_boundary != mb || !line_dir || !nr_boundary)
+    return fail(PYOMGPU_EINVAL, "island arrays sized for (%d,%d), need (%d,%d)", *nisle, *max_boundary, n, mb);
+  IslandSet S;
+  rc = island_trace(nx, ny, cyclic_x != 0, allmap, n, mb, L, S);
+  if (rc) return island_error(rc);
+  std::copy(S.boundary.begin(), S.boundary.end(), boundary);
+  std::copy(S.line_dir.begin(), S.line_dir.end(), line_dir);
+  std::copy(S.nr_boundary.begin(), S.nr_boundary.end(), nr_boundary);
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_isleperim(const int32_t* kmt, int32_t imt, int32_t jmt, int32_t cyclic, int32_t mnisle,
+                          int32_t maxipp, int32_t maxq, int32_t* map, int32_t* nisle, int32_t* nippts) {
+  if (!kmt || !map || !nisle || imt < 3 || jmt < 3) return fail(PYOMGPU_EINVAL, "bad isleperim arguments");
+  IslandLimits L = limits(mnisle, maxipp, maxq);
+  std::vector<int> np;
+  int rc = pyomgpu::isleperim(kmt, imt, jmt, cyclic != 0, L, map, nisle, &np);
+  if (rc) return island_error(rc);
+  if (nippts) std::copy(np.begin(), np.end(), nippts);
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* c, const int32_t* kbot, int32_t mnisle, int32_t maxipp, int32_t maxq,
+                                    double eps, int32_t max_it, pyomgpu_stream stream) {
+  if (!c || !kbot) return fail(PYOMGPU_EINVAL, "null argument");
+  if (c->g.cyclic_y)  // streamfct_init.f90:27-30
+    return fail(PYOMGPU_EINVAL, "cyclic meridional boundary conditions not implemented for the streamfunction");
+  cudaStream_t st = (cudaStream_t)stream;
+  IslandLimits L = limits(mnisle, maxipp, maxq);
+  std::vector<int> allmap;
+  int nisle = 0, maxb = 0;
+  int rc = island_map(c->nx, c->ny, c->g.cyclic_x != 0, kbot, L, allmap, &nisle, &maxb);
+  if (rc) return island_error(rc);
+  IslandSet S;
+  rc = island_trace(c->nx, c->ny, c->g.cyclic_x != 0, allmap, nisle, maxb, L, S);
+  if (rc) return island_error(rc);
+  c->isl = std::move(S);
+  if ((rc = rebuild_islands(c))) return rc;
+  return psin_and_line_psin(c, eps, max_it, st);
+}
+
+int32_t pyomgpu_island_sizes(pyomgpu_ctx* c, int32_t* nisle, int32_t* max_boundary) {
+  if (!c || !c->have_islands) return fail(PYOMGPU_ESTATE, "no islands set");
+  if (nisle) *nisle = c->isl.nisle;
+  if (max_boundary) *max_boundary = c->isl.max_boundary;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_get_islands(pyomgpu_ctx* c, int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary, double* psin,
+                            double* line_psin, int32_t* psin_iterations, pyomgpu_stream stream) {
+  if (!c || !c->have_islands) return fail(PYOMGPU_ESTATE, "no islands set");
+  const IslandSet& I = c->isl;
+  if (boundary) std::copy(I.boundary.begin(), I.boundary.end(), boundary);
+  if (line_dir) std::copy(I.line_dir.begin(), I.line_dir.end(), line_dir);
+  if (nr_boundary) std::copy(I.nr_boundary.begin(), I.nr_boundary.end(), nr_boundary);
+  if (psin_iterations && !c->psin_iters.empty()) std::copy(c->psin_iters.begin(), c->psin_iters.end(), psin_iterations);
+  if (line_psin && c->have_line_psin) std::copy(c->line_psin.begin(), c->line_psin.end(), line_psin);
+  if (psin && c->have_psin) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = c->n2 * (size_t)I.nisle * sizeof(double);
+    CK(cudaMemcpyAsync(psin, c->psin, bytes, cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_set_islands(pyomgpu_ctx* c, const pyomgpu_islands* isl, const double* psin, const double* line_psin,
+                            pyomgpu_stream stream) {
+  if (!c || !isl || isl->nisle < 0 || (isl->nisle > 0 && (!isl->boundary || !isl->line_dir || !isl->nr_boundary)))
+    return fail(PYOMGPU_EINVAL, "bad island description");
+  IslandSet S;
+  S.nisle = isl->nisle;
+  S.max_boundary = isl->max_boundary;
+  const size_t nb = (size_t)isl->nisle * isl->max_boundary * 2;
+  S.boundary.assign(isl->boundary, isl->boundary + nb);
+  S.line_dir.assign(isl->line_dir, isl->line_dir + nb);
+  S.nr_boundary.assign(isl->nr_boundary, isl->nr_boundary + isl->nisle);
+  for (int k = 0; k < S.nisle; ++k)
+    if (S.nr_boundary[k] < 0 || S.nr_boundary[k] > S.max_boundary)
+      return fail(PYOMGPU_EINVAL, "nr_boundary(%d) out of range", k + 1);
+  c->isl = std::move(S);
+  c->have_psin = c->have_line_psin = false;
+  int rc = rebuild_islands(c);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (psin) {
+    if (c->psin) cudaFree(c->psin);
+    c->psin = nullptr;
+    if ((rc = dalloc(&c->psin, c->n2 * (size_t)std::max(1, c->isl.nisle)))) return rc;
+    CK(cudaMemcpyAsync(c->psin, psin, c->n2 * (size_t)c->isl.nisle * sizeof(double), cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+    c->have_psin = true;
+  }
+  if (line_psin) {
+    c->line_psin.assign(line_psin, line_psin + (size_t)c->isl.nisle * c->isl.nisle);
+    c->have_line_psin = true;
+    if ((rc = factor_line_psin(c))) return rc;
+  }
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_congrad_streamfunction(pyomgpu_ctx* c, const double* forc, double* sol, double eps, int32_t max_it,
+                                       pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!c || !forc || !sol) return fail(PYOMGPU_EINVAL, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* f = nullptr;
+  if (int rc = stage_in(c, forc, c->stage_a, &f, st)) return rc;
+  const bool sol_dev = is_device_ptr(sol);
+  const double* s_in = sol;
+  if (!sol_dev) {
+    CK(cudaMemcpyAsync(c->stage_b, sol, c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+    s_in = c->stage_b;
+  }
+  launch_pack(c->g, s_in, c->sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
+  int rc = run_cg_ref(c, false, f, eps, max_it, 0.0, info, st);
+  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  if (sol_dev) {
+    launch_unpack(c->g, c->sol, sol, false, false, false, st);
+  } else {
+    launch_unpack(c->g, c->sol, c->stage_b, false, false, false, st);
+    CK(cudaMemcpyAsync(sol, c->stage_b, c->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return rc;
+}
+
+int32_t pyomgpu_congrad_surf_press(pyomgpu_ctx* c, const double* forc, double* psi, double eps, int32_t max_it,
+                                   pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!c || !forc || !psi) return fail(PYOMGPU_EINVAL, "null argument");
+  if (!c->have_sp) return fail(PYOMGPU_ESTATE, "context has no surface-pressure operator (hu/hv/maskT_top)");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* f = nullptr;
+  if (int rc = stage_in(c, forc, c->stage_a, &f, st)) return rc;
+  const bool dev = is_device_ptr(psi);
+  const double* p_in = psi;
+  if (!dev) {
+    CK(cudaMemcpyAsync(c->stage_b, psi, c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+    p_in = c->stage_b;
+  }
+  launch_pack(c->g, p_in, c->sol, false, st);
+  int rc = run_cg_ref(c, true, f, eps, max_it, 0.0, info, st);
+  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  if (dev) {
+    launch_unpack(c->g, c->sol, psi, false, false, false, st);
+  } else {
+    launch_unpack(c->g, c->sol, c->stage_b, false, false, false, st);
+    CK(cudaMemcpyAsync(psi, c->stage_b, c->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return rc;
+}
+
+int32_t pyomgpu_solve_rtol(pyomgpu_ctx* c, const double* forc, double* sol, double rtol, int32_t precision,
+                           int32_t max_it, pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!c || !forc || !sol || !(rtol > 0)) return fail(PYOMGPU_EINVAL, "bad arguments");
+  if (precision != PYOMGPU_PREC_F64) return fail(PYOMGPU_EINVAL, "precision %d not available", precision);
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* f = nullptr;
+  if (int rc = stage_in(c, forc, c->stage_a, &f, st)) return rc;
+  const bool dev = is_device_ptr(sol);
+  const double* s_in = sol;
+  if (!dev) {
+    CK(cudaMemcpyAsync(c->stage_b, sol, c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+    s_in = c->stage_b;
+  }
+  launch_pack(c->g, s_in, c->sol, true, st);
+  pyomgpu_solve_info tmp{};
+  pyomgpu_solve_info* I = info ? info : &tmp;
+  int rc = run_cg_ref(c, false, f, 0.0, max_it, rtol, I, st);
+  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  launch_fill_cyclic(c->g, c->sol, st);  // the border exchange that follows a solve
+  launch_residual(c->g, c->sf.dev(), f, c->sol, c->part, 1024, c->scal, st);
+  CK(cudaMemcpyAsync(c->h_scal, c->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (dev) {
+    launch_unpack(c->g, c->sol, sol, false, false, false, st);
+  } else {
+    launch_unpack(c->g, c->sol, c->stage_b, false, false, false, st);
+    CK(cudaMemcpyAsync(sol, c->stage_b, c->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  const double rr = c->h_scal[0], bb = c->h_scal[1];
+  I->rel_residual = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+  return rc;
+}
+
+int32_t pyomgpu_apply_op(pyomgpu_ctx* c, int32_t op, const double* p, double* res, pyomgpu_stream stream) {
+  if (!c || !p || !res) return fail(PYOMGPU_EINVAL, "null argument");
+  if (op == PYOMGPU_OP_SURF_PRESS && !c->have_sp) return fail(PYOMGPU_ESTATE, "no surface-pressure operator");
+  if (op != PYOMGPU_OP_STREAMFUNCTION && op != PYOMGPU_OP_SURF_PRESS) return fail(PYOMGPU_EINVAL, "unknown operator");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* pin = nullptr;
+  if (int rc = stage_in(c, p, c->stage_a, &pin, st)) return rc;
+  const OpBuf& o = op == PYOMGPU_OP_SURF_PRESS ? c->sp : c->sf;
+  if (is_device_ptr(res)) {
+    launch_apply_op_user(c->g, o.dev(), pin, res, c->As, st);
+  } else {
+    launch_apply_op_user(c->g, o.dev(), pin, c->stage_b, c->As, st);
+    CK(cudaMemcpyAsync(res, c->stage_b, c->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_get_inv_diag(pyomgpu_ctx* c, double* Z, pyomgpu_stream stream) {
+  if (!c || !Z) return fail(PYOMGPU_EINVAL, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (is_device_ptr(Z)) {
+    launch_unpack(c->g, c->sf.W, Z, false, false, true, st);
+  } else {
+    launch_unpack(c->g, c->sf.W, c->stage_b, false, false, true, st);
+    CK(cudaMemcpyAsync(Z, c->stage_b, c->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_line_integral(pyomgpu_ctx* c, int32_t isle, const double* uloc, const double* vloc, double* line,
+                              pyomgpu_stream stream) {
+  if (!c || !uloc || !vloc || !line) return fail(PYOMGPU_EINVAL, "null argument");
+  if (!c->have_islands) return fail(PYOMGPU_ESTATE, "no islands set");
+  if (isle < 1 || isle > c->isl.nisle) return fail(PYOMGPU_EINVAL, "island %d out of range", isle);
+  cudaStream_t st = (cudaStream_t)stream;
+  const double *u = nullptr, *v = nullptr;
+  if (int rc = stage_in(c, uloc, c->stage_a, &u, st)) return rc;
+  if (int rc = stage_in(c, vloc, c->stage_b, &v, st)) return rc;
+  launch_line_integral_uv(c->nx, c->idev, line_geo(c), u, v, isle - 1, 1, c->scal, st);
+  CK(cudaMemcpyAsync(c->h_scal, c->scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *line = c->h_scal[0];
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_solve_streamfunction(pyomgpu_ctx* c, pyomgpu_state* s, pyomgpu_solve_info* info,
+                                     pyomgpu_stream stream) {
+  if (!c || !s) return fail(PYOMGPU_EINVAL, "null argument");
+  if (!state_ok(s)) return fail(PYOMGPU_EINVAL, "state arrays must be device pointers with valid time levels");
+  if (!c->have_islands) return fail(PYOMGPU_ESTATE, "islands not set up (streamfunction_init)");
+  const int nisle = c->isl.nisle;
+  if (nisle > 1 && (!c->have_psin || !c->have_line_psin)) return fail(PYOMGPU_ESTATE, "psin / line_psin missing");
+  if (nisle > 1 && !is_device_ptr(s->dpsin)) return fail(PYOMGPU_EINVAL, "dpsin must be a device pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  StepDev d = step_dev(c, s);
+  const size_t n2 = c->n2;
+  launch_hydrostatic(d, st);
+  launch_sf_forcing(d, c->fpx, c->fpy, c->forc, st);
+  double* dp1 = s->dpsi + (size_t)(s->taup1 - 1) * n2;
+  launch_first_guess(c->g, dp1, s->dpsi + (size_t)(s->tau - 1) * n2, s->dpsi + (size_t)(s->taum1 - 1) * n2, st);
+  launch_pack(c->g, dp1, c->sol, true, st);
+  pyomgpu_solve_info tmp{};
+  pyomgpu_solve_info* I = info ? info : &tmp;
+  int rc = run_cg_ref(c, false, c->forc, s->congr_epsilon, s->congr_max_iterations, 0.0, I, st);
+  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  s->congr_itts = I->iterations;
+  launch_unpack(c->g, c->sol, dp1, true, false, false, st);  // + border_exchg/setcyclic (:58-59)
+  if (nisle > 1) {
+    if (c->lu_singular) return fail(PYOMGPU_SINGULAR, "in solve_streamfunction, lapack info not zero");
+    LineGeo lg = line_geo(c);
+    launch_line_integral_uv(c->nx, c->idev, lg, c->fpx, c->fpy, 1, nisle - 1, c->line_forc, st);
+    launch_line_integral_psi(c->nx, c->ny, c->idev, lg, dp1, n2, 1, 1, nisle - 1, c->line_psi0, st);
+    launch_island_solve(nisle, c->lu, c->ipiv, c->line_forc, c->line_psi0, s->dpsin, s->tau, st);
+  }
+  launch_sf_psi_update(d, c->psin, nisle, s->dpsin, st);
+  launch_sf_velocity_update(d, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return rc;
+}
+
+int32_t pyomgpu_solve_pressure(pyomgpu_ctx* c, pyomgpu_state* s, pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!c || !s) return fail(PYOMGPU_EINVAL, "null argument");
+  if (!c->have_sp) return fail(PYOMGPU_ESTATE, "context has no surface-pressure operator");
+  if (!state_ok(s)) return fail(PYOMGPU_EINVAL, "state arrays must be device pointers with valid time levels");
+  cudaStream_t st = (cudaStream_t)stream;
+  StepDev d = step_dev(c, s);
+  const size_t n2 = c->n2;
+  launch_hydrostatic(d, st);
+  launch_sp_forcing(d, c->free_surface, c->fpx, c->fpy, c->forc, st);
+  double* ps1 = s->psi + (size_t)(s->taup1 - 1) * n2;
+  launch_first_guess(c->g, ps1, s->psi + (size_t)(s->tau - 1) * n2, s->psi + (size_t)(s->taum1 - 1) * n2, st);
+  launch_pack(c->g, ps1, c->sol, false, st);
+  pyomgpu_solve_info tmp{};
+  pyomgpu_solve_info* I = info ? info : &tmp;
+  int rc = run_cg_ref(c, true, c->forc, s->congr_epsilon, s->congr_max_iterations, 0.0, I, st);
+  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  s->congr_itts = I->iterations;
+  launch_unpack(c->g, c->sol, ps1, true, false, false, st);  // border_exchg/setcyclic (:71-72)
+  launch_sp_velocity_update(d, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return rc;
+}
+
+}  // extern "C"
