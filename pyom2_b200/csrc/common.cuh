@@ -106,8 +106,8 @@ __device__ __forceinline__ bool grid_sync(SyncCtl* ctl, unsigned nblocks, unsign
                                           unsigned long long timeout_ns, unsigned extra = 0) {
   __shared__ int s_ok;
   __syncthreads();
+  epoch += 1;  // every thread keeps the same count (slot parities derive from it)
   if (threadIdx.x == 0) {
-    epoch += 1;
     const unsigned long long target = epoch * (unsigned long long)nblocks + extra;
     red_release_add_u64(&ctl->arrive, 1ull);
     int ok = 1;

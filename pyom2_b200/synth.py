@@ -231,6 +231,17 @@ def clean_land_mask(land, cyclic_x, keep_islands=None, rng=None, max_passes=50):
     nx, ny = land.shape
     for _ in range(max_passes):
         changed = False
+        if cyclic_x:
+            # pyOM2's isleperim treats columns 0..nx+1 as one periodic row of
+            # nx+2 cells (island_module.f90:71-77,373-419), so land in column 1
+            # or nx that does not cross the seam gets a second label that the
+            # halo copy then erases (streamfct_init.f90:56-83 halts on it).
+            # Keep the two seam columns identical so seam land always crosses.
+            seam = land[0] | land[-1]
+            if (seam != land[0]).any() or (seam != land[-1]).any():
+                land[0] = seam
+                land[-1] = seam
+                changed = True
         ext = np.ones((nx, ny + 2), dtype=bool)           # closed N/S
         ext[:, 1:-1] = land
         if not cyclic_x:
