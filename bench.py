@@ -33,6 +33,9 @@ sys.path.insert(0, ROOT)
 METRIC = "ms/solve to FP64 rel. residual 1e-10: learned FCG vs plain PCG, 1 B200"
 RTOL = 1e-10
 BYTES_PER_POINT_ITER = {"f64": 72, "f32": 36}  # algorithmic bytes, plain PCG iteration
+# DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of this
+# workload (profiles/cg_ref_kernel_c1_1440x720.md), per iteration, keyed by kernel
+MEASURED_TRAFFIC_PER_ITER = {"cg_ref_kernel": (1.219541e9 + 2.498041e9) / 1760}
 CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
            "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -260,7 +263,9 @@ def main():
                    "iterations": it_med, "max_rel_residual": max(relres), "l2": "flushed (256 MiB write) per step",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind, "kernel": "cg_ref_kernel",
+                     "traffic": (MEASURED_TRAFFIC_PER_ITER["cg_ref_kernel"] * it_med
+                                 if args.precision == "f64" else None),
+                     "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "kernel": "cg_ref_kernel",
                      "kernel_ms": kern_med, "bytes_per_point_iter": BYTES_PER_POINT_ITER[args.precision]},
         "e2e": {"value": statistics.median(e2e), "unit": "ms/solve", "h2d_bytes_per_step": 2 * n2 * 8,
                 "d2h_bytes_per_step": n2 * 8},
