@@ -185,6 +185,31 @@ int32_t pyomgpu_congrad_streamfunction(pyomgpu_ctx* ctx, const double* forc, dou
                                        int32_t congr_max_iterations, pyomgpu_solve_info* info,
                                        pyomgpu_stream stream);
 
+/* Allocation-free congrad_streamfunction.  No counterpart in the reference
+ * (pyOM2 runs on the CPU and never meets this constraint).  For callers that
+ * cannot call cudaMalloc: a host program whose device memory is fully claimed
+ * by its own pool, code running where new device allocations are forbidden,
+ * or a time loop that must not allocate (an allocation can synchronise the
+ * device or fail under memory pressure mid-run).  It takes no context: the
+ * grid (every pointer in `grid` a DEVICE pointer; hur/hvr and the six 1-D
+ * metrics are read, the rest ignored), the island perimeter points bnd_i/bnd_j
+ * (device int32, Fortran indices, nbnd of them: make_inv_sfc's Dirichlet
+ * points), forc (device) and sol (device, in/out) are the only memory it
+ * touches besides a static device array of PYOMGPU_NOALLOC_SCRATCH_BYTES that
+ * the library reserves on every GPU that loads it, until the process exits.
+ * Grids whose operator and work vectors exceed that array (about 1.0e6
+ * padded points, e.g. 1000 x 1000) are rejected with PYOMGPU_EINVAL and a
+ * message.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call reuses the same array and clears what must start at zero; calls
+ * that overlap on the GPU (other streams or host threads) race on it.
+ * Results equal pyomgpu_congrad_streamfunction's on the same inputs. */
+#define PYOMGPU_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* grid, const int32_t* bnd_i, const int32_t* bnd_j,
+                                               int32_t nbnd, const double* forc, double* sol, double congr_epsilon,
+                                               int32_t congr_max_iterations, pyomgpu_solve_info* info,
+                                               pyomgpu_stream stream);
+
 /* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
  * products.  psi is psi(:,:,taup1), in/out, host or device. */
 int32_t pyomgpu_congrad_surf_press(pyomgpu_ctx* ctx, const double* forc, double* psi, double congr_epsilon,

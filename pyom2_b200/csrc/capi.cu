@@ -59,6 +59,11 @@ int dalloc(T** p, size_t n) {
 
 }  // namespace
 
+namespace pyomgpu {
+// lets other translation units of the library report through pyomgpu_last_error()
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace pyomgpu
+
 struct pyomgpu_ctx {
   int device = 0, nsm = 0;
   Geo g{};
