@@ -104,7 +104,9 @@ typedef struct pyomgpu_solve_info {
   int32_t outer_iterations; /* refinement sweeps (pyomgpu_solve_rtol F32) */
   double estimated_error;   /* the reference's estimated_error */
   double rel_residual;      /* FP64 ||b-Ax||/||b|| over the unknowns (solve_rtol only) */
-  double device_ms;         /* device time of the solve, CUDA events on the stream */
+  double device_ms;         /* device time of the CG kernel launch(es), CUDA events on the stream */
+  int32_t kernel_launches;  /* kernels the call launched (solve_rtol; 1 = the CG kernel elsewhere) */
+  int32_t pad_;
 } pyomgpu_solve_info;
 
 /* Model arrays of one time step (all DEVICE pointers, Fortran layout). */

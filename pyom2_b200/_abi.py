@@ -58,7 +58,8 @@ class Islands(C.Structure):
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("status", C.c_int32),
                 ("outer_iterations", C.c_int32), ("estimated_error", C.c_double),
-                ("rel_residual", C.c_double), ("device_ms", C.c_double)]
+                ("rel_residual", C.c_double), ("device_ms", C.c_double),
+                ("kernel_launches", C.c_int32), ("pad_", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -12,61 +12,65 @@
 // grid barriers that carry the reductions (the reference's global_sum /
 // global_max, parallel_mpi.f90:232-277):
 //
-//   sweep A: s_new = W1*res + (beta/beta_old)*s_old on the strip plus a one-cell
-//            halo (recomputed locally, so no extra barrier is needed before the
-//            stencil), As = A s_new; partials (s,As), max|s|
-//   sweep B: sol += alpha*s_new; res -= alpha*As; partial beta_next = (W1 res, res)
+//   sweep A: per tile, TMA loads of res, W, s_old, FX, FY (tile + halo) into
+//            shared memory; s_new = W1*res + (beta/beta_old)*s_old on the tile
+//            and its one-cell halo (recomputed locally, so no barrier is needed
+//            before the stencil); As = A s_new; partials (s,As), max|s|
+//   sweep B: per point, sol += alpha*s_new; res -= alpha*As; partial
+//            beta_next = (W1 res, res)
 //
 // The search direction is double-buffered (s_old is read by neighbouring
-// strips while s_new is written).  Cyclic halos are written by the owner of
-// the source point (setcyclic_xy, parallel_none.f90:188-211).
-//
-// Work decomposition: a warp owns a strip of 32 consecutive columns x R rows;
-// lane L owns column x0+1+L and walks the rows with a 3-row register window.
-// x-neighbours come from warp shuffles, the two columns outside the strip from
-// one extra predicated load per row.
+// tiles while s_new is written).  Cyclic halos are written by the owner of the
+// source point (setcyclic_xy, parallel_none.f90:188-211).
 #include <math.h>
 
 #include "cg_ref.cuh"
 
 namespace pyomgpu {
 
-constexpr unsigned kFull = 0xffffffffu;
-
-template <bool SP>
-__device__ __forceinline__ void strip_coords(const CGRefParams& P, int s, int& x0, int& y0, int& jend) {
-  const int sx = s % P.SX, sy = s / P.SX;
-  x0 = 32 * sx;
-  y0 = P.R * sy;
-  jend = min(y0 + P.R, P.g.ny);
+__device__ __forceinline__ void tile_origin(const CGRefParams& P, int t, int& i0, int& j0) {
+  i0 = 1 + kTileX * (t % P.ntx);
+  j0 = 1 + kTileY * (t / P.ntx);
 }
 
 template <bool SP>
-__global__ void __launch_bounds__(kCGThreads, 2) cg_ref_kernel(const CGRefParams P) {
+__global__ void __launch_bounds__(kCGThreads, 3) cg_ref_kernel(const __grid_constant__ CGRefParams P) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  double* tres = reinterpret_cast<double*>(smem);
+  double* tW = reinterpret_cast<double*>(smem + kTileBytes);
+  double* ts = reinterpret_cast<double*>(smem + 2 * kTileBytes);
+  double* tFX = reinterpret_cast<double*>(smem + 3 * kTileBytes);
+  double* tFY = reinterpret_cast<double*>(smem + 4 * kTileBytes);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 5 * kTileBytes);
+
   const Geo g = P.g;
   const OpDev<double> op = P.op;
-  const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * (kCGThreads / 32) + (threadIdx.x >> 5);
-  const int nwarps = gridDim.x * (kCGThreads / 32);
-  const int nstrips = P.SX * P.SY;
   const unsigned nb = gridDim.x;
+  const int ntiles = P.ntx * P.nty;
   unsigned long long epoch = 0;
+  uint32_t phase = 0;
   double* __restrict__ res = P.res;
   double* __restrict__ As = P.As;
   double* __restrict__ sol = P.sol;
   const double* __restrict__ Wf = op.W;
   const double F_1EM10 = (double)1.e-10f;  // solve_streamfct.f90:262, a default-real literal
 
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
   // ------------------------------------------------------------------ init
   // res = forc - A sol (interior), solve_streamfct.f90:196-201 / solve_pressure.f90:163-168
   {
     double v[4] = {0.0, 0.0, 0.0, 0.0};  // beta, bb, rr, zresmax
-    for (int s = gw; s < nstrips; s += nwarps) {
-      int x0, y0, jend;
-      strip_coords<SP>(P, s, x0, y0, jend);
-      const int i = x0 + 1 + lane;
-      if (i > g.nx) continue;
-      for (int j = y0 + 1; j <= jend; j++) {
+    for (int t = blockIdx.x; t < ntiles; t += nb) {
+      int i0, j0;
+      tile_origin(P, t, i0, j0);
+      for (int e = threadIdx.x; e < kTileX * kTileY; e += kCGThreads) {
+        const int i = i0 + e % kTileX, j = j0 + e / kTileX;
+        if (i > g.nx || j > g.ny) continue;
         const double f = P.forc[fidx(g.nx, i, j)];
         const double r = f - apply_point(op, g, sol, i, j);
         store_cyclic(res, g, i, j, r);
@@ -95,7 +99,7 @@ __global__ void __launch_bounds__(kCGThreads, 2) cg_ref_kernel(const CGRefParams
   }
   if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns, P.stall_extra)) return;
   double red[4];
-  grid_allreduce<4, 3>(P.slots, nb, red);
+  grid_collect<4, 3, kCGThreads>(P.slots, 4, nb, red);
   double beta = red[0];
   const double bb = red[1];
   double rr = red[2];
@@ -150,60 +154,56 @@ __global__ void __launch_bounds__(kCGThreads, 2) cg_ref_kernel(const CGRefParams
     }
     // -------------------------------------------------------------- sweep A
     {
-      const double* __restrict__ so = P.s[(n + 1) & 1];
       double* __restrict__ sn = P.s[n & 1];
+      const CUtensorMap* map_so = &P.map_s[(n + 1) & 1];
       double acc_dot = 0.0, acc_max = 0.0;
-      for (int s = gw; s < nstrips; s += nwarps) {
-        int x0, y0, jend;
-        strip_coords<SP>(P, s, x0, y0, jend);
-        const int i = x0 + 1 + lane;
-        const bool own = i <= g.nx;
-        const bool valid = i <= g.nx + 1;
-        const int ie = (lane == 0) ? x0 : x0 + 33;
-        const bool edge = (lane == 0) || (lane == 31 && x0 + 33 <= g.nx + 1);
-        const double axi = valid ? op.ax[i + 1] : 0.0;
-        auto dirv = [&](int ii, int jj) -> double {
-          const size_t q = g.at(ii, jj);
-          const double r = res[q];
-          const double w1 = SP ? 1.0 : Wf[q];
-          return w1 * r + bq * so[q];
-        };
-        double sm = valid ? dirv(i, y0) : 0.0;
-        double sc = valid ? dirv(i, y0 + 1) : 0.0;
-        double fys = valid ? op.FY[g.at(i, y0 + 1)] : 0.0;
-        for (int j = y0 + 1; j <= jend; j++) {
-          const double snx = valid ? dirv(i, j + 1) : 0.0;
-          const double sedge = edge ? dirv(ie, j) : 0.0;
-          const double fxw = valid ? op.FX[g.at(i, j)] : 0.0;
-          const double fxedge = (lane == 31 && edge) ? op.FX[g.at(x0 + 33, j)] : 0.0;
-          const double fyn = valid ? op.FY[g.at(i, j + 1)] : 0.0;
-          double sW = __shfl_up_sync(kFull, sc, 1);
-          double sE = __shfl_down_sync(kFull, sc, 1);
-          double fxe = __shfl_down_sync(kFull, fxw, 1);
-          if (lane == 0) sW = sedge;
-          if (lane == 31) {
-            sE = sedge;
-            fxe = fxedge;
+      for (int t = blockIdx.x; t < ntiles; t += nb) {
+        int i0, j0;
+        tile_origin(P, t, i0, j0);
+        __syncthreads();  // the previous tile's shared-memory reads are done
+        if (threadIdx.x == 0) {
+          fence_proxy_async_smem();
+          fence_proxy_async_global();
+          mbar_arrive_expect_tx(bar, 5u * kBoxX * kBoxY * 8u);
+          const int ex = i0 + 1, ey = j0;  // padded element column of Fortran i0-2, row of j0-1
+          tma_load_2d(tres, &P.map_res, ex, ey, bar);
+          tma_load_2d(tW, &P.map_W, ex, ey, bar);
+          tma_load_2d(ts, map_so, ex, ey, bar);
+          tma_load_2d(tFX, &P.map_FX, ex, ey, bar);
+          tma_load_2d(tFY, &P.map_FY, ex, ey, bar);
+        }
+        const bool ok = __syncthreads_and(mbar_wait_bounded(bar, phase, P.timeout_ns));
+        phase ^= 1u;
+        if (!ok) {
+          if (threadIdx.x == 0) atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+          return;
+        }
+        // direction on the tile and its one-cell halo: box columns 1..kBoxX-2, all rows
+        for (int e = threadIdx.x; e < (kBoxX - 2) * kBoxY; e += kCGThreads) {
+          const int k = (e / (kBoxX - 2)) * kBoxX + 1 + e % (kBoxX - 2);
+          const double w1 = SP ? 1.0 : tW[k];
+          ts[k] = w1 * tres[k] + bq * ts[k];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < kTileX * kTileY; e += kCGThreads) {
+          const int c = e % kTileX, r = e / kTileX;
+          const int i = i0 + c, j = j0 + r;
+          if (i > g.nx || j > g.ny) continue;
+          const int k = (r + 1) * kBoxX + c + 2;
+          const double sc = ts[k];
+          double a = op.ax[i + 1] * op.bx[j + 1] * (tFX[k + 1] * (ts[k + 1] - sc) + tFX[k] * (ts[k - 1] - sc)) +
+                     op.by[j + 1] * (tFY[k + kBoxX] * (ts[k + kBoxX] - sc) + tFY[k] * (ts[k - kBoxX] - sc));
+          const double w = tW[k];
+          if (SP) a += op.dcoef * w * sc;
+          store_cyclic(sn, g, i, j, sc);
+          As[g.at(i, j)] = a;
+          if (SP) {
+            acc_dot += sc * a * w;
+            acc_max = fmax(acc_max, fabs(sc * w));
+          } else {
+            acc_dot += sc * a;
+            acc_max = fmax(acc_max, fabs(sc));
           }
-          if (own) {
-            const double sxx = axi * op.bx[j + 1];
-            const double syy = op.by[j + 1];
-            double a = sxx * (fxe * (sE - sc) + fxw * (sW - sc)) + syy * (fyn * (snx - sc) + fys * (sm - sc));
-            const double w = Wf[g.at(i, j)];
-            if (SP) a += op.dcoef * w * sc;
-            store_cyclic(sn, g, i, j, sc);
-            As[g.at(i, j)] = a;
-            if (SP) {
-              acc_dot += sc * a * w;
-              acc_max = fmax(acc_max, fabs(sc * w));
-            } else {
-              acc_dot += sc * a;
-              acc_max = fmax(acc_max, fabs(sc));
-            }
-          }
-          sm = sc;
-          sc = snx;
-          fys = fyn;
         }
       }
       double v[2] = {acc_dot, acc_max}, out[2];
@@ -216,33 +216,13 @@ __global__ void __launch_bounds__(kCGThreads, 2) cg_ref_kernel(const CGRefParams
     }
     const unsigned long long ep_a = epoch;
     if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
-    double ra[4];
+    double sAs, smax;
     {
       double r2[2];
-      // slots written before this barrier live in parity (ep_a & 1)
-      const double* sl = P.slots + (size_t)((ep_a & 1) * nb) * 4;
-      __shared__ double shr[2];
-      if (threadIdx.x < 32) {
-        double d = 0.0, m = 0.0;
-        for (unsigned b = threadIdx.x; b < nb; b += 32) {
-          d += __ldcg(sl + (size_t)b * 4);
-          m = fmax(m, __ldcg(sl + (size_t)b * 4 + 1));
-        }
-        d = warp_sum(d);
-        m = warp_max(m);
-        if (threadIdx.x == 0) {
-          shr[0] = d;
-          shr[1] = m;
-        }
-      }
-      __syncthreads();
-      r2[0] = shr[0];
-      r2[1] = shr[1];
-      __syncthreads();
-      ra[0] = r2[0];
-      ra[1] = r2[1];
+      grid_collect<2, 1, kCGThreads>(P.slots + (size_t)((ep_a & 1) * nb) * 4, 4, nb, r2);
+      sAs = r2[0];
+      smax = r2[1];
     }
-    const double sAs = ra[0], smax = ra[1];
 
     bool stop_after = false;
     if (SP) {
@@ -304,12 +284,12 @@ __global__ void __launch_bounds__(kCGThreads, 2) cg_ref_kernel(const CGRefParams
     {
       const double* __restrict__ sn = P.s[n & 1];
       double acc_b = 0.0, acc_r = 0.0;
-      for (int s = gw; s < nstrips; s += nwarps) {
-        int x0, y0, jend;
-        strip_coords<SP>(P, s, x0, y0, jend);
-        const int i = x0 + 1 + lane;
-        if (i > g.nx) continue;
-        for (int j = y0 + 1; j <= jend; j++) {
+      for (int t = blockIdx.x; t < ntiles; t += nb) {
+        int i0, j0;
+        tile_origin(P, t, i0, j0);
+        for (int e = threadIdx.x; e < kTileX * kTileY; e += kCGThreads) {
+          const int i = i0 + e % kTileX, j = j0 + e / kTileX;
+          if (i > g.nx || j > g.ny) continue;
           const size_t q = g.at(i, j);
           const double sc = sn[q];
           const double w = Wf[q];
@@ -341,25 +321,10 @@ __global__ void __launch_bounds__(kCGThreads, 2) cg_ref_kernel(const CGRefParams
     if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
     double beta_next, rr_next;
     {
-      const double* sl = P.slots + (size_t)((ep_b & 1) * nb) * 4;
-      __shared__ double shb[2];
-      if (threadIdx.x < 32) {
-        double d = 0.0, m = 0.0;
-        for (unsigned b = threadIdx.x; b < nb; b += 32) {
-          d += __ldcg(sl + (size_t)b * 4);
-          m += __ldcg(sl + (size_t)b * 4 + 1);
-        }
-        d = warp_sum(d);
-        m = warp_sum(m);
-        if (threadIdx.x == 0) {
-          shb[0] = d;
-          shb[1] = m;
-        }
-      }
-      __syncthreads();
-      beta_next = shb[0];
-      rr_next = shb[1];
-      __syncthreads();
+      double r2[2];
+      grid_collect<2, -1, kCGThreads>(P.slots + (size_t)((ep_b & 1) * nb) * 4, 4, nb, r2);
+      beta_next = r2[0];
+      rr_next = r2[1];
     }
     if (SP) {
       const double rsnew = beta_next;
@@ -403,11 +368,36 @@ done:
   }
 }
 
-template __global__ void cg_ref_kernel<false>(const CGRefParams P);
-template __global__ void cg_ref_kernel<true>(const CGRefParams P);
+template __global__ void cg_ref_kernel<false>(const __grid_constant__ CGRefParams P);
+template __global__ void cg_ref_kernel<true>(const __grid_constant__ CGRefParams P);
 
 const void* cg_ref_kernel_ptr(bool sp) {
   return sp ? (const void*)cg_ref_kernel<true> : (const void*)cg_ref_kernel<false>;
+}
+
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return -1;
+    fn = (EncodeTiledFn)p;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)g.pitch, (cuuint64_t)(g.ny + 2 * kOnx)};
+  const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)kBoxX, (cuuint32_t)kBoxY};
+  const cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (int)r;
 }
 
 }  // namespace pyomgpu

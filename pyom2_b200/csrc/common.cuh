@@ -169,6 +169,42 @@ __device__ __forceinline__ void block_reduce(const double (&v)[NV], double (&out
   __syncthreads();
 }
 
+// After a grid_sync: every block combines all published partials
+// (slots[b*stride + k], b < nblocks) with every thread loading at most a few
+// slots at once (one L2 round trip), then a fixed-order block reduction, so all
+// blocks obtain the same values.  Slot kMaxSlot (if >= 0) is a max, the others
+// sums.  Result broadcast to every thread.
+template <int NV, int kMaxSlot, int kThreads>
+__device__ __forceinline__ void grid_collect(const double* __restrict__ slots, int stride, unsigned nblocks,
+                                             double (&out)[NV]) {
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = 0.0;
+  constexpr int kMaxPer = 4;  // nblocks <= 4 * kThreads
+#pragma unroll
+  for (int u = 0; u < kMaxPer; u++) {
+    const unsigned b = threadIdx.x + u * kThreads;
+    if (b < nblocks) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        const double x = __ldcg(slots + (size_t)b * stride + k);
+        v[k] = (k == kMaxSlot) ? fmax(v[k], x) : v[k] + x;
+      }
+    }
+  }
+  __shared__ double sh_out[NV];
+  double r[NV];
+  block_reduce<NV, kMaxSlot, kThreads>(v, r);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) sh_out[k] = r[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; k++) out[k] = sh_out[k];
+  __syncthreads();
+}
+
 // After a grid_sync: every block sums all published slots (layout
 // slots[block*NV + k]) in a fixed order; warp 0 does the work, the result is
 // broadcast through shared memory.

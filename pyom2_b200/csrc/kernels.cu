@@ -2,6 +2,8 @@
 // column-wise pre/post work of one external-mode step.
 #include <math.h>
 
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace pyomgpu {
@@ -481,6 +483,36 @@ __global__ void k_residual_final(const double* part, int nb, double* out) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// mixed precision: FP32 copies, scaled FP32 residual, FP64 correction
+// ---------------------------------------------------------------------------
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    b[t] = (float)a[t];
+}
+
+// b32 = s (forc - A x) at the unknowns (W != 0), 0 elsewhere; forc in Fortran layout
+__global__ void k_residual_f32(Geo g, OpDev<double> op, const double* __restrict__ forc_user,
+                               const double* __restrict__ x, double s, float* __restrict__ b32) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  int i, j;
+  if (!decode_full(g, t, i, j)) return;
+  float v = 0.f;
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && op.W[g.at(i, j)] != 0.0)
+    v = (float)(s * (forc_user[fidx(g.nx, i, j)] - apply_point(op, g, x, i, j)));
+  b32[g.at(i, j)] = v;
+}
+
+// x += c e over the interior
+__global__ void k_add_correction(Geo g, double* __restrict__ x, const float* __restrict__ e, double c) {
+  const size_t n = (size_t)g.nx * g.ny;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx) + 1, j = (int)(t / g.nx) + 1;
+    const size_t o = g.at(i, j);
+    x[o] = x[o] + c * (double)e[o];
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -520,6 +552,19 @@ void launch_unpack(const Geo& g, const double* padded, double* user, bool setcyc
 void launch_setcyclic_user(const Geo& g, double* user, cudaStream_t st) {
   if (g.cyclic_x) k_setcyclic_user_x<<<nblk(g.ny + 4, 128), 128, 0, st>>>(g.nx, g.ny, user);
   if (g.cyclic_y) k_setcyclic_user_y<<<nblk(g.nx + 4, 128), 128, 0, st>>>(g.nx, g.ny, user);
+}
+
+void launch_to_f32(const double* a, float* b, size_t n, cudaStream_t st) {
+  k_to_f32<<<std::min<size_t>(nblk(n, 256), 4096), 256, 0, st>>>(a, b, n);
+}
+
+void launch_residual_f32(const Geo& g, const OpDev<double>& op, const double* forc_user, const double* x, double s,
+                         float* b32, cudaStream_t st) {
+  k_residual_f32<<<nblk(full_count(g), 256), 256, 0, st>>>(g, op, forc_user, x, s, b32);
+}
+
+void launch_add_correction(const Geo& g, double* x, const float* e, double c, cudaStream_t st) {
+  k_add_correction<<<std::min<size_t>(nblk((size_t)g.nx * g.ny, 256), 4096), 256, 0, st>>>(g, x, e, c);
 }
 
 void launch_fill_cyclic(const Geo& g, double* a, cudaStream_t st) {

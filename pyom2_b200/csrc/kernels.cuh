@@ -69,6 +69,14 @@ void launch_island_solve(int nisle, const double* lu, const int* ipiv, const dou
 void launch_residual(const Geo& g, const OpDev<double>& op, const double* forc_user, const double* sol_padded,
                      double* part, int nb, double* out2, cudaStream_t st);
 
+// mixed precision helpers
+void launch_to_f32(const double* a, float* b, size_t n, cudaStream_t st);
+// b32 = s (forc - A x) at the unknowns (W != 0), zero elsewhere (x padded with valid halo)
+void launch_residual_f32(const Geo& g, const OpDev<double>& op, const double* forc_user, const double* x, double s,
+                         float* b32, cudaStream_t st);
+// x += c e over the interior
+void launch_add_correction(const Geo& g, double* x, const float* e, double c, cudaStream_t st);
+
 // ---- solve_streamfunction / solve_pressure pre and post ----------------------
 struct StepDev {
   int nx, ny, nz, cyclic_x, cyclic_y;

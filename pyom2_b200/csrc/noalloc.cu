@@ -129,8 +129,10 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
   // launch shape: the same rule as the context path, so results match it bit for bit
   int dev = 0, nsm = 0, o1 = 0, o2 = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, cg_ref_kernel_ptr(false), kCGThreads, 0) ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, cg_ref_kernel_ptr(true), kCGThreads, 0) || o1 < 1)
+      cudaFuncSetAttribute(cg_ref_kernel_ptr(false), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmem) ||
+      cudaFuncSetAttribute(cg_ref_kernel_ptr(true), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmem) ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, cg_ref_kernel_ptr(false), kCGThreads, kCGSmem) ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, cg_ref_kernel_ptr(true), kCGThreads, kCGSmem) || o1 < 1)
     return nfail(PYOMGPU_ECUDA, "device query failed");
   const int max_blocks = std::min(o1, std::max(1, o2)) * nsm;
 
@@ -175,13 +177,14 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
   launch_pack(g, sol, spad, true, st);
 
   // the same persistent kernel as pyomgpu_congrad_streamfunction
-  const int SX = (g.nx + 31) / 32;
-  const int maxwarps = max_blocks * (kCGThreads / 32);
-  int R = (SX * g.ny + maxwarps - 1) / std::max(1, maxwarps);
-  R = std::max(4, std::min(R, 256));
-  const int SY = (g.ny + R - 1) / R;
-  const int grid = std::max(1, std::min(max_blocks, (SX * SY + (kCGThreads / 32) - 1) / (kCGThreads / 32)));
   CGRefParams Pm{};
+  if (encode_tile_map(&Pm.map_res, res, g) || encode_tile_map(&Pm.map_W, op.W, g) ||
+      encode_tile_map(&Pm.map_FX, op.FX, g) || encode_tile_map(&Pm.map_FY, op.FY, g) ||
+      encode_tile_map(&Pm.map_s[0], s0, g) || encode_tile_map(&Pm.map_s[1], s1, g))
+    return nfail(PYOMGPU_ECUDA, "cuTensorMapEncodeTiled failed");
+  Pm.ntx = (g.nx + kTileX - 1) / kTileX;
+  Pm.nty = (g.ny + kTileY - 1) / kTileY;
+  const int grid = std::max(1, std::min(max_blocks, Pm.ntx * Pm.nty));
   Pm.g = g;
   Pm.op = op.dev();
   Pm.forc = forc;
@@ -193,16 +196,13 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
   Pm.eps = congr_epsilon;
   Pm.max_it = congr_max_iterations;
   Pm.rtol = 0.0;
-  Pm.R = R;
-  Pm.SX = SX;
-  Pm.SY = SY;
   Pm.ctl = ctl;
   Pm.slots = slots;
   Pm.timeout_ns = 2000000000ull;
   Pm.stall_extra = 0;
   Pm.out = result;
   void* args[] = {&Pm};
-  e = cudaLaunchCooperativeKernel(cg_ref_kernel_ptr(false), dim3(grid), dim3(kCGThreads), args, 0, st);
+  e = cudaLaunchCooperativeKernel(cg_ref_kernel_ptr(false), dim3(grid), dim3(kCGThreads), args, kCGSmem, st);
   if (e != cudaSuccess) return nfail(PYOMGPU_ECUDA, "cg launch: %s", cudaGetErrorString(e));
   launch_unpack(g, spad, sol, false, false, false, st);
   CGResult h{};
@@ -220,6 +220,7 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
     info->estimated_error = h.est;
     info->rel_residual = -1.0;
     info->device_ms = -1.0;
+    info->kernel_launches = 8;  // build x2, inverse x2-3, pack, cg, unpack
   }
   if (hc.error) return nfail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded 2 s");
   return h.status;

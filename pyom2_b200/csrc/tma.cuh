@@ -1,0 +1,70 @@
+// TMA (cp.async.bulk.tensor) tile loads into shared memory with an mbarrier,
+// for the stencil sweeps.  Loads only, from this GPU's own memory, no cluster
+// multicast.  Every wait on the mbarrier is bounded by %globaltimer.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace pyomgpu {
+
+// Fortran (i,j) tile geometry of the stencil sweeps: a tile is kTileX interior
+// columns by kTileY interior rows; its shared-memory box covers Fortran
+// columns i0-2 .. i0+kTileX+1 (kBoxX = kTileX+4, so the box starts on a
+// 16-byte boundary of the padded layout) and rows j0-1 .. j0+kTileY.
+constexpr int kTileX = 64;
+constexpr int kTileY = 16;
+constexpr int kBoxX = kTileX + 4;
+constexpr int kBoxY = kTileY + 2;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// order this thread's generic-proxy shared-memory accesses before later async-proxy (TMA) writes
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// make global-memory data this thread observes through the generic proxy (e.g.
+// other blocks' stores, acquired at a grid barrier) visible to its later TMA reads
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Waits for the mbarrier phase; false after timeout_ns (the caller records
+// PYOMGPU_TIMEOUT and leaves the kernel once the in-flight copies are done).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned long long timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (globaltimer_ns() - t0 > timeout_ns) return false;
+  return true;
+}
+
+// Host: tensor map of a padded FP64 field ((ny+4) rows of `pitch` elements)
+// with a kBoxX x kBoxY box.  Returns 0 or a CUDA driver error code.
+int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g);
+
+}  // namespace pyomgpu

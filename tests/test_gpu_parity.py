@@ -237,11 +237,12 @@ def test_solve_pressure_step(oracle_lib, name, free_surface):
 
 
 @pytest.mark.parametrize("name", list(WORLDS))
-def test_solve_rtol_reaches_1e10(oracle_lib, name):
+@pytest.mark.parametrize("precision", [_abi.PREC_F64, _abi.PREC_F32])
+def test_solve_rtol_reaches_1e10(oracle_lib, name, precision):
     W, Mg, Mo, O, E, _ = setup(name, oracle_lib)
     sol = np.zeros(Mg.shape2d, order="F")
-    info = E.solve_rtol(W.forc, sol, rtol=1e-10)
-    assert info["status"] == 0 and info["rel_residual"] <= 1e-10
+    info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=precision)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
     cf = O.make_coeff_streamfunction()
     Z = O.make_inv_sfc(cf)
     assert O.rel_residual(cf, Z, W.forc, sol) <= 1.5e-10
