@@ -157,7 +157,7 @@ def run_reference(args, rank, world):
 
 METHODS = {
     # name: (precision code, dtype label, algorithmic bytes key, dominant kernel)
-    "pcg64": ("PREC_F64", "f64", "f64", "cg_pipe_kernel<double>"),
+    "pcg64": ("PREC_F64", "f64", "f64", "cg_ref_kernel<false>"),
     "mixed32": ("PREC_F32", "f32+f64", "f32", "cg_pipe_kernel<float>"),
 }
 

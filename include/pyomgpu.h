@@ -212,6 +212,25 @@ int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* grid, const i
                                                int32_t congr_max_iterations, pyomgpu_solve_info* info,
                                                pyomgpu_stream stream);
 
+/* `count` congrad_streamfunction solves in ONE launch of a persistent
+ * work-queue kernel.  Replaces the reference's one-after-another calls of
+ * congrad_streamfunction (the psin loop, streamfct_init.f90:272-287, or a loop
+ * over independent grids).  Solve k runs on ctx[k]'s grid and operator;
+ * contexts may repeat (several right-hand sides on one grid) but must live on
+ * one device.  forc[k] (read; forc or forc[k] NULL = zero forcing) and sol[k]
+ * (in/out) are Fortran-layout, host or device.  Every solve keeps its own
+ * scalars and follows congrad_streamfunction's control flow, so its
+ * iterations, status and estimated_error are those of a separate call (dot
+ * products are summed in another order).  rtol > 0 adds the stop of
+ * pyomgpu_solve_rtol on the recursively updated residual and fills each
+ * info's rel_residual with the FP64 true residual; congr_epsilon = 0 leaves
+ * rtol as the only stop.  info: count entries or NULL; device_ms and
+ * kernel_launches describe the whole call.  The work buffers live in ctx[0]
+ * and grow to the largest batch it has run.  Returns the largest status. */
+int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t count, const double* const* forc,
+                                             double* const* sol, double congr_epsilon, int32_t congr_max_iterations,
+                                             double rtol, pyomgpu_solve_info* info, pyomgpu_stream stream);
+
 /* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
  * products.  psi is psi(:,:,taup1), in/out, host or device. */
 int32_t pyomgpu_congrad_surf_press(pyomgpu_ctx* ctx, const double* forc, double* psi, double congr_epsilon,

@@ -29,6 +29,7 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_island_boundaries", "pyomgpu_streamfunction_init",
            "pyomgpu_island_sizes", "pyomgpu_get_islands", "pyomgpu_set_islands",
            "pyomgpu_congrad_streamfunction", "pyomgpu_congrad_streamfunction_noalloc",
+           "pyomgpu_congrad_streamfunction_batch",
            "pyomgpu_congrad_surf_press", "pyomgpu_solve_rtol",
            "pyomgpu_apply_op", "pyomgpu_get_inv_diag", "pyomgpu_line_integral",
            "pyomgpu_solve_streamfunction", "pyomgpu_solve_pressure")
@@ -104,6 +105,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_set_islands": (i32, [vp, P(Islands), vp, vp, vp]),
         "pyomgpu_congrad_streamfunction": (i32, [vp, vp, vp, d, i32, P(SolveInfo), vp]),
         "pyomgpu_congrad_streamfunction_noalloc": (i32, [P(Grid), vp, vp, i32, vp, vp, d, i32, P(SolveInfo), vp]),
+        "pyomgpu_congrad_streamfunction_batch": (i32, [P(vp), i32, P(vp), P(vp), d, i32, d, P(SolveInfo), vp]),
         "pyomgpu_congrad_surf_press": (i32, [vp, vp, vp, d, i32, P(SolveInfo), vp]),
         "pyomgpu_solve_rtol": (i32, [vp, vp, vp, d, i32, i32, P(SolveInfo), vp]),
         "pyomgpu_apply_op": (i32, [vp, i32, vp, vp, vp]),

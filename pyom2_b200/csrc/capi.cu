@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/pyomgpu.h"
+#include "cg_batch.cuh"
 #include "cg_pipe.cuh"
 #include "cg_ref.cuh"
 #include "common.cuh"
@@ -120,10 +121,34 @@ struct pyomgpu_ctx {
     std::vector<void*> owned;
   } fast;
 
+  // work-queue batch (pyomgpu_congrad_streamfunction_batch and the psin
+  // solves); grows to the largest batch run through this context
+  struct Batch {
+    int max_blocks = 0;
+    double* pool = nullptr;  // per solve: padded sol, res, s0, s1, As + Fortran staging of forc, sol
+    size_t cap = 0;          // doubles
+    BatchProblem* d_probs = nullptr;
+    BatchProblem* h_probs = nullptr;  // pinned
+    BatchState* d_state = nullptr;
+    BatchState* h_state = nullptr;    // pinned
+    int cap_probs = 0;
+    double* part = nullptr;  // 4 per task
+    size_t cap_tasks = 0;
+    double* d_rr = nullptr;  // 2 per solve: true residual, forcing norm
+    double* h_rr = nullptr;  // pinned
+    unsigned long long* sync = nullptr;  // SyncCtl, gen, any_active
+  } batch;
+
   ~pyomgpu_ctx() {
     for (void* p : fast.owned)
       if (p) cudaFree(p);
     if (fast.h_res) cudaFreeHost(fast.h_res);
+    for (void* p : {(void*)batch.pool, (void*)batch.d_probs, (void*)batch.d_state, (void*)batch.part,
+                    (void*)batch.d_rr, (void*)batch.sync})
+      if (p) cudaFree(p);
+    if (batch.h_probs) cudaFreeHost(batch.h_probs);
+    if (batch.h_state) cudaFreeHost(batch.h_state);
+    if (batch.h_rr) cudaFreeHost(batch.h_rr);
     void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
                     sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,
                     res, s0, s1, As, sol, stage_a, stage_b, fpx, fpy, forc, zeros, part, scal, ctl, slots, d_result,
@@ -326,6 +351,168 @@ int run_pipe(pyomgpu_ctx* c, const OpDev<T>& op, const T* b, T* x, T* const r[2]
   return 0;
 }
 
+// One solve of a batch: its grid/operator context and its device Fortran-layout
+// forcing (NULL = zero) and solution (in/out).
+struct BatchSpec {
+  pyomgpu_ctx* c;
+  const double* forc;
+  double* sol;
+};
+
+inline size_t align32(size_t n) { return (n + 31) / 32 * 32; }
+
+// Grows the owner's batch workspace for `count` solves needing `pool` doubles and `tasks` tiles.
+int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
+  auto& B = o->batch;
+  if (!B.sync) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_batch_kernel_ptr(), kBatchThreads, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+      return fail(PYOMGPU_ECUDA, "occupancy query of the batch kernel failed");
+    B.max_blocks = per_sm * o->nsm;
+    if (int rc = dalloc(&B.sync, 8)) return rc;
+  }
+  if (pool > B.cap) {
+    if (B.pool) cudaFree(B.pool);
+    B.pool = nullptr;
+    B.cap = 0;
+    if (int rc = dalloc(&B.pool, pool)) return rc;
+    B.cap = pool;
+  }
+  if (count > B.cap_probs) {
+    if (B.d_probs) cudaFree(B.d_probs);
+    if (B.h_probs) cudaFreeHost(B.h_probs);
+    if (B.d_state) cudaFree(B.d_state);
+    if (B.h_state) cudaFreeHost(B.h_state);
+    if (B.d_rr) cudaFree(B.d_rr);
+    if (B.h_rr) cudaFreeHost(B.h_rr);
+    B.d_probs = nullptr;
+    B.h_probs = nullptr;
+    B.d_state = nullptr;
+    B.h_state = nullptr;
+    B.d_rr = B.h_rr = nullptr;
+    B.cap_probs = 0;
+    if (int rc = dalloc(&B.d_probs, (size_t)count)) return rc;
+    if (int rc = dalloc(&B.d_state, (size_t)count)) return rc;
+    if (int rc = dalloc(&B.d_rr, (size_t)count * 2)) return rc;
+    if (cudaMallocHost((void**)&B.h_probs, sizeof(BatchProblem) * count) != cudaSuccess ||
+        cudaMallocHost((void**)&B.h_state, sizeof(BatchState) * count) != cudaSuccess ||
+        cudaMallocHost((void**)&B.h_rr, sizeof(double) * 2 * count) != cudaSuccess)
+      return fail(PYOMGPU_ENOMEM, "cudaMallocHost");
+    B.cap_probs = count;
+  }
+  if (tasks > B.cap_tasks) {
+    if (B.part) cudaFree(B.part);
+    B.part = nullptr;
+    B.cap_tasks = 0;
+    if (int rc = dalloc(&B.part, tasks * 4)) return rc;
+    B.cap_tasks = tasks;
+  }
+  return 0;
+}
+
+// Runs the solves of `v` in one launch of the work-queue kernel with the
+// workspace of `o`.  infos (v.size() entries) get each solve's result; with
+// want_res the FP64 true relative residual of each solution as well.
+int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol, bool want_res,
+              pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st) {
+  const int count = (int)v.size();
+  size_t pool = 0, tasks = 0;
+  for (const BatchSpec& b : v) {
+    pool += 5 * align32(b.c->g.size());
+    tasks += (size_t)((b.c->nx + kTileX - 1) / kTileX) * ((b.c->ny + kTileY - 1) / kTileY);
+  }
+  if (tasks > (size_t)0x7fffffff) return fail(PYOMGPU_EINVAL, "batch too large");
+  if (int rc = batch_reserve(o, count, pool, tasks)) return rc;
+  auto& B = o->batch;
+  CK(cudaMemsetAsync(B.pool, 0, pool * sizeof(double), st));
+  CK(cudaMemsetAsync(B.sync, 0, 8 * sizeof(unsigned long long), st));
+  double* cur = B.pool;
+  int tile0 = 0;
+  for (int k = 0; k < count; ++k) {
+    const BatchSpec& b = v[k];
+    const size_t P = align32(b.c->g.size());
+    BatchProblem pr{};
+    pr.g = b.c->g;
+    pr.op = b.c->sf.dev();
+    pr.forc = b.forc ? b.forc : b.c->zeros;
+    pr.sol = cur;
+    pr.res = cur + P;
+    pr.s[0] = cur + 2 * P;
+    pr.s[1] = cur + 3 * P;
+    pr.As = cur + 4 * P;
+    cur += 5 * P;
+    pr.eps = eps;
+    pr.rtol = rtol;
+    pr.max_it = max_it;
+    pr.ntx = (b.c->nx + kTileX - 1) / kTileX;
+    pr.nty = (b.c->ny + kTileY - 1) / kTileY;
+    pr.tile0 = tile0;
+    tile0 += pr.ntx * pr.nty;
+    B.h_probs[k] = pr;
+    launch_pack(b.c->g, b.sol, pr.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
+  }
+  CK(cudaMemcpyAsync(B.d_probs, B.h_probs, sizeof(BatchProblem) * count, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(B.d_state, 0, sizeof(BatchState) * count, st));
+  BatchParams P{};
+  P.probs = B.d_probs;
+  P.state = B.d_state;
+  P.nprob = count;
+  P.ntasks = tile0;
+  P.part = B.part;
+  P.ctl = reinterpret_cast<SyncCtl*>(B.sync);
+  P.gen = B.sync + 2;
+  P.any_active = reinterpret_cast<int*>(B.sync + 3);
+  P.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
+  P.stall_extra = o->stall_next;
+  o->stall_next = 0;
+  const int grid = std::max(1, std::min(B.max_blocks, tile0));
+  CK(cudaEventRecord(o->e0, st));
+  CK(launch_cg_batch(P, grid, st));
+  CK(cudaEventRecord(o->e1, st));
+  CK(cudaMemcpyAsync(B.h_state, B.d_state, sizeof(BatchState) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(o->h_scal, &P.ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  for (int k = 0; k < count; ++k) {
+    const BatchProblem& pr = B.h_probs[k];
+    if (want_res) {
+      launch_fill_cyclic(pr.g, pr.sol, st);
+      launch_residual(pr.g, pr.op, pr.forc, pr.sol, v[k].c->part, 1024, B.d_rr + 2 * k, st);
+    }
+    launch_unpack(pr.g, pr.sol, v[k].sol, false, false, false, st);
+  }
+  if (want_res) CK(cudaMemcpyAsync(B.h_rr, B.d_rr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  int err = 0;
+  std::memcpy(&err, o->h_scal, sizeof(int));
+  if (err) return fail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded %.3f s", o->timeout_s);
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, o->e0, o->e1));
+  if (ms_out) *ms_out = ms;
+  int worst = PYOMGPU_OK;
+  for (int k = 0; k < count; ++k) {
+    const BatchState& S = B.h_state[k];
+    worst = std::max(worst, S.status);
+    if (!infos) continue;
+    pyomgpu_solve_info& I = infos[k];
+    I.iterations = S.n;
+    I.converged = S.converged;
+    I.status = S.status;
+    I.outer_iterations = 1;
+    I.estimated_error = S.est;
+    I.device_ms = ms;
+    I.kernel_launches = 1;
+    if (want_res) {
+      const double rr = B.h_rr[2 * k], bb = B.h_rr[2 * k + 1];
+      I.rel_residual = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+    } else {
+      I.rel_residual = -1.0;
+    }
+  }
+  return worst;
+}
+
 int rebuild_islands(pyomgpu_ctx* c) {
   // Z of make_inv_sfc and the segment lists of line_integral from c->isl.
   const IslandSet& I = c->isl;
@@ -428,6 +615,7 @@ int psin_and_line_psin(pyomgpu_ctx* c, double eps, int max_it, cudaStream_t st) 
   int worst = 0;
   std::vector<double> init(c->n2);
   const IslandSet& I = c->isl;
+  // psin(:,:,isle) = 1 on the island's perimeter, 0 elsewhere (streamfct_init.f90:274-280)
   for (int isle = 1; isle <= nisle; ++isle) {
     std::fill(init.begin(), init.end(), 0.0);
     for (int n = 1; n <= I.nr_boundary[isle - 1]; ++n) {
@@ -435,17 +623,27 @@ int psin_and_line_psin(pyomgpu_ctx* c, double eps, int max_it, cudaStream_t st) 
       const int i = I.boundary[o], j = I.boundary[o + (size_t)nisle * I.max_boundary];
       if (i >= -1 && i <= c->nx + 2 && j >= -1 && j <= c->ny + 2) init[fidx(c->nx, i, j)] = 1.0;
     }
-    double* dst = c->psin + (size_t)(isle - 1) * c->n2;
-    CK(cudaMemcpyAsync(c->stage_b, init.data(), c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
-    launch_pack(c->g, c->stage_b, c->sol, true, st);
-    pyomgpu_solve_info info{};
-    int rc = run_cg_ref(c, false, c->zeros, eps, max_it, 0.0, &info, st);
-    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
-    if (info.status == PYOMGPU_NAN) return fail(PYOMGPU_NAN, "psin solve of island %d: estimated error is NaN", isle);
-    worst = std::max(worst, info.status);
-    c->psin_iters[isle - 1] = info.iterations;
-    launch_unpack(c->g, c->sol, dst, true, false, false, st);
+    CK(cudaMemcpyAsync(c->psin + (size_t)(isle - 1) * c->n2, init.data(), c->n2 * sizeof(double),
+                       cudaMemcpyHostToDevice, st));
   }
+  // all islands' solves (zero forcing) in one work-queue launch per chunk of at most 4 GiB of work vectors
+  const size_t per = 5 * align32(c->g.size());
+  const int chunk = (int)std::max<size_t>(1, ((size_t)1 << 29) / per);
+  for (int k0 = 0; k0 < nisle; k0 += chunk) {
+    const int k1 = std::min(nisle, k0 + chunk);
+    std::vector<BatchSpec> v;
+    for (int k = k0; k < k1; ++k) v.push_back(BatchSpec{c, nullptr, c->psin + (size_t)k * c->n2});
+    std::vector<pyomgpu_solve_info> infos(v.size());
+    int rc = run_batch(c, v, eps, max_it, 0.0, false, infos.data(), nullptr, st);
+    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    for (int k = k0; k < k1; ++k) {
+      const pyomgpu_solve_info& info = infos[k - k0];
+      if (info.status == PYOMGPU_NAN) return fail(PYOMGPU_NAN, "psin solve of island %d: estimated error is NaN", k + 1);
+      worst = std::max(worst, info.status);
+      c->psin_iters[k] = info.iterations;
+    }
+  }
+  for (int k = 0; k < nisle; ++k) launch_setcyclic_user(c->g, c->psin + (size_t)k * c->n2, st);
   CK(cudaGetLastError());
   c->have_psin = true;
   // line_psin(n, isle) = line integral around island n of the velocity of psin(:,:,isle)
@@ -791,6 +989,64 @@ int32_t pyomgpu_congrad_streamfunction(pyomgpu_ctx* c, const double* forc, doubl
   return rc;
 }
 
+int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t count, const double* const* forc,
+                                             double* const* sol, double eps, int32_t max_it, double rtol,
+                                             pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!ctx || count < 1 || !sol) return fail(PYOMGPU_EINVAL, "bad batch arguments");
+  if (!(rtol >= 0.0)) return fail(PYOMGPU_EINVAL, "rtol must be >= 0");
+  for (int k = 0; k < count; ++k) {
+    if (!ctx[k] || !sol[k]) return fail(PYOMGPU_EINVAL, "null context or solution in batch entry %d", k);
+    if (ctx[k]->device != ctx[0]->device) return fail(PYOMGPU_EINVAL, "batch contexts on different devices");
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  pyomgpu_ctx* o = ctx[0];
+  // host arrays are staged in the tail of the owner's pool, after the solve buffers
+  size_t work = 0, stage = 0;
+  std::vector<char> f_host(count), s_host(count);
+  for (int k = 0; k < count; ++k) {
+    work += 5 * align32(ctx[k]->g.size());
+    f_host[k] = forc && forc[k] && !is_device_ptr(forc[k]);
+    s_host[k] = !is_device_ptr(sol[k]);
+    stage += (f_host[k] + s_host[k]) * align32(ctx[k]->n2);
+  }
+  size_t tasks = 0;
+  for (int k = 0; k < count; ++k)
+    tasks += (size_t)((ctx[k]->nx + kTileX - 1) / kTileX) * ((ctx[k]->ny + kTileY - 1) / kTileY);
+  if (int rc = batch_reserve(o, count, work + stage, tasks)) return rc;
+  std::vector<BatchSpec> v(count);
+  double* cur = o->batch.pool + work;
+  for (int k = 0; k < count; ++k) {
+    pyomgpu_ctx* c = ctx[k];
+    v[k].c = c;
+    v[k].forc = forc ? forc[k] : nullptr;
+    v[k].sol = sol[k];
+    if (f_host[k]) {
+      CK(cudaMemcpyAsync(cur, forc[k], c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+      v[k].forc = cur;
+      cur += align32(c->n2);
+    }
+    if (s_host[k]) {
+      CK(cudaMemcpyAsync(cur, sol[k], c->n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+      v[k].sol = cur;
+      cur += align32(c->n2);
+    }
+  }
+  std::vector<pyomgpu_solve_info> tmp;
+  if (!info) {
+    tmp.resize(count);
+    info = tmp.data();
+  }
+  int rc = run_batch(o, v, eps, max_it, rtol, rtol > 0.0, info, nullptr, st);
+  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  for (int k = 0; k < count; ++k) {
+    if (s_host[k]) CK(cudaMemcpyAsync(sol[k], v[k].sol, ctx[k]->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // the whole call: the work-queue kernel, pack + unpack per solve (+ halo fill and 2-pass residual)
+    info[k].kernel_launches = 1 + count * (rtol > 0.0 ? 5 : 2);
+  }
+  CK(cudaStreamSynchronize(st));
+  return rc;
+}
+
 int32_t pyomgpu_congrad_surf_press(pyomgpu_ctx* c, const double* forc, double* psi, double eps, int32_t max_it,
                                    pyomgpu_solve_info* info, pyomgpu_stream stream) {
   if (!c || !forc || !psi) return fail(PYOMGPU_EINVAL, "null argument");
@@ -843,39 +1099,11 @@ int32_t pyomgpu_solve_rtol(pyomgpu_ctx* c, const double* forc, double* sol, doub
   I->device_ms = 0.0;
   I->estimated_error = 0.0;
   if (!f32) {
-    // FP64 Jacobi-PCG, pipelined (one sweep and one barrier per iteration).  The
-    // stop uses the recursive residual; the FP64 true residual is checked after
-    // the launch and the solve restarts from x if the two have drifted apart.
-    launch_pack(c->g, f, F.b, false, st);
-    I->kernel_launches = 2;  // pack sol, pack forc
-    rc = PYOMGPU_MAXITER;
-    for (int restart = 0; restart < 4; ++restart) {
-      PipeResult R{};
-      float ms = 0.f;
-      if (int e = run_pipe<double>(c, c->sf.dev(), F.b, c->sol, F.r, F.q, F.w, rtol,
-                                   std::max(1, max_it - I->iterations), &R, &ms, st))
-        return e;
-      I->iterations += R.iterations;
-      I->outer_iterations += 1;
-      I->device_ms += ms;
-      I->kernel_launches += 4;  // cg_pipe, fill_cyclic, residual x2
-      if (R.status == PYOMGPU_NAN) {
-        rc = PYOMGPU_NAN;
-        break;
-      }
-      launch_fill_cyclic(c->g, c->sol, st);
-      launch_residual(c->g, c->sf.dev(), f, c->sol, c->part, 1024, c->scal, st);
-      CK(cudaMemcpyAsync(c->h_scal, c->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      if (c->h_scal[0] <= rtol * rtol * c->h_scal[1]) {
-        rc = PYOMGPU_OK;
-        break;
-      }
-      if (R.status == PYOMGPU_MAXITER || I->iterations >= max_it) break;
-    }
-    I->status = rc;
-    I->kernel_launches += 1;  // unpack (the final check below re-runs fill + residual: +3)
-    I->kernel_launches += 3;
+    // FP64 Jacobi-PCG: the reference algorithm (two-barrier tile kernel) with
+    // the residual stop
+    rc = run_cg_ref(c, false, f, 0.0, max_it, rtol, I, st);
+    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    I->kernel_launches = 6;  // pack, cg_ref, fill_cyclic, residual x2, unpack
   } else {
     I->kernel_launches = 5;  // pack, final fill_cyclic + residual x2, unpack (+6 per refinement below)
     // FP32 PCG (FP64 products) for the correction, FP64 true residual outside

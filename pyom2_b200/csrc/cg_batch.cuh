@@ -1,0 +1,53 @@
+// Persistent work-queue kernel: many independent congrad_streamfunction solves
+// (the island right-hand sides of streamfunction_init, or unevenly sized grids)
+// in one launch (cg_batch.cu).
+#pragma once
+#include "common.cuh"
+#include "ops.cuh"
+
+namespace pyomgpu {
+
+constexpr int kBatchThreads = 256;
+
+// One solve: grid, operator and work buffers (constant during a launch).
+struct BatchProblem {
+  Geo g;
+  OpDev<double> op;    // FX, FY, ax, bx, by, W = Z
+  const double* forc;  // Fortran layout (ld nx+4)
+  double* sol;         // padded, halo set (setcyclic) on entry
+  double* res;         // padded work buffers, zero on entry
+  double* s[2];
+  double* As;
+  double eps;
+  double rtol;         // > 0: extra stop on ||res|| / ||forc|| over the unknowns
+  int max_it;
+  int tile0, ntx, nty; // first task index, tiles in x and y
+};
+
+// Scalars of one solve, advanced only by the block that reduces at a grid
+// barrier and read by all blocks through L2 (11 x 8 bytes).
+struct BatchState {
+  int n, phase;  // iteration; phase: 0 done, 1 sweep A next, 2 sweep B next
+  int status, converged, stop_after, pad;
+  double beta, betam1, betamin, step1, est, bq, alpha, bb;
+};
+static_assert(sizeof(BatchState) == 88, "BatchState is moved as 11 words");
+
+struct BatchParams {
+  const BatchProblem* probs;
+  BatchState* state;     // zero on entry
+  int nprob;
+  int ntasks;            // total tiles of all problems
+  double* part;          // per task, 4 partials
+  SyncCtl* ctl;
+  unsigned long long* gen;  // release flag of the reducing block
+  int* any_active;
+  unsigned long long timeout_ns;
+  unsigned stall_extra;  // test hook: the first barrier awaits this many blocks more than launched
+};
+
+// Cooperative launch (all blocks co-resident: grid <= occupancy x SMs).
+cudaError_t launch_cg_batch(const BatchParams& P, int grid, cudaStream_t st);
+const void* cg_batch_kernel_ptr();
+
+}  // namespace pyomgpu

@@ -363,6 +363,29 @@ def congrad_surf_press(M, forc):
     return it
 
 
+def congrad_streamfunction_batch(contexts, forcs, sols, eps=1e-12, max_it=1000000, rtol=0.0):
+    """Many congrad_streamfunction solves (solve_streamfct.f90:153-327) in one
+    work-queue launch: solve k on ``contexts[k]`` (an :class:`ExternalMode`;
+    repeats allowed) with ``forcs[k]`` (None = zero forcing) and ``sols[k]``
+    updated in place.  The reference runs such solves one after another
+    (streamfct_init.f90:272-287).  ``rtol`` > 0 adds the relative-residual
+    stop.  Returns one info dict per solve."""
+    L = _abi.load()
+    n = len(contexts)
+    if n < 1 or len(forcs) != n or len(sols) != n:
+        raise PyOMGPUError(_abi.EINVAL, "contexts, forcs and sols must have the same non-zero length")
+    VP = C.c_void_p * n
+    ctx = VP(*[em._ctx for em in contexts])
+    fp = VP(*[None if f is None else _ptr(f, em.shape).value for em, f in zip(contexts, forcs)])
+    sp = VP(*[_ptr(s, em.shape, True).value for em, s in zip(contexts, sols)])
+    infos = (_abi.SolveInfo * n)()
+    rc = L.pyomgpu_congrad_streamfunction_batch(ctx, n, fp, sp, float(eps), int(max_it), float(rtol), infos,
+                                                _stream())
+    _abi.check(rc, allow=(_abi.OK, _abi.MAXITER, _abi.DIVERGED))
+    _warn_status(rc, "congrad_streamfunction_batch")
+    return [i.as_dict() for i in infos]
+
+
 def island_boundaries(M, mnisle=0, maxipp=0, maxq=0):
     """Island labels and traced perimeters (streamfct_init.f90:35-267) on the
     host: returns (boundary, line_dir, nr_boundary) in the reference layout."""
