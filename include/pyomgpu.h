@@ -262,6 +262,28 @@ int32_t pyomgpu_solve_streamfunction(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgp
 int32_t pyomgpu_solve_pressure(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_solve_info* info,
                                pyomgpu_stream stream);
 
+/* ---- learned preconditioner (no counterpart in the reference) ----------------- */
+/* Building block of the U-Net preconditioner: one 3x3 convolution (stride 1,
+ * zero padding 1) on the tcgen05 tensor cores, BF16 operands, FP32
+ * accumulation.  Activations are "channel-group planar" bf16:
+ * [C/8][H][W][8] (a pixel's 8 channels of one group in 16 bytes).  All
+ * pointers DEVICE.  w is f32 [cout][cin][3][3] (PyTorch order), bias f32
+ * [cout] or NULL.  cin, cout in {16, 32, 64}.  epilogue:
+ *   0  y = act(conv + bias (+ addend)) as planar bf16 [cout/8][H][W][8];
+ *      gate (planar like y, may be NULL) zeroes y where gate <= 0 (the ReLU
+ *      backward); pool_out (may be NULL; H, W even) receives the 2x2 average
+ *      of y, planar [cout/8][H/2][W/2][8];
+ *   1  y (2H x 2W) = act(conv broadcast to 2x2 blocks + addend) (decoder
+ *      upsample + skip; addend required, 2H x 2W);
+ *   2  y = f32 [H][W], channel 0 of conv + bias.
+ * relu != 0 selects act = max(0, .).  flip != 0 runs the backward-data
+ * convolution of a forward layer whose weight w is [cin][cout][3][3]
+ * (channels transposed, kernel rotated 180 degrees). */
+int32_t pyomgpu_conv3x3_bf16(int32_t cin, int32_t cout, int32_t H, int32_t W, const uint16_t* x, const float* w,
+                             const float* bias, int32_t relu, int32_t epilogue, const uint16_t* gate,
+                             const uint16_t* addend, void* y, uint16_t* pool_out, int32_t flip,
+                             pyomgpu_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,7 +32,8 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_congrad_streamfunction_batch",
            "pyomgpu_congrad_surf_press", "pyomgpu_solve_rtol",
            "pyomgpu_apply_op", "pyomgpu_get_inv_diag", "pyomgpu_line_integral",
-           "pyomgpu_solve_streamfunction", "pyomgpu_solve_pressure")
+           "pyomgpu_solve_streamfunction", "pyomgpu_solve_pressure",
+           "pyomgpu_conv3x3_bf16")
 
 
 class PyOMGPUError(RuntimeError):
@@ -113,6 +114,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_line_integral": (i32, [vp, i32, vp, vp, P(d), vp]),
         "pyomgpu_solve_streamfunction": (i32, [vp, P(State), P(SolveInfo), vp]),
         "pyomgpu_solve_pressure": (i32, [vp, P(State), P(SolveInfo), vp]),
+        "pyomgpu_conv3x3_bf16": (i32, [i32, i32, i32, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, i32, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

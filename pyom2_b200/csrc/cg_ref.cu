@@ -380,16 +380,24 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g) {
+namespace {
+EncodeTiledFn tiled_encoder() {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     cudaDriverEntryPointQueryResult q;
     void* p = nullptr;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess || !p)
-      return -1;
+      return nullptr;
     fn = (EncodeTiledFn)p;
   }
+  return fn;
+}
+}  // namespace
+
+int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g) {
+  EncodeTiledFn fn = tiled_encoder();
+  if (!fn) return -1;
   const cuuint64_t dims[2] = {(cuuint64_t)g.pitch, (cuuint64_t)(g.ny + 2 * kOnx)};
   const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(double)};
   const cuuint32_t box[2] = {(cuuint32_t)kBoxX, (cuuint32_t)kBoxY};
@@ -397,6 +405,23 @@ int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g) {
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (int)r;
+}
+
+int encode_map(CUtensorMap* map, CUtensorMapDataType dtype, int rank, const void* base, const uint64_t* dims,
+               const uint64_t* strides_bytes, const uint32_t* box) {
+  EncodeTiledFn fn = tiled_encoder();
+  if (!fn || rank < 1 || rank > 5) return -1;
+  cuuint64_t d[5], s[4];
+  cuuint32_t b[5], es[5];
+  for (int k = 0; k < rank; k++) {
+    d[k] = dims[k];
+    b[k] = box[k];
+    es[k] = 1;
+    if (k < rank - 1) s[k] = strides_bytes[k];
+  }
+  CUresult r = fn(map, dtype, (cuuint32_t)rank, (void*)base, d, s, b, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return (int)r;
 }
 

@@ -63,8 +63,22 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return true;
 }
 
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Host: tensor map of a padded FP64 field ((ny+4) rows of `pitch` elements)
 // with a kBoxX x kBoxY box.  Returns 0 or a CUDA driver error code.
 int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g);
+
+// Host: general tiled tensor map (no swizzle, zero fill out of bounds).
+// dims[0] is the contiguous dimension; strides_bytes has rank-1 entries.
+int encode_map(CUtensorMap* map, CUtensorMapDataType dtype, int rank, const void* base, const uint64_t* dims,
+               const uint64_t* strides_bytes, const uint32_t* box);
 
 }  // namespace pyomgpu
