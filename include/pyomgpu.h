@@ -106,7 +106,7 @@ typedef struct pyomgpu_solve_info {
   double rel_residual;      /* FP64 ||b-Ax||/||b|| over the unknowns (solve_rtol only) */
   double device_ms;         /* device time of the CG kernel launch(es), CUDA events on the stream */
   int32_t kernel_launches;  /* kernels the call launched (solve_rtol; 1 = the CG kernel elsewhere) */
-  int32_t pad_;
+  int32_t fcg_iterations;   /* iterations of the flexible-CG phase (pyomgpu_solve_fcg), else 0 */
 } pyomgpu_solve_info;
 
 /* Model arrays of one time step (all DEVICE pointers, Fortran layout). */
@@ -283,6 +283,50 @@ int32_t pyomgpu_conv3x3_bf16(int32_t cin, int32_t cout, int32_t H, int32_t W, co
                              const float* bias, int32_t relu, int32_t epilogue, const uint16_t* gate,
                              const uint16_t* addend, void* y, uint16_t* pool_out, int32_t flip,
                              pyomgpu_stream stream);
+
+/* The learned preconditioner of one grid: a 4-level U-Net (16/32/64/64
+ * channels, 3x3 convolutions, BF16 weights and activations, FP32
+ * accumulation) whose input is the residual scaled to unit rms, the unknown
+ * mask, hur/mean(hur) and cosu, and whose output is a search direction
+ * z ~ A^-1 r (scale free).  The context must have its islands set (Z).
+ * training != 0 adds gradient and Adam buffers.  Parameters start at zero:
+ * load them with pyomgpu_precond_set_params (f32, weights of the 12 layers in
+ * PyTorch order [cout][cin][3][3], then their biases). */
+typedef struct pyomgpu_precond pyomgpu_precond;
+int64_t pyomgpu_precond_num_params(void);
+int32_t pyomgpu_precond_create(pyomgpu_ctx* ctx, int32_t training, pyomgpu_precond** out);
+void pyomgpu_precond_destroy(pyomgpu_precond* p);
+/* Moves the network (parameters and optimiser state kept) to another grid of
+ * the same size, e.g. to train on a family of grids. */
+int32_t pyomgpu_precond_rebind(pyomgpu_precond* p, pyomgpu_ctx* ctx);
+/* params: host or device, n = pyomgpu_precond_num_params(). */
+int32_t pyomgpu_precond_set_params(pyomgpu_precond* p, const float* params, int64_t n);
+int32_t pyomgpu_precond_get_params(pyomgpu_precond* p, float* params, int64_t n);
+/* gradients of the last pyomgpu_precond_train_step / _unet_forward_backward */
+int32_t pyomgpu_precond_get_grads(pyomgpu_precond* p, float* grads, int64_t n);
+/* z = M(r); r, z Fortran-layout DEVICE arrays (z's halo holds the cyclic copies). */
+int32_t pyomgpu_precond_apply(pyomgpu_precond* p, const double* r, double* z, pyomgpu_stream stream);
+/* One training step on the pair (r, e): r a residual b - A x of the plain
+ * solver, e = x* - x its error (Fortran-layout DEVICE arrays).  loss = 1 -
+ * cos^2 of the angle between M(r) and e in the energy inner product
+ * u^T D A v (D = dxu dyu cosu).  lr > 0 applies an Adam step (beta1 0.9,
+ * beta2 0.999); lr = 0 only computes the gradients. */
+int32_t pyomgpu_precond_train_step(pyomgpu_precond* p, const double* r, const double* e, float lr, float* loss,
+                                   pyomgpu_stream stream);
+/* The network alone, for gradient checks: x0 = planar bf16 input
+ * [2][Hp][Wp][8] (Hp, Wp = ny, nx rounded up to multiples of 8), z = f32
+ * output [Hp][Wp]; with gz (f32 [Hp][Wp], training only) also the parameter
+ * gradients of sum(gz * z).  Host or device pointers. */
+int32_t pyomgpu_unet_forward_backward(pyomgpu_precond* p, const uint16_t* x0, const float* gz, float* z,
+                                      pyomgpu_stream stream);
+/* Flexible CG (FCG(1)) preconditioned by the network, FP64 vectors and dot
+ * products in the D-weighted inner product, to the FP64 true relative
+ * residual rtol (as pyomgpu_solve_rtol).  When FCG stalls or breaks down the
+ * iterate goes to the Jacobi-PCG kernel; the true residual decides.  info:
+ * iterations (FCG + PCG), outer_iterations (1, or 2 when PCG took over),
+ * rel_residual. */
+int32_t pyomgpu_solve_fcg(pyomgpu_ctx* ctx, pyomgpu_precond* p, const double* forc, double* sol, double rtol,
+                          int32_t max_iterations, pyomgpu_solve_info* info, pyomgpu_stream stream);
 
 #ifdef __cplusplus
 }

@@ -33,7 +33,10 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_congrad_surf_press", "pyomgpu_solve_rtol",
            "pyomgpu_apply_op", "pyomgpu_get_inv_diag", "pyomgpu_line_integral",
            "pyomgpu_solve_streamfunction", "pyomgpu_solve_pressure",
-           "pyomgpu_conv3x3_bf16")
+           "pyomgpu_conv3x3_bf16", "pyomgpu_precond_num_params", "pyomgpu_precond_create",
+           "pyomgpu_precond_destroy", "pyomgpu_precond_rebind", "pyomgpu_precond_set_params", "pyomgpu_precond_get_params",
+           "pyomgpu_precond_get_grads", "pyomgpu_precond_apply", "pyomgpu_precond_train_step",
+           "pyomgpu_unet_forward_backward", "pyomgpu_solve_fcg")
 
 
 class PyOMGPUError(RuntimeError):
@@ -61,7 +64,7 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("status", C.c_int32),
                 ("outer_iterations", C.c_int32), ("estimated_error", C.c_double),
                 ("rel_residual", C.c_double), ("device_ms", C.c_double),
-                ("kernel_launches", C.c_int32), ("pad_", C.c_int32)]
+                ("kernel_launches", C.c_int32), ("fcg_iterations", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -115,6 +118,17 @@ def load(path: str = LIB_PATH):
         "pyomgpu_solve_streamfunction": (i32, [vp, P(State), P(SolveInfo), vp]),
         "pyomgpu_solve_pressure": (i32, [vp, P(State), P(SolveInfo), vp]),
         "pyomgpu_conv3x3_bf16": (i32, [i32, i32, i32, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, i32, vp]),
+        "pyomgpu_precond_num_params": (C.c_int64, []),
+        "pyomgpu_precond_create": (i32, [vp, i32, P(vp)]),
+        "pyomgpu_precond_destroy": (None, [vp]),
+        "pyomgpu_precond_rebind": (i32, [vp, vp]),
+        "pyomgpu_precond_set_params": (i32, [vp, vp, C.c_int64]),
+        "pyomgpu_precond_get_params": (i32, [vp, vp, C.c_int64]),
+        "pyomgpu_precond_get_grads": (i32, [vp, vp, C.c_int64]),
+        "pyomgpu_precond_apply": (i32, [vp, vp, vp, vp]),
+        "pyomgpu_precond_train_step": (i32, [vp, vp, vp, C.c_float, P(C.c_float), vp]),
+        "pyomgpu_unet_forward_backward": (i32, [vp, vp, vp, vp, vp]),
+        "pyomgpu_solve_fcg": (i32, [vp, vp, vp, vp, d, i32, P(SolveInfo), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

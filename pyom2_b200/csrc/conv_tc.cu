@@ -35,7 +35,7 @@ __host__ __device__ constexpr uint32_t pow2_cols(uint32_t n) {
 
 template <int CIN, int COUT>
 struct ConvShape {
-  static constexpr int GIN = CIN / 8, GOUT = COUT / 8;
+  static constexpr int GIN = CIN / 8;
   static constexpr uint32_t XBYTES = (uint32_t)GIN * kBH * kBW * 16;
   static constexpr uint32_t WBYTES = 9u * CIN * COUT * 2;
   static constexpr uint32_t WOFF = (XBYTES + 1023u) / 1024u * 1024u;

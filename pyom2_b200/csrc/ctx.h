@@ -1,0 +1,129 @@
+// Private: the solver context behind the opaque pyomgpu_ctx handle of the C
+// ABI, shared by the translation units that implement entry points
+// (capi.cu, precond.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pyomgpu.h"
+#include "cg_batch.cuh"
+#include "cg_pipe.cuh"
+#include "cg_ref.cuh"
+#include "common.cuh"
+#include "islands.h"
+#include "kernels.cuh"
+
+using pyomgpu::BatchProblem;
+using pyomgpu::BatchState;
+using pyomgpu::CGResult;
+using pyomgpu::Geo;
+using pyomgpu::IslandDev;
+using pyomgpu::IslandSet;
+using pyomgpu::OpBuf;
+using pyomgpu::OpDev;
+using pyomgpu::PipeResult;
+using pyomgpu::SyncCtl;
+
+struct pyomgpu_ctx {
+  int device = 0, nsm = 0;
+  Geo g{};
+  int nx = 0, ny = 0;
+  size_t n2 = 0;  // (nx+4)*(ny+4)
+  int free_surface = 0;
+  double grav = 0, dt_mom = 0;
+  std::vector<double> h_maskU, h_maskV;
+  // device grid copies
+  double *dxt = nullptr, *dxu = nullptr, *dyt = nullptr, *dyu = nullptr, *cost = nullptr, *cosu = nullptr;
+  double *hur = nullptr, *hvr = nullptr, *hu = nullptr, *hv = nullptr, *mT = nullptr, *mU = nullptr, *mV = nullptr;
+  OpBuf sf, sp;
+  bool have_sp = false;
+  // islands
+  bool have_islands = false, have_psin = false, have_line_psin = false, lu_singular = false;
+  IslandSet isl;
+  IslandDev idev;
+  std::vector<int> psin_iters;
+  std::vector<double> line_psin;
+  int *bnd_i = nullptr, *bnd_j = nullptr;
+  int nbnd = 0;
+  double* psin = nullptr;  // Fortran layout, nisle fields
+  double *lu = nullptr, *line_forc = nullptr, *line_psi0 = nullptr;
+  int* ipiv = nullptr;
+  // CG work
+  double *res = nullptr, *s0 = nullptr, *s1 = nullptr, *As = nullptr, *sol = nullptr;
+  double *stage_a = nullptr, *stage_b = nullptr, *fpx = nullptr, *fpy = nullptr, *forc = nullptr, *zeros = nullptr;
+  double *part = nullptr, *scal = nullptr;
+  SyncCtl* ctl = nullptr;
+  double* slots = nullptr;
+  CGResult* d_result = nullptr;
+  CGResult* h_result = nullptr;
+  double* h_scal = nullptr;
+  int max_blocks = 0;  // co-resident blocks of the CG kernels
+  double timeout_s = 2.0;
+  unsigned stall_next = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+  // single-barrier PCG (pyomgpu_solve_rtol), allocated on first use
+  struct Fast {
+    bool ready = false, f32_ready = false, op32_stale = true;
+    int max_blocks = 0;
+    double* b = nullptr;
+    double *r[2] = {}, *q[2] = {}, *w[2] = {};
+    double* p = nullptr;
+    OpDev<float> op32{};
+    float *FX = nullptr, *FY = nullptr, *W = nullptr, *ax = nullptr, *bx = nullptr, *by = nullptr;
+    float *b32 = nullptr, *x32 = nullptr, *p32 = nullptr;
+    float *r32[2] = {}, *q32[2] = {}, *w32[2] = {};
+    double* slots = nullptr;
+    PipeResult* d_res = nullptr;
+    PipeResult* h_res = nullptr;
+    std::vector<void*> owned;
+  } fast;
+
+  // work-queue batch (pyomgpu_congrad_streamfunction_batch and the psin
+  // solves); grows to the largest batch run through this context
+  struct Batch {
+    int max_blocks = 0;
+    double* pool = nullptr;  // per solve: padded sol, res, s0, s1, As + Fortran staging of forc, sol
+    size_t cap = 0;          // doubles
+    BatchProblem* d_probs = nullptr;
+    BatchProblem* h_probs = nullptr;  // pinned
+    BatchState* d_state = nullptr;
+    BatchState* h_state = nullptr;    // pinned
+    int cap_probs = 0;
+    double* part = nullptr;  // 4 per task
+    size_t cap_tasks = 0;
+    double* d_rr = nullptr;  // 2 per solve: true residual, forcing norm
+    double* h_rr = nullptr;  // pinned
+    unsigned long long* sync = nullptr;  // SyncCtl, gen, any_active
+  } batch;
+
+  ~pyomgpu_ctx() {
+    for (void* p : fast.owned)
+      if (p) cudaFree(p);
+    if (fast.h_res) cudaFreeHost(fast.h_res);
+    for (void* p : {(void*)batch.pool, (void*)batch.d_probs, (void*)batch.d_state, (void*)batch.part,
+                    (void*)batch.d_rr, (void*)batch.sync})
+      if (p) cudaFree(p);
+    if (batch.h_probs) cudaFreeHost(batch.h_probs);
+    if (batch.h_state) cudaFreeHost(batch.h_state);
+    if (batch.h_rr) cudaFreeHost(batch.h_rr);
+    void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
+                    sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,
+                    res, s0, s1, As, sol, stage_a, stage_b, fpx, fpy, forc, zeros, part, scal, ctl, slots, d_result,
+                    idev.seg_i, idev.seg_j, idev.seg_d, idev.seg_off};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+    if (h_result) cudaFreeHost(h_result);
+    if (h_scal) cudaFreeHost(h_scal);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+// Jacobi-PCG (the reference algorithm of congrad_streamfunction with the
+// relative-residual stop) on c->sol (padded, halo valid), forcing in Fortran
+// layout on the device (capi.cu).
+int run_pcg_from_sol(pyomgpu_ctx* c, const double* forc_dev, int max_it, double rtol, pyomgpu_solve_info* info,
+                     cudaStream_t st);

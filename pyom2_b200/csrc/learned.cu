@@ -20,6 +20,16 @@ int lfail(int code, const char* msg) {
   return code;
 }
 
+bool on_device(const void* p) {
+  if (!p) return true;  // optional arguments
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 int sm_count() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);
@@ -38,6 +48,9 @@ int32_t pyomgpu_conv3x3_bf16(int32_t cin, int32_t cout, int32_t H, int32_t W, co
   if (!x || !w || !y || H < 1 || W < 1) return lfail(PYOMGPU_EINVAL, "conv3x3: null pointer or empty image");
   if (!conv3x3_supported(cin, cout)) return lfail(PYOMGPU_EINVAL, "conv3x3: channel counts must be 16, 32 or 64");
   if (epilogue < kEpiPlain || epilogue > kEpiF32) return lfail(PYOMGPU_EINVAL, "conv3x3: unknown epilogue");
+  for (const void* p : {(const void*)x, (const void*)w, (const void*)bias, (const void*)gate, (const void*)addend,
+                        (const void*)y, (const void*)pool_out})
+    if (!on_device(p)) return lfail(PYOMGPU_EINVAL, "conv3x3: every array must be in device memory");
   cudaStream_t st = (cudaStream_t)stream;
   uint16_t* wpack = nullptr;
   int* err = nullptr;

@@ -1,0 +1,178 @@
+"""GPU tests of the learned preconditioner: network values and gradients
+against the FP64 CPU oracle (oracle/unet_oracle.py, with the GPU's bf16
+storage points emulated), the training loss against a numpy evaluation with
+the oracle operator, flexible CG to the 1e-10 true residual, and an ablation:
+what training the network gains over the untrained network and over
+Jacobi-PCG.
+
+Tolerances: the GPU accumulates in FP32 and rounds activations and gradients
+to bf16 at the same points as the oracle; rare round-to-nearest ties broken
+the other way change single elements by one bf16 ulp (2**-8 relative), so
+values agree to 1e-2 relative in L2 and gradients to 3e-2 per layer.
+"""
+import numpy as np
+import pytest
+
+from oracle import unet_oracle as U
+from pyom2_b200 import _abi, learned, synth
+from pyom2_b200.external import ExternalMode
+
+pytestmark = pytest.mark.gpu
+LIMITS = dict(maxipp=10**6, maxq=10**6)
+
+
+def rel(a, b):
+    n = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / n if n > 0 else np.linalg.norm(a - b)
+
+
+def grid(name):
+    if name == "c0":
+        return synth.config0()
+    if name == "cyc96":
+        return synth._global_like(96, 48, -80.0, 80.0, 13, n_land_masses=6, mask_sigma=4.0, depth_sigma=4.0,
+                                  name="cyc96")
+    if name == "cyc192":
+        return synth._global_like(192, 96, -80.0, 80.0, 21, n_land_masses=8, mask_sigma=5.0, depth_sigma=5.0,
+                                  name="cyc192")
+    raise KeyError(name)
+
+
+def setup(name):
+    W = grid(name)
+    E = ExternalMode(W.M)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        E.streamfunction_init(**LIMITS)
+    return W, E
+
+
+def test_network_values_and_gradients_match_oracle():
+    W, E = setup("c0")
+    pc = learned.LearnedPreconditioner(E, training=True, params=None, seed=3)
+    rng = np.random.default_rng(5)
+    p = learned.init_params(3)
+    nw = sum(9 * a * b for a, b in learned.LAYERS)
+    p[nw:] = rng.standard_normal(p.size - nw).astype(np.float32) * 0.1  # non-zero biases
+    p[:nw] *= 1.5
+    pc.set_params(p)
+    Hp, Wp = 40, 40
+    x0 = U.bf16_round(rng.standard_normal((16, Hp, Wp)))
+    bits = U.bf16_bits(U.to_planar(x0))
+    gz = rng.standard_normal((Hp, Wp)).astype(np.float32)
+    z = pc.forward_backward(bits, gz)
+    g = pc.get_grads()
+    zo, A = U.unet_forward(p, x0, emulate=True)
+    go = U.unet_backward(p, A, gz.astype(np.float64), emulate=True)
+    assert rel(z, zo) < 1e-2, rel(z, zo)
+    # per layer: weights then biases
+    o = 0
+    for l, (ci, co) in enumerate(learned.LAYERS):
+        n = 9 * ci * co
+        assert rel(g[o:o + n], go[o:o + n]) < 3e-2, (l, rel(g[o:o + n], go[o:o + n]))
+        o += n
+    for l, (ci, co) in enumerate(learned.LAYERS):
+        assert rel(g[o:o + co], go[o:o + co]) < 3e-2, ("bias", l)
+        o += co
+    # the oracle's own FP64 gradients agree with the emulated ones to bf16 level
+    zf, Af = U.unet_forward(p, x0, emulate=False)
+    assert rel(zo, zf) < 5e-2
+    pc.close()
+
+
+def test_training_loss_matches_numpy(oracle_lib):
+    W, E = setup("cyc96")
+    import torch
+    Mo = W.M.copy()
+    O = oracle_lib.Oracle(Mo)
+    O.streamfunction_init(**LIMITS)
+    cf = O.make_coeff_streamfunction()
+    pc = learned.LearnedPreconditioner(E, training=True, seed=1)
+    rng = np.random.default_rng(2)
+    Z = E.make_inv_sfc()
+    mask = (Z != 0).astype(np.float64)
+    r = np.asfortranarray(rng.standard_normal(W.M.shape2d) * mask)
+    e = np.asfortranarray(rng.standard_normal(W.M.shape2d) * mask)
+    rt, et = learned._dev(r), learned._dev(e)
+    z = pc.apply(rt).cpu().numpy()
+    loss = pc.train_step(rt, et, 0.0)
+    M = W.M
+    D = M.dxu[:, None] * M.dyu[None, :] * M.cosu[None, :]
+    inner = (slice(2, M.nx + 2), slice(2, M.ny + 2))
+
+    def S(u):
+        return (D * O.apply_op(cf, np.asfortranarray(u)))[inner]
+
+    m = mask > 0
+    nu = m.sum()
+    dbar = np.mean(1.0 / np.abs(Z[m]))
+    # both fields enter the operator with their cyclic halo copies, as on the GPU
+    zi = np.asfortranarray(np.where(m, z, 0.0))
+    es = np.asfortranarray(e * dbar / np.sqrt(np.sum(r[m] ** 2) / nu))
+    O.setcyclic_xy(zi)
+    O.setcyclic_xy(es)
+    a = np.sum(zi[inner] * S(es))
+    b = np.sum(zi[inner] * S(zi))
+    c = np.sum(es[inner] * S(es))
+    want = (b - 2 * a + c) / c
+    assert abs(loss - want) < 1e-6 * max(1.0, abs(want)), (loss, want)
+    pc.close()
+
+
+@pytest.mark.parametrize("name", ["c0", "cyc96"])
+def test_fcg_reaches_1e10_and_matches_oracle(oracle_lib, name):
+    import torch
+    W, E = setup(name)
+    pc = learned.LearnedPreconditioner(E, seed=7)  # untrained: FCG still converges (PCG takes over if needed)
+    sol = np.zeros(W.M.shape2d, order="F")
+    info = learned.solve_fcg(E, pc, W.forc, sol, rtol=1e-10)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
+    O = oracle_lib.Oracle(W.M.copy())
+    O.streamfunction_init(**LIMITS)
+    cf = O.make_coeff_streamfunction()
+    Z = O.make_inv_sfc(cf)
+    assert O.rel_residual(cf, Z, W.forc, sol) <= 1.5e-10
+    so = np.zeros(W.M.shape2d, order="F")
+    O.congrad_streamfunction(cf, W.forc, so, eps=0.0, max_it=100000, rtol=1e-12)
+    O.setcyclic_xy(so)
+    m = Z != 0
+    assert np.linalg.norm((sol - so)[m]) / np.linalg.norm(so[m]) < 1e-8
+    # device tensors in place give the same answer
+    s_t = learned._dev(np.zeros(W.M.shape2d))
+    learned.solve_fcg(E, pc, learned._dev(W.forc), s_t, rtol=1e-10)
+    assert np.linalg.norm(s_t.cpu().numpy() - sol) <= 1e-9 * np.linalg.norm(sol)
+    pc.close()
+
+
+def test_ablation_training_gains():
+    """Train on solver-generated pairs of one grid for a few hundred steps,
+    then count iterations to the 1e-10 true residual on a fresh right-hand
+    side: the solver with the trained network needs fewer than with the
+    untrained one, and fewer than Jacobi-PCG (the method without the
+    network)."""
+    W, E = setup("cyc192")
+    basis = learned.rhs_basis(W, 6, seed=11)
+    pc = learned.LearnedPreconditioner(E, training=True, seed=0)
+    losses = learned.generate_and_train(pc, W, E, basis, steps=600, lr=1e-3, seed=4)
+    assert np.mean(losses[-100:]) < np.mean(losses[:50])
+    trained = pc.get_params()
+    test_rhs = learned.rhs_basis(W, 1, seed=999)[0]
+
+    def fcg_iters(params):
+        q = learned.LearnedPreconditioner(E, params=params)
+        s = np.zeros(W.M.shape2d, order="F")
+        info = learned.solve_fcg(E, q, test_rhs, s, rtol=1e-10)
+        q.close()
+        assert info["status"] == 0 and info["rel_residual"] <= 1e-10
+        return info
+
+    it_trained = fcg_iters(trained)
+    it_untrained = fcg_iters(learned.init_params(0))
+    s = np.zeros(W.M.shape2d, order="F")
+    pcg = E.solve_rtol(test_rhs, s, rtol=1e-10, precision=_abi.PREC_F64)
+    print("ablation", it_trained, it_untrained, pcg["iterations"])
+    assert it_trained["outer_iterations"] == 1  # no fallback needed
+    assert it_trained["iterations"] < it_untrained["iterations"]
+    assert it_trained["iterations"] < pcg["iterations"]
+    pc.close()

@@ -66,3 +66,29 @@ def test_planar_roundtrip():
     p = U.to_planar(x)
     assert p.shape == (2, 3, 5, 8) and p[1, 2, 4, 3] == x[11, 2, 4]
     assert np.array_equal(U.from_planar(p), x)
+
+
+def test_network_backward_finite_differences():
+    """The oracle's U-Net gradient (pure FP64) against central differences."""
+    rng = np.random.default_rng(4)
+    n = U.num_params()
+    p = rng.standard_normal(n) * 0.2
+    x0 = rng.standard_normal((16, 16, 24))
+    gz = rng.standard_normal((16, 24))
+    z, A = U.unet_forward(p, x0, emulate=False)
+    g = U.unet_backward(p, A, gz, emulate=False)
+    f = lambda q: float(np.sum(gz * U.unet_forward(q, x0, emulate=False)[0]))
+    h = 1e-6
+    # one weight and one bias of several layers (offsets of the flat layout)
+    offs, o = [], 0
+    for ci, co, _, _ in U.LAYERS:
+        offs.append(o + 9 * ci * co // 2)
+        o += 9 * ci * co
+    for ci, co, _, _ in U.LAYERS:
+        offs.append(o + co // 2)
+        o += co
+    for k in offs[::3]:
+        e = np.zeros(n)
+        e[k] = h
+        fd = (f(p + e) - f(p - e)) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-5 * max(1.0, abs(fd)), (k, fd, g[k])
