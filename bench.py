@@ -35,7 +35,7 @@ RTOL = 1e-10
 BYTES_PER_POINT_ITER = {"f64": 72, "f32": 36}  # algorithmic bytes, plain PCG iteration
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of this
 # workload (profiles/cg_ref_kernel_c1_1440x720.md), per iteration, keyed by kernel
-MEASURED_TRAFFIC_PER_ITER = {"cg_ref_kernel": (1.219541e9 + 2.498041e9) / 1760}
+MEASURED_TRAFFIC_PER_ITER = {"cg_ref_kernel<false>": (1.219541e9 + 2.498041e9) / 1760}
 CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
            "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -159,6 +159,8 @@ METHODS = {
     # name: (precision code, dtype label, algorithmic bytes key, dominant kernel)
     "pcg64": ("PREC_F64", "f64", "f64", "cg_ref_kernel<false>"),
     "mixed32": ("PREC_F32", "f32+f64", "f32", "cg_pipe_kernel<float>"),
+    # flexible CG with the learned U-Net (bf16 tensor-core network, FP64 vectors)
+    "fcg": (None, "f64+bf16", "f64", "conv3x3_tc_kernel"),
 }
 
 
@@ -168,7 +170,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--methods", default="pcg64,mixed32",
+    ap.add_argument("--methods", default="pcg64,mixed32,fcg",
                     help="comma list of solve methods to time; the fastest is the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -203,10 +205,19 @@ def main():
     n2 = M.shape2d[0] * M.shape2d[1]
     peak, peak_kind = peaks()
 
-    def solve(prec, forc, sol):
+    pc = None
+    if "fcg" in args.methods.split(","):
+        from pyom2_b200 import learned
+        pc = learned.LearnedPreconditioner(E, params=learned.load_params())
+
+    def solve(name, forc, sol):
         info = _abi.SolveInfo()
-        rc = L.pyomgpu_solve_rtol(E._ctx, _ptr(forc), _ptr(sol), RTOL, prec, 1000000, C.byref(info),
-                                  C.c_void_p(stream.cuda_stream))
+        if name == "fcg":
+            rc = L.pyomgpu_solve_fcg(E._ctx, pc._h, _ptr(forc), _ptr(sol), RTOL, 100000, C.byref(info),
+                                     C.c_void_p(stream.cuda_stream))
+        else:
+            rc = L.pyomgpu_solve_rtol(E._ctx, _ptr(forc), _ptr(sol), RTOL, getattr(_abi, METHODS[name][0]), 1000000,
+                                      C.byref(info), C.c_void_p(stream.cuda_stream))
         _abi.check(rc)
         return info
 
@@ -214,10 +225,9 @@ def main():
     clk_summary = None
     for name in [m for m in args.methods.split(",") if m]:
         code, dtype, bkey, kname = METHODS[name]
-        prec = getattr(_abi, code)
         for _ in range(args.warmup):
             sol_d.zero_()
-            solve(prec, forc_d, sol_d)
+            solve(name, forc_d, sol_d)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -229,7 +239,7 @@ def main():
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                info = solve(prec, forc_d, sol_d)
+                info = solve(name, forc_d, sol_d)
                 e1.record(stream)
                 e1.synchronize()
                 times.append(e0.elapsed_time(e1))
@@ -260,7 +270,6 @@ def main():
 
     best = min(results, key=lambda k: results[k]["value"])
     R = results[best]
-    prec = getattr(_abi, METHODS[best][0])
     # end to end through the C ABI with host buffers (copies inside the timed region)
     forc_h = np.asfortranarray(W.forc)
     sol_h = np.zeros(M.shape2d, order="F")
@@ -270,7 +279,7 @@ def main():
         flush.fill_(1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        solve(prec, forc_h, sol_h)
+        solve(best, forc_h, sol_h)
         dt = (time.perf_counter() - t0) * 1e3
         if k >= args.warmup:
             e2e.append(dt)
@@ -295,6 +304,11 @@ def main():
         "clocks": R["clocks"],
         "methods": {k: {kk: vv for kk, vv in v.items() if kk != "clocks"} for k, v in results.items()},
     }
+    if "fcg" in results and "pcg64" in results:
+        out["learned_fcg_vs_pcg"] = {"fcg_ms": results["fcg"]["value"], "pcg64_ms": results["pcg64"]["value"],
+                                     "fcg_iterations": results["fcg"]["iterations"],
+                                     "pcg64_iterations": results["pcg64"]["iterations"],
+                                     "speedup": results["pcg64"]["value"] / results["fcg"]["value"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(W, results.get("pcg64", R)["iterations"])
     if rank == 0:

@@ -18,9 +18,8 @@
 
 namespace pyomgpu {
 
-constexpr int kConvTileX = 128;  // output pixels per row tile (MMA M)
-constexpr int kConvRows = 4;     // output rows per CTA tile
-constexpr int kConvThreads = 128;
+constexpr int kConvTileX = 128;   // output pixels per row tile (MMA M)
+constexpr int kConvThreads = 256;  // 2 warpgroups: TMEM lane quarter = warp % 4, channel half = warp / 4
 
 // Epilogue of one convolution: v = acc + bias, then
 //   kEpiPlain: y = act(v (+ addend)) at the input resolution, optional gate
@@ -32,7 +31,7 @@ constexpr int kConvThreads = 128;
 enum ConvEpilogue : int { kEpiPlain = 0, kEpiUp = 1, kEpiF32 = 2 };
 
 struct ConvArgs {
-  CUtensorMap map_x;      // input, box (8, 130, kConvRows+2, Cin/8)
+  CUtensorMap map_x;      // input, box (8, 130, rows+2, Cin/8), rows = the instantiation's tile height
   const uint16_t* wpack;  // [9][Cin/8][Cout][8] bf16
   const float* bias;      // [Cout] or null
   void* y;

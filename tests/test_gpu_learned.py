@@ -1,9 +1,9 @@
 """GPU tests of the learned preconditioner: network values and gradients
 against the FP64 CPU oracle (oracle/unet_oracle.py, with the GPU's bf16
 storage points emulated), the training loss against a numpy evaluation with
-the oracle operator, flexible CG to the 1e-10 true residual, and an ablation:
-what training the network gains over the untrained network and over
-Jacobi-PCG.
+the oracle operator, flexible CG to the 1e-10 true residual, training, and
+an ablation: what the trained network gains over the untrained network and
+over Jacobi-PCG on a held-out grid.
 
 Tolerances: the GPU accumulates in FP32 and rounds activations and gradients
 to bf16 at the same points as the oracle; rare round-to-nearest ties broken
@@ -145,34 +145,46 @@ def test_fcg_reaches_1e10_and_matches_oracle(oracle_lib, name):
     pc.close()
 
 
-def test_ablation_training_gains():
-    """Train on solver-generated pairs of one grid for a few hundred steps,
-    then count iterations to the 1e-10 true residual on a fresh right-hand
-    side: the solver with the trained network needs fewer than with the
-    untrained one, and fewer than Jacobi-PCG (the method without the
-    network)."""
+def test_training_reduces_loss():
+    """A few hundred Adam steps on solver-generated pairs of one grid lower
+    the relative energy-norm loss (the training loop runs end to end on the
+    GPU: pair generation, forward, loss, backward, update)."""
     W, E = setup("cyc192")
     basis = learned.rhs_basis(W, 6, seed=11)
     pc = learned.LearnedPreconditioner(E, training=True, seed=0)
-    losses = learned.generate_and_train(pc, W, E, basis, steps=600, lr=1e-3, seed=4)
-    assert np.mean(losses[-100:]) < np.mean(losses[:50])
-    trained = pc.get_params()
-    test_rhs = learned.rhs_basis(W, 1, seed=999)[0]
+    losses = learned.generate_and_train(pc, W, E, basis, steps=400, lr=1e-3, seed=4)
+    assert np.all(np.isfinite(losses))
+    assert np.mean(losses[-100:]) < 0.8 * np.mean(losses[:50])
+    pc.close()
 
-    def fcg_iters(params):
+
+def test_ablation_trained_network_gains():
+    """What the trained network gains over the method without it, on a
+    held-out grid of the family it was trained on (1440x720 recipe, a seed no
+    training grid used): iterations to the 1e-10 true residual with the
+    committed weights, with the untrained initial weights, and with
+    Jacobi-PCG alone."""
+    W = synth._global_like(1440, 720, -80.0, 80.0, 3001, n_land_masses=20, name="heldout_3001")
+    E = ExternalMode(W.M)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        E.streamfunction_init(**LIMITS)
+
+    def fcg(params):
         q = learned.LearnedPreconditioner(E, params=params)
         s = np.zeros(W.M.shape2d, order="F")
-        info = learned.solve_fcg(E, q, test_rhs, s, rtol=1e-10)
+        info = learned.solve_fcg(E, q, W.forc, s, rtol=1e-10, max_it=20000)
         q.close()
-        assert info["status"] == 0 and info["rel_residual"] <= 1e-10
+        assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
         return info
 
-    it_trained = fcg_iters(trained)
-    it_untrained = fcg_iters(learned.init_params(0))
+    trained = fcg(learned.load_params())
+    untrained = fcg(learned.init_params(0))
     s = np.zeros(W.M.shape2d, order="F")
-    pcg = E.solve_rtol(test_rhs, s, rtol=1e-10, precision=_abi.PREC_F64)
-    print("ablation", it_trained, it_untrained, pcg["iterations"])
-    assert it_trained["outer_iterations"] == 1  # no fallback needed
-    assert it_trained["iterations"] < it_untrained["iterations"]
-    assert it_trained["iterations"] < pcg["iterations"]
-    pc.close()
+    pcg = E.solve_rtol(W.forc, s, rtol=1e-10, precision=_abi.PREC_F64)
+    print("ablation iterations: trained", trained["iterations"], "untrained", untrained["iterations"], "pcg",
+          pcg["iterations"])
+    assert trained["outer_iterations"] == 1  # converged without the Jacobi-PCG fallback
+    assert trained["iterations"] < 0.8 * untrained["iterations"]
+    assert trained["iterations"] < 0.8 * pcg["iterations"]
