@@ -145,6 +145,18 @@ int32_t pyomgpu_set_sync_timeout(pyomgpu_ctx* ctx, double seconds);
  * context stays usable).  Cleared after that launch. */
 int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* ctx, int32_t enable);
 
+/* Autotuner of the solve kernel: times `iterations` iterations of the
+ * Jacobi-PCG kernel on this grid (a fixed pseudo-random right-hand side) for
+ * every tile shape tx x ty in {32,64,96,128} x {8,16,24,32} and every
+ * co-resident grid size that changes the busiest block's tile count, and
+ * keeps the fastest for all later streamfunction solves of the context
+ * (congrad_streamfunction, solve_rtol F64, solve_streamfunction, the
+ * learned solver's fallback).  Reduction order follows the tiling, so results
+ * change at rounding level (iteration counts within one).  Outputs may be
+ * NULL.  Not in the reference. */
+int32_t pyomgpu_autotune(pyomgpu_ctx* ctx, int32_t iterations, int32_t* tile_x, int32_t* tile_y, int32_t* grid,
+                         double* us_per_iteration, pyomgpu_stream stream);
+
 /* ---- islands (streamfct_init.f90, island_module.f90) ------------------------ */
 /* isleperim on a (imt,jmt) int map; map, nippts (>= mnisle entries) host.
  * Limits default to the reference's (mnisle 1000, maxipp 20000, maxq 10000)

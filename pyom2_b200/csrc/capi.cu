@@ -105,13 +105,17 @@ int run_cg_ref(pyomgpu_ctx* c, bool surf_press, const double* forc_dev, double e
   CGRefParams P{};
   P.g = c->g;
   P.op = op.dev();
-  if (encode_tile_map(&P.map_res, c->res, c->g) || encode_tile_map(&P.map_W, op.W, c->g) ||
-      encode_tile_map(&P.map_FX, op.FX, c->g) || encode_tile_map(&P.map_FY, op.FY, c->g) ||
-      encode_tile_map(&P.map_s[0], c->s0, c->g) || encode_tile_map(&P.map_s[1], c->s1, c->g))
+  const int tx = c->tune.done ? c->tune.tx : kTileX, ty = c->tune.done ? c->tune.ty : kTileY;
+  const int bx = tx + 4, by = ty + 2;
+  if (encode_tile_map(&P.map_res, c->res, c->g, bx, by) || encode_tile_map(&P.map_W, op.W, c->g, bx, by) ||
+      encode_tile_map(&P.map_FX, op.FX, c->g, bx, by) || encode_tile_map(&P.map_FY, op.FY, c->g, bx, by) ||
+      encode_tile_map(&P.map_s[0], c->s0, c->g, bx, by) || encode_tile_map(&P.map_s[1], c->s1, c->g, bx, by))
     return fail(PYOMGPU_ECUDA, "cuTensorMapEncodeTiled failed");
-  P.ntx = (c->nx + kTileX - 1) / kTileX;
-  P.nty = (c->ny + kTileY - 1) / kTileY;
-  const int grid = std::max(1, std::min(c->max_blocks, P.ntx * P.nty));
+  P.tx = tx;
+  P.ty = ty;
+  P.ntx = (c->nx + tx - 1) / tx;
+  P.nty = (c->ny + ty - 1) / ty;
+  const int grid = c->tune.done ? c->tune.grid : std::max(1, std::min(c->max_blocks, P.ntx * P.nty));
   P.forc = forc_dev;
   P.sol = c->sol;
   P.res = c->res;
@@ -129,7 +133,8 @@ int run_cg_ref(pyomgpu_ctx* c, bool surf_press, const double* forc_dev, double e
   P.out = c->d_result;
   void* args[] = {&P};
   CK(cudaEventRecord(c->e0, st));
-  CK(cudaLaunchCooperativeKernel(cg_ref_kernel_ptr(surf_press), dim3(grid), dim3(kCGThreads), args, kCGSmem, st));
+  CK(cudaLaunchCooperativeKernel(cg_ref_kernel_ptr(surf_press), dim3(grid), dim3(kCGThreads), args,
+                                 cg_smem_bytes(tx, ty), st));
   CK(cudaEventRecord(c->e1, st));
   CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
   int err = 0;
@@ -726,9 +731,9 @@ int32_t pyomgpu_ctx_create(const pyomgpu_grid* gr, pyomgpu_ctx** out) {
     return bail(fail(PYOMGPU_ECUDA, "memset"));
   int per_sm = 0;
   for (bool sp : {false, true})
-    if (cudaFuncSetAttribute(cg_ref_kernel_ptr(sp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmem) !=
-        cudaSuccess)
-      return bail(fail(PYOMGPU_ECUDA, "cannot reserve %zu bytes of shared memory", kCGSmem));
+    if (cudaFuncSetAttribute(cg_ref_kernel_ptr(sp), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kCGSmemMax) != cudaSuccess)
+      return bail(fail(PYOMGPU_ECUDA, "cannot reserve %zu bytes of shared memory", kCGSmemMax));
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_ref_kernel_ptr(false), kCGThreads, kCGSmem) !=
           cudaSuccess ||
       per_sm < 1)
@@ -762,6 +767,56 @@ int32_t pyomgpu_set_sync_timeout(pyomgpu_ctx* c, double seconds) {
 int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* c, int32_t enable) {
   if (!c) return fail(PYOMGPU_EINVAL, "null context");
   c->stall_next = enable ? 1u : 0u;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_autotune(pyomgpu_ctx* c, int32_t iterations, int32_t* tile_x, int32_t* tile_y, int32_t* grid,
+                         double* us_per_iteration, pyomgpu_stream stream) {
+  if (!c || iterations < 10) return fail(PYOMGPU_EINVAL, "autotune: bad arguments");
+  if (!c->have_islands) return fail(PYOMGPU_ESTATE, "autotune: set up the islands first");
+  cudaStream_t st = (cudaStream_t)stream;
+  launch_fill_pseudorandom(c->stage_a, c->n2, 12345u, st);  // a fixed right-hand side with all scales
+  const size_t bytes = c->g.size() * sizeof(double);
+  struct Cand {
+    int tx, ty, grid;
+  };
+  std::vector<Cand> cands;
+  for (int tx : {32, 64, 96, 128})
+    for (int ty : {8, 16, 24, 32}) {
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_ref_kernel_ptr(false), kCGThreads,
+                                                        cg_smem_bytes(tx, ty)) != cudaSuccess ||
+          per_sm < 1)
+        continue;
+      const int maxb = std::min(per_sm * c->nsm, c->max_blocks);
+      const int ntiles = ((c->nx + tx - 1) / tx) * ((c->ny + ty - 1) / ty);
+      const int g1 = std::min(maxb, ntiles);
+      cands.push_back({tx, ty, g1});
+      const int per = (ntiles + maxb - 1) / maxb;  // tiles of the busiest block
+      const int g2 = (ntiles + per - 1) / per;     // fewest blocks with the same busiest load
+      if (g2 != g1 && g2 >= 1) cands.push_back({tx, ty, g2});
+    }
+  pyomgpu_ctx::Tune best{};
+  best.us_per_it = 1e300;
+  for (int pass = 0; pass < 2; ++pass)  // every candidate twice, the faster run counts
+    for (const Cand& k : cands) {
+      c->tune = pyomgpu_ctx::Tune{true, k.tx, k.ty, k.grid, 0.0};
+      CK(cudaMemsetAsync(c->sol, 0, bytes, st));
+      pyomgpu_solve_info info{};
+      int rc = run_cg_ref(c, false, c->stage_a, 0.0, iterations, 0.0, &info, st);
+      if (rc < 0 || rc == PYOMGPU_TIMEOUT) {
+        c->tune = pyomgpu_ctx::Tune{};
+        return rc;
+      }
+      if (info.iterations < 1) continue;
+      const double us = 1e3 * info.device_ms / info.iterations;
+      if (us < best.us_per_it) best = pyomgpu_ctx::Tune{true, k.tx, k.ty, k.grid, us};
+    }
+  c->tune = best.done ? best : pyomgpu_ctx::Tune{};
+  if (tile_x) *tile_x = c->tune.done ? c->tune.tx : kTileX;
+  if (tile_y) *tile_y = c->tune.done ? c->tune.ty : kTileY;
+  if (grid) *grid = c->tune.grid;
+  if (us_per_iteration) *us_per_iteration = c->tune.us_per_it;
   return PYOMGPU_OK;
 }
 

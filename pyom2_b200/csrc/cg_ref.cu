@@ -29,19 +29,23 @@
 namespace pyomgpu {
 
 __device__ __forceinline__ void tile_origin(const CGRefParams& P, int t, int& i0, int& j0) {
-  i0 = 1 + kTileX * (t % P.ntx);
-  j0 = 1 + kTileY * (t / P.ntx);
+  i0 = 1 + P.tx * (t % P.ntx);
+  j0 = 1 + P.ty * (t / P.ntx);
 }
 
 template <bool SP>
 __global__ void __launch_bounds__(kCGThreads, 3) cg_ref_kernel(const __grid_constant__ CGRefParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
+  const int TX = P.tx, TY = P.ty, BX = TX + 4, BY = TY + 2;
+  constexpr int kCGWarps = kCGThreads / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t tb = cg_box_bytes(TX, TY);
   double* tres = reinterpret_cast<double*>(smem);
-  double* tW = reinterpret_cast<double*>(smem + kTileBytes);
-  double* ts = reinterpret_cast<double*>(smem + 2 * kTileBytes);
-  double* tFX = reinterpret_cast<double*>(smem + 3 * kTileBytes);
-  double* tFY = reinterpret_cast<double*>(smem + 4 * kTileBytes);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 5 * kTileBytes);
+  double* tW = reinterpret_cast<double*>(smem + tb);
+  double* ts = reinterpret_cast<double*>(smem + 2 * tb);
+  double* tFX = reinterpret_cast<double*>(smem + 3 * tb);
+  double* tFY = reinterpret_cast<double*>(smem + 4 * tb);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 5 * tb);
 
   const Geo g = P.g;
   const OpDev<double> op = P.op;
@@ -68,8 +72,8 @@ __global__ void __launch_bounds__(kCGThreads, 3) cg_ref_kernel(const __grid_cons
     for (int t = blockIdx.x; t < ntiles; t += nb) {
       int i0, j0;
       tile_origin(P, t, i0, j0);
-      for (int e = threadIdx.x; e < kTileX * kTileY; e += kCGThreads) {
-        const int i = i0 + e % kTileX, j = j0 + e / kTileX;
+      for (int e = threadIdx.x; e < TX * TY; e += kCGThreads) {
+        const int i = i0 + e % TX, j = j0 + e / TX;
         if (i > g.nx || j > g.ny) continue;
         const double f = P.forc[fidx(g.nx, i, j)];
         const double r = f - apply_point(op, g, sol, i, j);
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(kCGThreads, 3) cg_ref_kernel(const __grid_cons
         if (threadIdx.x == 0) {
           fence_proxy_async_smem();
           fence_proxy_async_global();
-          mbar_arrive_expect_tx(bar, 5u * kBoxX * kBoxY * 8u);
+          mbar_arrive_expect_tx(bar, 5u * (unsigned)(BX * BY) * 8u);
           const int ex = i0 + 1, ey = j0;  // padded element column of Fortran i0-2, row of j0-1
           tma_load_2d(tres, &P.map_res, ex, ey, bar);
           tma_load_2d(tW, &P.map_W, ex, ey, bar);
@@ -178,21 +182,22 @@ __global__ void __launch_bounds__(kCGThreads, 3) cg_ref_kernel(const __grid_cons
           if (threadIdx.x == 0) atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
           return;
         }
-        // direction on the tile and its one-cell halo: box columns 1..kBoxX-2, all rows
-        for (int e = threadIdx.x; e < (kBoxX - 2) * kBoxY; e += kCGThreads) {
-          const int k = (e / (kBoxX - 2)) * kBoxX + 1 + e % (kBoxX - 2);
-          const double w1 = SP ? 1.0 : tW[k];
-          ts[k] = w1 * tres[k] + bq * ts[k];
-        }
+        // direction on the tile and its one-cell halo: box columns 1..BX-2, all rows
+        // (rows to warps, columns to lanes: no division by the run-time tile width)
+        for (int rr = warp; rr < BY; rr += kCGWarps)
+          for (int k = rr * BX + 1 + lane; k < rr * BX + BX - 1; k += 32) {
+            const double w1 = SP ? 1.0 : tW[k];
+            ts[k] = w1 * tres[k] + bq * ts[k];
+          }
         __syncthreads();
-        for (int e = threadIdx.x; e < kTileX * kTileY; e += kCGThreads) {
-          const int c = e % kTileX, r = e / kTileX;
+        for (int r = warp; r < TY; r += kCGWarps)
+          for (int c = lane; c < TX; c += 32) {
           const int i = i0 + c, j = j0 + r;
           if (i > g.nx || j > g.ny) continue;
-          const int k = (r + 1) * kBoxX + c + 2;
+          const int k = (r + 1) * BX + c + 2;
           const double sc = ts[k];
           double a = op.ax[i + 1] * op.bx[j + 1] * (tFX[k + 1] * (ts[k + 1] - sc) + tFX[k] * (ts[k - 1] - sc)) +
-                     op.by[j + 1] * (tFY[k + kBoxX] * (ts[k + kBoxX] - sc) + tFY[k] * (ts[k - kBoxX] - sc));
+                     op.by[j + 1] * (tFY[k + BX] * (ts[k + BX] - sc) + tFY[k] * (ts[k - BX] - sc));
           const double w = tW[k];
           if (SP) a += op.dcoef * w * sc;
           store_cyclic(sn, g, i, j, sc);
@@ -287,8 +292,9 @@ __global__ void __launch_bounds__(kCGThreads, 3) cg_ref_kernel(const __grid_cons
       for (int t = blockIdx.x; t < ntiles; t += nb) {
         int i0, j0;
         tile_origin(P, t, i0, j0);
-        for (int e = threadIdx.x; e < kTileX * kTileY; e += kCGThreads) {
-          const int i = i0 + e % kTileX, j = j0 + e / kTileX;
+        for (int r = warp; r < TY; r += kCGWarps)
+          for (int c = lane; c < TX; c += 32) {
+          const int i = i0 + c, j = j0 + r;
           if (i > g.nx || j > g.ny) continue;
           const size_t q = g.at(i, j);
           const double sc = sn[q];
@@ -395,12 +401,12 @@ EncodeTiledFn tiled_encoder() {
 }
 }  // namespace
 
-int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g) {
+int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g, int box_x, int box_y) {
   EncodeTiledFn fn = tiled_encoder();
   if (!fn) return -1;
   const cuuint64_t dims[2] = {(cuuint64_t)g.pitch, (cuuint64_t)(g.ny + 2 * kOnx)};
   const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)kBoxX, (cuuint32_t)kBoxY};
+  const cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)box_y};
   const cuuint32_t es[2] = {1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

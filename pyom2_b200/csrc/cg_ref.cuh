@@ -9,9 +9,16 @@
 namespace pyomgpu {
 
 constexpr int kCGThreads = 256;
-// shared memory: five kBoxX x kBoxY FP64 tiles (128-byte aligned) + the mbarrier
-constexpr size_t kTileBytes = ((size_t)kBoxX * kBoxY * 8 + 127) / 128 * 128;
-constexpr size_t kCGSmem = 5 * kTileBytes + 128;
+// Tile shape is a launch parameter (tx x ty interior points, box (tx+4) x
+// (ty+2)); tx even so every box starts on a 16-byte boundary.  Shared memory:
+// five boxes (128-byte aligned) + the mbarrier.
+constexpr int kCGMaxTX = 128, kCGMaxTY = 32;
+__host__ __device__ constexpr size_t cg_box_bytes(int tx, int ty) {
+  return ((size_t)(tx + 4) * (ty + 2) * 8 + 127) / 128 * 128;
+}
+__host__ __device__ constexpr size_t cg_smem_bytes(int tx, int ty) { return 5 * cg_box_bytes(tx, ty) + 128; }
+constexpr size_t kCGSmem = cg_smem_bytes(kTileX, kTileY);        // default tile
+constexpr size_t kCGSmemMax = cg_smem_bytes(kCGMaxTX, kCGMaxTY);  // attribute reserved once
 
 struct CGResult {
   int iterations;
@@ -34,7 +41,8 @@ struct alignas(64) CGRefParams {
   double eps;          // congr_epsilon
   int max_it;          // congr_max_iterations
   double rtol;         // > 0: extra stop on ||res||/||forc|| over the unknowns
-  int ntx, nty;        // tiles in x and y (kTileX x kTileY interior points each)
+  int tx, ty;          // tile shape (interior points)
+  int ntx, nty;        // tiles in x and y
   SyncCtl* ctl;
   double* slots;       // 2 * gridDim.x * 4 doubles
   unsigned long long timeout_ns;

@@ -81,6 +81,13 @@ struct pyomgpu_ctx {
     std::vector<void*> owned;
   } fast;
 
+  // tile shape and grid of cg_ref_kernel chosen by pyomgpu_autotune (default 64x16, all co-resident blocks)
+  struct Tune {
+    bool done = false;
+    int tx = 0, ty = 0, grid = 0;
+    double us_per_it = 0;
+  } tune;
+
   // work-queue batch (pyomgpu_congrad_streamfunction_batch and the psin
   // solves); grows to the largest batch run through this context
   struct Batch {

@@ -554,6 +554,23 @@ void launch_setcyclic_user(const Geo& g, double* user, cudaStream_t st) {
   if (g.cyclic_y) k_setcyclic_user_y<<<nblk(g.nx + 4, 128), 128, 0, st>>>(g.nx, g.ny, user);
 }
 
+__global__ void k_fill_pseudorandom(double* __restrict__ a, size_t n, uint32_t seed) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    // 32-bit integer mix of (k, seed); the top 31 bits give a uniform value in [-1, 1)
+    uint32_t h = (uint32_t)k * 0x9E3779B1u ^ seed;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    a[k] = (double)(h >> 1) * (2.0 / 2147483648.0) - 1.0;
+  }
+}
+
+void launch_fill_pseudorandom(double* a, size_t n, uint32_t seed, cudaStream_t st) {
+  k_fill_pseudorandom<<<std::min<size_t>(nblk(n, 256), 4096), 256, 0, st>>>(a, n, seed);
+}
+
 void launch_to_f32(const double* a, float* b, size_t n, cudaStream_t st) {
   k_to_f32<<<std::min<size_t>(nblk(n, 256), 4096), 256, 0, st>>>(a, b, n);
 }

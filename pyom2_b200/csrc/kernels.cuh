@@ -69,6 +69,9 @@ void launch_island_solve(int nisle, const double* lu, const int* ipiv, const dou
 void launch_residual(const Geo& g, const OpDev<double>& op, const double* forc_user, const double* sol_padded,
                      double* part, int nb, double* out2, cudaStream_t st);
 
+// a[k] = a deterministic pseudo-random value in [-1, 1) (integer hash of k and seed)
+void launch_fill_pseudorandom(double* a, size_t n, uint32_t seed, cudaStream_t st);
+
 // mixed precision helpers
 void launch_to_f32(const double* a, float* b, size_t n, cudaStream_t st);
 // b32 = s (forc - A x) at the unknowns (W != 0), zero elsewhere (x padded with valid halo)

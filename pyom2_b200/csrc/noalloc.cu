@@ -129,8 +129,8 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
   // launch shape: the same rule as the context path, so results match it bit for bit
   int dev = 0, nsm = 0, o1 = 0, o2 = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) ||
-      cudaFuncSetAttribute(cg_ref_kernel_ptr(false), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmem) ||
-      cudaFuncSetAttribute(cg_ref_kernel_ptr(true), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmem) ||
+      cudaFuncSetAttribute(cg_ref_kernel_ptr(false), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmemMax) ||
+      cudaFuncSetAttribute(cg_ref_kernel_ptr(true), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCGSmemMax) ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, cg_ref_kernel_ptr(false), kCGThreads, kCGSmem) ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, cg_ref_kernel_ptr(true), kCGThreads, kCGSmem) || o1 < 1)
     return nfail(PYOMGPU_ECUDA, "device query failed");
@@ -182,6 +182,8 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
       encode_tile_map(&Pm.map_FX, op.FX, g) || encode_tile_map(&Pm.map_FY, op.FY, g) ||
       encode_tile_map(&Pm.map_s[0], s0, g) || encode_tile_map(&Pm.map_s[1], s1, g))
     return nfail(PYOMGPU_ECUDA, "cuTensorMapEncodeTiled failed");
+  Pm.tx = kTileX;
+  Pm.ty = kTileY;
   Pm.ntx = (g.nx + kTileX - 1) / kTileX;
   Pm.nty = (g.ny + kTileY - 1) / kTileY;
   const int grid = std::max(1, std::min(max_blocks, Pm.ntx * Pm.nty));

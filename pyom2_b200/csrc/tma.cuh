@@ -73,8 +73,8 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
 }
 
 // Host: tensor map of a padded FP64 field ((ny+4) rows of `pitch` elements)
-// with a kBoxX x kBoxY box.  Returns 0 or a CUDA driver error code.
-int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g);
+// with a box_x x box_y box.  Returns 0 or a CUDA driver error code.
+int encode_tile_map(CUtensorMap* map, const double* base, const Geo& g, int box_x = kBoxX, int box_y = kBoxY);
 
 // Host: general tiled tensor map (no swizzle, zero fill out of bounds).
 // dims[0] is the contiguous dimension; strides_bytes has rank-1 entries.

@@ -135,6 +135,14 @@ class ExternalMode:
     def set_sync_timeout(self, seconds: float):
         _abi.check(self._L.pyomgpu_set_sync_timeout(self._ctx, float(seconds)))
 
+    def autotune(self, iterations: int = 200):
+        """Pick the solve kernel's tile shape and grid for this grid by timing
+        candidates on the GPU; returns (tile_x, tile_y, grid, us_per_iteration)."""
+        tx, ty, gr, us = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        _abi.check(self._L.pyomgpu_autotune(self._ctx, int(iterations), C.byref(tx), C.byref(ty), C.byref(gr),
+                                            C.byref(us), _stream()))
+        return tx.value, ty.value, gr.value, us.value
+
     def inject_barrier_stall(self, enable: bool = True):
         """Failure-detection test hook: the next solve's first grid barrier
         can never complete, so it ends with PYOMGPU_TIMEOUT."""

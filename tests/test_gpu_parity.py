@@ -86,6 +86,27 @@ def test_congrad_streamfunction(oracle_lib, name):
     assert np.array_equal(sg[:2], so[:2]) or rel(sg[:2], so[:2]) < RTOL_SOL
 
 
+def test_autotuned_kernel_matches_oracle(oracle_lib):
+    """After the autotuner picks a tile shape and grid, congrad_streamfunction
+    still follows the oracle (solution to 1e-10, iterations within one) and
+    solve_rtol still reaches the 1e-10 true residual."""
+    W, Mg, Mo, O, E, _ = setup("cyclic200", oracle_lib)
+    tx, ty, grid, us = E.autotune(iterations=50)
+    assert tx in (32, 64, 96, 128) and ty in (8, 16, 24, 32) and grid >= 1 and us > 0
+    cf = O.make_coeff_streamfunction()
+    rng = np.random.default_rng(2)
+    sol0 = np.asfortranarray(rng.standard_normal(Mg.shape2d) * 1e3)
+    so = sol0.copy(order="F")
+    ro = O.congrad_streamfunction(cf, W.forc, so)
+    sg = sol0.copy(order="F")
+    it, conv, info = E.congrad_streamfunction(W.forc, sg)
+    assert conv == ro["converged"] and abs(it - ro["iterations"]) <= 1
+    assert rel(sg, so) < RTOL_SOL
+    s2 = np.zeros(Mg.shape2d, order="F")
+    info = E.solve_rtol(W.forc, s2, rtol=1e-10, precision=_abi.PREC_F64)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10
+
+
 def test_congrad_torch_in_place(oracle_lib):
     import torch
     W, Mg, Mo, O, E, _ = setup("cyclic96", oracle_lib)
