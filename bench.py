@@ -155,7 +155,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def c2_batch(steps, warmup):
+def c2_batch(steps, warmup, count=64):
     """Config 2: 64 closed basins (128-1024 x 128-768, 10-40 % land, 0-12
     islands), each solved to FP64 relative residual 1e-10 from zero: all 64 in
     one work-queue launch (congrad_streamfunction_batch) against 64
@@ -166,7 +166,7 @@ def c2_batch(steps, warmup):
     from pyom2_b200 import _abi, synth
     from pyom2_b200.external import ExternalMode, congrad_streamfunction_batch
 
-    ws = synth.config2()
+    ws = synth.config2(count=count)
     ems = []
     for w in ws:
         E = ExternalMode(w.M)
@@ -225,6 +225,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default 64x16 tiles of the solve kernel")
     ap.add_argument("--with-c2", action="store_true",
                     help="also time config 2 (64 basins in one work-queue launch vs 64 sequential solves)")
+    ap.add_argument("--c2-count", type=int, default=64, help="basins of config 2 (fewer for profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
@@ -365,7 +366,7 @@ def main():
                                      "pcg64_iterations": results["pcg64"]["iterations"],
                                      "speedup": results["pcg64"]["value"] / results["fcg"]["value"]}
     if args.with_c2 and rank == 0:
-        out["c2_batch"] = c2_batch(max(1, args.steps // 3), 1)
+        out["c2_batch"] = c2_batch(max(1, args.steps // 3), 1, args.c2_count)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(W, results.get("pcg64", R)["iterations"])
     if rank == 0:

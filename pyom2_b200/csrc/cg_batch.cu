@@ -218,7 +218,7 @@ __device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kBatchThreads, 3) cg_batch_kernel(const BatchParams P) {
+__global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchParams P) {
   __shared__ double b_s[kBoxN], b_FX[kBoxN], b_FY[kBoxN];
   unsigned long long epoch = 0;
 
