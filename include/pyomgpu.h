@@ -19,6 +19,10 @@
  *   line_integral              streamfct_init.f90:311   pyomgpu_line_integral
  *   solve_streamfunction       solve_streamfct.f90:10   pyomgpu_solve_streamfunction
  *   solve_pressure             solve_pressure.f90:10    pyomgpu_solve_pressure
+ *   make_coeff_non_hydro       non_hydrostatic.f90:70   pyomgpu_nh_create (operator kept, like the SAVE'd cf)
+ *   congrad_non_hydro          non_hydrostatic.f90:146  pyomgpu_congrad_non_hydro
+ *   apply_op_3D                non_hydrostatic.f90:247  pyomgpu_apply_op_3d
+ *   dot_3D/absmax_3D           non_hydrostatic.f90:279-322 (fused into the CG kernel)
  *
  * Array conventions: every 2-D field has the Fortran extents of
  * main_module.f90 for one PE, (1-onx:nx+onx, 1-onx:ny+onx) with onx = 2, in
@@ -273,6 +277,49 @@ int32_t pyomgpu_solve_streamfunction(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgp
 /* solve_pressure (solve_pressure.f90:10-82) on device-resident model arrays. */
 int32_t pyomgpu_solve_pressure(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_solve_info* info,
                                pyomgpu_stream stream);
+
+/* ---- non-hydrostatic pressure (non_hydrostatic.f90) --------------------------- */
+/* Grid of the 3-D solve: main_module arrays, host pointers, Fortran order.
+ * Masks hold only 0 and 1 (as calc_topo builds them, numerics.f90:187-249);
+ * maskW(:,:,k) = min(maskT(:,:,k), maskT(:,:,k+1)) for k < nz. */
+typedef struct pyomgpu_grid3d {
+  int32_t nx, ny, nz;          /* nx >= 4, ny >= 1, nz >= 2 */
+  int32_t onx;                 /* halo width; must be 2 */
+  int32_t enable_cyclic_x, enable_cyclic_y;
+  const double *dxt, *dxu;     /* [nx+4] */
+  const double *dyt, *dyu;     /* [ny+4] */
+  const double *cost, *cosu;   /* [ny+4] */
+  const double *dzt, *dzw;     /* [nz] */
+  const double *maskT, *maskU, *maskV, *maskW; /* (nx+4, ny+4, nz) */
+} pyomgpu_grid3d;
+typedef struct pyomgpu_nh pyomgpu_nh;
+
+/* Builds the operator of make_coeff_non_hydro (non_hydrostatic.f90:70-138)
+ * on the current device, in compact form: one flag byte per cell (its face
+ * masks and maskT) and the metric factors as 2-D/1-D tables.  Applying it is
+ * bit-identical to apply_op_3D with the reference's 27-entry cf. */
+int32_t pyomgpu_nh_create(const pyomgpu_grid3d* grid, pyomgpu_nh** out);
+void pyomgpu_nh_destroy(pyomgpu_nh* nh);
+/* Device-side time limit of every grid-barrier wait (default 2 s). */
+int32_t pyomgpu_nh_set_sync_timeout(pyomgpu_nh* nh, double seconds);
+/* Failure-detection test hook, as pyomgpu_inject_barrier_stall. */
+int32_t pyomgpu_nh_inject_barrier_stall(pyomgpu_nh* nh, int32_t enable);
+/* Blocks of the CG launch (0 = one 8-warp block per 256 cells' worth of
+ * 32-cell rows, capped at the co-resident maximum).  Reduction order follows
+ * the grid, so results change at rounding level. */
+int32_t pyomgpu_nh_set_grid(pyomgpu_nh* nh, int32_t blocks);
+/* res = A p1 over the interior, zero halo (apply_op_3D).  (nx+4, ny+4, nz)
+ * Fortran-layout arrays, host or device. */
+int32_t pyomgpu_apply_op_3d(pyomgpu_nh* nh, const double* p1, double* res, pyomgpu_stream stream);
+/* congrad_non_hydro (non_hydrostatic.f90:146-242): plain FP64 CG with
+ * maskT-weighted dot_3D/absmax_3D, the reference's stopping estimate and
+ * divergence test.  forc (read) and p = p_non_hydro(:,:,:,taup1) (in/out,
+ * halo updated as the reference's whole-array update does) are Fortran-layout
+ * (nx+4, ny+4, nz), host or device.  eps = congr_epsilon_non_hydro, max_it =
+ * congr_max_itts_non_hydro; info->iterations = congr_itts_non_hydro.  An
+ * immediate stop (zero initial residual) reports 0 iterations. */
+int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* nh, const double* forc, double* p, double eps, int32_t max_it,
+                                  pyomgpu_solve_info* info, pyomgpu_stream stream);
 
 /* ---- learned preconditioner (no counterpart in the reference) ----------------- */
 /* Building block of the U-Net preconditioner: one 3x3 convolution (stride 1,

@@ -38,6 +38,11 @@ class OGrid(C.Structure):
                 ("cost", C.c_void_p), ("cosu", C.c_void_p)]
 
 
+class OGrid3(C.Structure):
+    _fields_ = [("g", OGrid), ("nz", C.c_int), ("dzt", C.c_void_p), ("dzw", C.c_void_p), ("maskT", C.c_void_p),
+                ("maskU", C.c_void_p), ("maskV", C.c_void_p), ("maskW", C.c_void_p)]
+
+
 class OIslands(C.Structure):
     _fields_ = [("nisle", C.c_int), ("max_boundary", C.c_int), ("boundary", C.c_void_p),
                 ("line_dir", C.c_void_p), ("nr_boundary", C.c_void_p)]
@@ -93,6 +98,12 @@ def lib():
             "o_dgesv": (i, [i, p, p, p]),
             "o_solve_streamfunction": (i, [p, p, p, p]),
             "o_solve_pressure": (i, [p, p, p]),
+            "o_setcyclic_xyz": (v, [p, p]),
+            "o_make_coeff_non_hydro": (v, [p, p]),
+            "o_apply_op_3d": (v, [p, p, p, p]),
+            "o_dot_3d": (d, [p, p, p]),
+            "o_absmax_3d": (d, [p, p]),
+            "o_congrad_non_hydro": (i, [p, p, p, p, d, i, p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(_lib, name)
@@ -301,3 +312,49 @@ class Oracle:
         rc = lib().o_solve_pressure(self.gp, _p(cf), C.byref(s))
         M.congr_itts = s.congr_itts
         return rc
+
+
+class Oracle3D:
+    """Oracle of the non-hydrostatic pressure solve (non_hydrostatic.f90) bound
+    to one model state (3-D fields (nx+4, ny+4, nz), Fortran order)."""
+
+    def __init__(self, M):
+        if M.nz < 2:
+            raise ValueError("make_coeff_non_hydro reads maskW(:,:,nz-1): nz >= 2")
+        self.M = M
+        self.o2 = Oracle(M)
+        self._keep = [np.ascontiguousarray(M.dzt), np.ascontiguousarray(M.dzw)] + \
+            [np.asfortranarray(getattr(M, n)) for n in ("maskT", "maskU", "maskV", "maskW")]
+        k = self._keep
+        self.g = OGrid3(self.o2.g, M.nz, *[_p(a) for a in k])
+        self.gp = C.byref(self.g)
+        self.shape = M.shape2d + (M.nz,)
+
+    def make_coeff(self):
+        cf = np.zeros(self.shape + (3, 3, 3), order="F")
+        lib().o_make_coeff_non_hydro(self.gp, _p(cf))
+        return cf
+
+    def apply_op(self, cf, p):
+        res = np.zeros(self.shape, order="F")
+        lib().o_apply_op_3d(self.gp, _p(cf), _p(_f64(p)), _p(res))
+        return res
+
+    def dot(self, a, b):
+        return lib().o_dot_3d(self.gp, _p(_f64(a)), _p(_f64(b)))
+
+    def absmax(self, a):
+        return lib().o_absmax_3d(self.gp, _p(_f64(a)))
+
+    def setcyclic_xyz(self, a):
+        lib().o_setcyclic_xyz(self.gp, _p(_f64(a)))
+
+    def congrad(self, cf, forc, p, eps=None, max_it=None):
+        """congrad_non_hydro in place on ``p`` (p_non_hydro(:,:,:,taup1))."""
+        M = self.M
+        info = OInfo()
+        lib().o_congrad_non_hydro(self.gp, _p(cf), _p(_f64(forc)), _p(_f64(p)),
+                                  float(M.congr_epsilon_non_hydro if eps is None else eps),
+                                  int(M.congr_max_itts_non_hydro if max_it is None else max_it), C.byref(info))
+        return dict(iterations=info.iterations, converged=bool(info.converged), status=info.status,
+                    estimated_error=info.estimated_error)

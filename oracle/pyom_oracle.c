@@ -1113,3 +1113,175 @@ int o_solve_pressure(const o_grid *g, const double *cf, o_state *s) {
   free(forc);
   return st;
 }
+
+/* ------------------------------------------------------------------------- */
+/* non_hydrostatic.f90: make_coeff_non_hydro, apply_op_3D, dot_3D,            */
+/* absmax_3D, congrad_non_hydro                                               */
+/* ------------------------------------------------------------------------- */
+#define N3(g3) (N2(&(g3)->g) * (size_t)(g3)->nz)
+#define IX3(g3, i, j, k) (IX(&(g3)->g, i, j) + (size_t)((k)-1) * N2(&(g3)->g))
+#define CF3(g3, cf, i, j, k, ii, jj, kk) \
+  (cf)[IX3(g3, i, j, k) + (size_t)(((ii)-1) + 3 * (((jj)-1) + 3 * ((kk)-1))) * N3(g3)]
+
+/* setcyclic_xyz (parallel_none.f90): setcyclic_xy on every level */
+void o_setcyclic_xyz(const o_grid3 *g3, double *p) {
+  for (int k = 1; k <= g3->nz; k++) o_setcyclic_xy(&g3->g, p + (size_t)(k - 1) * N2(&g3->g));
+}
+
+/* non_hydrostatic.f90:70-138, same accumulation order */
+void o_make_coeff_non_hydro(const o_grid3 *g3, double *cf) {
+  const o_grid *g = &g3->g;
+  const int nx = g->nx, ny = g->ny, nz = g3->nz;
+  memset(cf, 0, N3(g3) * 27 * sizeof(double));
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        const double c2 = g->cost[Y1(g, j)] * g->cost[Y1(g, j)];
+        double mp = g3->maskU[IX3(g3, i, j, k)], mm = g3->maskU[IX3(g3, i - 1, j, k)];
+        CF3(g3, cf, i, j, k, 2, 2, 2) -= mp / g->dxu[X1(g, i)] / g->dxt[X1(g, i)] / c2;
+        CF3(g3, cf, i, j, k, 3, 2, 2) += mp / g->dxu[X1(g, i)] / g->dxt[X1(g, i)] / c2;
+        CF3(g3, cf, i, j, k, 2, 2, 2) -= mm / g->dxu[X1(g, i - 1)] / g->dxt[X1(g, i)] / c2;
+        CF3(g3, cf, i, j, k, 1, 2, 2) += mm / g->dxu[X1(g, i - 1)] / g->dxt[X1(g, i)] / c2;
+        mp = g3->maskV[IX3(g3, i, j, k)];
+        mm = g3->maskV[IX3(g3, i, j - 1, k)];
+        CF3(g3, cf, i, j, k, 2, 2, 2) -= mp / g->dyu[Y1(g, j)] / g->dyt[Y1(g, j)] * g->cosu[Y1(g, j)] / g->cost[Y1(g, j)];
+        CF3(g3, cf, i, j, k, 2, 3, 2) += mp / g->dyu[Y1(g, j)] / g->dyt[Y1(g, j)] * g->cosu[Y1(g, j)] / g->cost[Y1(g, j)];
+        CF3(g3, cf, i, j, k, 2, 2, 2) -=
+            mm / g->dyu[Y1(g, j - 1)] / g->dyt[Y1(g, j)] * g->cosu[Y1(g, j - 1)] / g->cost[Y1(g, j)];
+        CF3(g3, cf, i, j, k, 2, 1, 2) +=
+            mm / g->dyu[Y1(g, j - 1)] / g->dyt[Y1(g, j)] * g->cosu[Y1(g, j - 1)] / g->cost[Y1(g, j)];
+      }
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        if (k < nz) { /* k = 1 and 2..nz-1: the upper face */
+          const double mp = g3->maskW[IX3(g3, i, j, k)];
+          CF3(g3, cf, i, j, k, 2, 2, 2) -= mp / g3->dzw[k - 1] / g3->dzt[k - 1];
+          CF3(g3, cf, i, j, k, 2, 2, 3) += mp / g3->dzw[k - 1] / g3->dzt[k - 1];
+        }
+        if (k > 1) { /* 2..nz-1 and nz: the lower face */
+          const double mm = g3->maskW[IX3(g3, i, j, k - 1)];
+          CF3(g3, cf, i, j, k, 2, 2, 2) -= mm / g3->dzw[k - 2] / g3->dzt[k - 1];
+          CF3(g3, cf, i, j, k, 2, 2, 1) += mm / g3->dzw[k - 2] / g3->dzt[k - 1];
+        }
+      }
+}
+
+/* non_hydrostatic.f90:247-276: res = 0, then sum over (kk, jj, ii) outermost */
+void o_apply_op_3d(const o_grid3 *g3, const double *cf, const double *p1, double *res) {
+  const o_grid *g = &g3->g;
+  const int nz = g3->nz;
+  memset(res, 0, N3(g3) * sizeof(double));
+  for (int kk = -1; kk <= 1; kk++)
+    for (int jj = -1; jj <= 1; jj++)
+      for (int ii = -1; ii <= 1; ii++)
+        for (int k = 1; k <= nz; k++) {
+          const int kpkk = k + kk < 1 ? 1 : (k + kk > nz ? nz : k + kk);
+          for (int j = 1; j <= g->ny; j++)
+            for (int i = 1; i <= g->nx; i++)
+              res[IX3(g3, i, j, k)] =
+                  res[IX3(g3, i, j, k)] + CF3(g3, cf, i, j, k, ii + 2, jj + 2, kk + 2) * p1[IX3(g3, i + ii, j + jj, kpkk)];
+        }
+}
+
+/* non_hydrostatic.f90:300-322 */
+double o_dot_3d(const o_grid3 *g3, const double *p1, const double *p2) {
+  double s2 = 0;
+  for (int k = 1; k <= g3->nz; k++)
+    for (int j = 1; j <= g3->g.ny; j++)
+      for (int i = 1; i <= g3->g.nx; i++) {
+        const size_t q = IX3(g3, i, j, k);
+        s2 = s2 + p1[q] * p2[q] * g3->maskT[q];
+      }
+  return s2;
+}
+
+/* non_hydrostatic.f90:279-297 */
+double o_absmax_3d(const o_grid3 *g3, const double *p1) {
+  double s2 = 0;
+  for (int k = 1; k <= g3->nz; k++)
+    for (int j = 1; j <= g3->g.ny; j++)
+      for (int i = 1; i <= g3->g.nx; i++) {
+        const size_t q = IX3(g3, i, j, k);
+        s2 = fmax_f(fabs(p1[q] * g3->maskT[q]), s2);
+      }
+  return s2;
+}
+
+/* non_hydrostatic.f90:146-242; p is p_non_hydro(:,:,:,taup1), in/out.  An
+ * immediate stop (rsold == 0) reports 0 iterations (the reference leaves n
+ * undefined there). */
+int o_congrad_non_hydro(const o_grid3 *g3, const double *cf, const double *forc, double *p_nh, double eps, int max_it,
+                        o_info *info) {
+  const size_t n3 = N3(g3);
+  double *res = (double *)calloc(n3, sizeof(double));
+  double *p = (double *)calloc(n3, sizeof(double));
+  double *Ap = (double *)calloc(n3, sizeof(double));
+  double rsold, alpha, rsnew, fxa, step, step1 = 0, convergence_rate, estimated_error = 0, smax, rs_min = 0;
+  int n, status = 0, converged = 0;
+
+  o_apply_op_3d(g3, cf, p_nh, res);
+  for (int k = 1; k <= g3->nz; k++)
+    for (int j = 1; j <= g3->g.ny; j++)
+      for (int i = 1; i <= g3->g.nx; i++) res[IX3(g3, i, j, k)] = forc[IX3(g3, i, j, k)] - res[IX3(g3, i, j, k)];
+  memcpy(p, res, n3 * sizeof(double));
+  o_setcyclic_xyz(g3, p);
+  rsold = o_dot_3d(g3, res, res);
+  if (rsold == 0.0) {
+    n = 0;
+    goto normal_end;
+  }
+  for (n = 1; n <= max_it; n++) {
+    o_apply_op_3d(g3, cf, p, Ap);
+    fxa = o_dot_3d(g3, p, Ap);
+    if (fxa == 0.0) goto normal_end;
+    alpha = rsold / fxa;
+    for (size_t q = 0; q < n3; q++) p_nh[q] = p_nh[q] + alpha * p[q];
+    for (size_t q = 0; q < n3; q++) res[q] = res[q] - alpha * Ap[q];
+    rsnew = o_dot_3d(g3, res, res);
+    const double bq = rsnew / rsold;
+    for (size_t q = 0; q < n3; q++) p[q] = res[q] + bq * p[q];
+    o_setcyclic_xyz(g3, p);
+    rsold = rsnew;
+    if (n == 1) {
+      rs_min = fabs(rsnew);
+    } else if (n > 2) {
+      rs_min = fmin_f(rs_min, fabs(rsnew));
+      if (fabs(rsnew) > 100.0 * rs_min) {
+        status = 2;
+        goto error_end;
+      }
+    }
+    smax = o_absmax_3d(g3, p);
+    step = fabs(alpha) * smax;
+    if (n == 1) {
+      step1 = step;
+      estimated_error = step;
+      if (step < eps) goto normal_end;
+    } else if (step < eps) {
+      convergence_rate = exp(log(step / step1) / (double)(n - 1));
+      estimated_error = step * convergence_rate / (1.0 - convergence_rate);
+      if (estimated_error < eps) goto normal_end;
+    }
+  }
+  status = 1;
+  goto error_end;
+normal_end:
+  converged = 1;
+  status = 0;
+  goto done;
+error_end:
+  converged = 0;
+  if (estimated_error != estimated_error) status = 3;
+done:
+  if (info) {
+    info->iterations = n;
+    info->converged = converged;
+    info->status = status;
+    info->estimated_error = estimated_error;
+  }
+  free(res);
+  free(p);
+  free(Ap);
+  return status;
+}

@@ -101,6 +101,23 @@ int o_line_psin(const o_grid *g, const o_islands *isl, const double *psin, const
                 const double *maskU_top, const double *maskV_top, double *line_psin);
 int o_dgesv(int n, double *a, int *ipiv, double *b);
 
+/* ---- non-hydrostatic pressure (non_hydrostatic.f90) ---------------------------
+ * 3-D arrays are (nx+4, ny+4, nz) Fortran order; cf is (nx+4, ny+4, nz, 3, 3, 3). */
+typedef struct o_grid3 {
+  o_grid g;
+  int nz;
+  const double *dzt, *dzw;                       /* [nz] */
+  const double *maskT, *maskU, *maskV, *maskW;   /* (nx+4, ny+4, nz) */
+} o_grid3;
+
+void o_setcyclic_xyz(const o_grid3 *g, double *p);
+void o_make_coeff_non_hydro(const o_grid3 *g, double *cf);
+void o_apply_op_3d(const o_grid3 *g, const double *cf, const double *p1, double *res);
+double o_dot_3d(const o_grid3 *g, const double *p1, const double *p2);
+double o_absmax_3d(const o_grid3 *g, const double *p1);
+int o_congrad_non_hydro(const o_grid3 *g, const double *cf, const double *forc, double *p, double eps, int max_it,
+                        o_info *info);
+
 int o_solve_streamfunction(const o_grid *g, const double *cf, const o_islands *isl, o_state *s);
 int o_solve_pressure(const o_grid *g, const double *cf, o_state *s);
 

@@ -36,7 +36,10 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_conv3x3_bf16", "pyomgpu_precond_num_params", "pyomgpu_precond_create",
            "pyomgpu_precond_destroy", "pyomgpu_precond_rebind", "pyomgpu_precond_set_params", "pyomgpu_precond_get_params",
            "pyomgpu_precond_get_grads", "pyomgpu_precond_apply", "pyomgpu_precond_train_step",
-           "pyomgpu_unet_forward_backward", "pyomgpu_solve_fcg")
+           "pyomgpu_unet_forward_backward", "pyomgpu_solve_fcg",
+           "pyomgpu_nh_create", "pyomgpu_nh_destroy", "pyomgpu_nh_set_sync_timeout",
+           "pyomgpu_nh_inject_barrier_stall", "pyomgpu_nh_set_grid", "pyomgpu_apply_op_3d",
+           "pyomgpu_congrad_non_hydro")
 
 
 class PyOMGPUError(RuntimeError):
@@ -53,6 +56,14 @@ class Grid(C.Structure):
                 ("cost", C.c_void_p), ("cosu", C.c_void_p), ("hur", C.c_void_p), ("hvr", C.c_void_p),
                 ("hu", C.c_void_p), ("hv", C.c_void_p), ("maskT_top", C.c_void_p),
                 ("maskU_top", C.c_void_p), ("maskV_top", C.c_void_p)]
+
+
+class Grid3D(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("onx", C.c_int32),
+                ("enable_cyclic_x", C.c_int32), ("enable_cyclic_y", C.c_int32),
+                ("dxt", C.c_void_p), ("dxu", C.c_void_p), ("dyt", C.c_void_p), ("dyu", C.c_void_p),
+                ("cost", C.c_void_p), ("cosu", C.c_void_p), ("dzt", C.c_void_p), ("dzw", C.c_void_p),
+                ("maskT", C.c_void_p), ("maskU", C.c_void_p), ("maskV", C.c_void_p), ("maskW", C.c_void_p)]
 
 
 class Islands(C.Structure):
@@ -130,6 +141,13 @@ def load(path: str = LIB_PATH):
         "pyomgpu_precond_train_step": (i32, [vp, vp, vp, C.c_float, P(C.c_float), vp]),
         "pyomgpu_unet_forward_backward": (i32, [vp, vp, vp, vp, vp]),
         "pyomgpu_solve_fcg": (i32, [vp, vp, vp, vp, d, i32, P(SolveInfo), vp]),
+        "pyomgpu_nh_create": (i32, [P(Grid3D), P(vp)]),
+        "pyomgpu_nh_destroy": (None, [vp]),
+        "pyomgpu_nh_set_sync_timeout": (i32, [vp, d]),
+        "pyomgpu_nh_inject_barrier_stall": (i32, [vp, i32]),
+        "pyomgpu_nh_set_grid": (i32, [vp, i32]),
+        "pyomgpu_apply_op_3d": (i32, [vp, vp, vp, vp]),
+        "pyomgpu_congrad_non_hydro": (i32, [vp, vp, vp, d, i32, P(SolveInfo), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,0 +1,625 @@
+// Non-hydrostatic pressure solve on the GPU: congrad_non_hydro
+// (non_hydrostatic.f90:146-242) as one persistent, grid-synchronised kernel,
+// apply_op_3D (:247-276) as a stand-alone kernel, and their C ABI.
+//
+// Per CG iteration the kernel makes two sweeps over the cells, separated by
+// grid barriers that carry the reductions (dot_3D / absmax_3D, :279-322):
+//
+//   sweep A  s_n = res + bq s_{n-1} at each cell and its six neighbours
+//            (recomputed where needed, so s_n is never stored before it is
+//            complete), partial sums of (s_n, A s_n) and max|s_n| over maskT
+//   sweep B  the same s_n and A s_n again, then res -= alpha A s_n,
+//            p += alpha s_n; res and s_n go to the other buffer of their
+//            double-buffered pair; partial sums of (res, res)
+//
+// so an iteration streams 64 bytes per cell (read res and s twice, read and
+// write p, write res and s) and stores no A s vector.  The convergence test of
+// iteration n needs max|s_{n+1}|, so it runs after sweep A of iteration n+1,
+// exactly as the reference evaluates it after forming the new direction.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/pyomgpu.h"
+#include "cg_ref.cuh"
+#include "nonhydro.cuh"
+
+namespace pyomgpu {
+
+void set_last_error(const char* msg);
+
+namespace {
+
+__device__ __forceinline__ size_t fidx3(int nx, int ny, int i, int j, int k) {
+  return (size_t)(i + 1) + (size_t)(nx + 2 * kOnx) * ((size_t)(j + 1) + (size_t)(ny + 2 * kOnx) * (size_t)(k - 1));
+}
+
+// Cell of lane `lane` in work unit u: a run of 32 consecutive i on row (j,k).
+__device__ __forceinline__ void nh_unit(uint32_t u, uint32_t nch, uint32_t ny, int lane, int& i, int& j, int& k) {
+  const uint32_t row = u / nch;
+  const uint32_t ch = u - row * nch;
+  const uint32_t kk = row / ny;
+  j = (int)(row - kk * ny) + 1;
+  k = (int)kk + 1;
+  i = (int)(ch * 32u) + lane + 1;
+}
+
+__device__ __forceinline__ ptrdiff_t nh_off(const NHGeo& G, int di, int dj, int dk) {
+  return (ptrdiff_t)di + (ptrdiff_t)dj * G.g.pitch + (ptrdiff_t)dk * (ptrdiff_t)G.plane;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_constant__ NHParams P) {
+  const NHGeo G = P.G;
+  const NHOp op = P.op;
+  const int nx = G.g.nx;
+  const uint32_t ny = (uint32_t)G.g.ny;
+  const uint32_t nch = (uint32_t)(nx + 31) >> 5;
+  const uint32_t nunits = nch * ny * (uint32_t)G.nz;
+  constexpr int kWarps = kNHThreads / 32;
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const uint32_t tw = gridDim.x * kWarps;
+  const unsigned nb = gridDim.x;
+  unsigned long long epoch = 0;
+  double* __restrict__ pnh = P.p;
+
+  // ------------------------------------------------------------------ init
+  // res = forc - A p (interior), rsold = dot_3D(res, res)  (:163-176)
+  {
+    double v[2] = {0.0, 0.0};
+    for (uint32_t u = gw; u < nunits; u += tw) {
+      int i, j, k;
+      nh_unit(u, nch, ny, lane, i, j, k);
+      if (i > nx) continue;
+      const size_t q = G.at(i, j, k);
+      const uint32_t f = op.flags[q];
+      const double a = nh_apply(op, G, i, j, k, f,
+                                [&](int di, int dj, int dk) { return __ldcg(pnh + q + nh_off(G, di, dj, dk)); });
+      const double fo = P.forc[fidx3(nx, (int)ny, i, j, k)];
+      const double r = __dsub_rn(fo, a);
+      nh_store_cyclic(P.res[1], G, i, j, k, r);
+      if (f & kNHMaskT) {
+        v[0] += r * r;
+        v[1] += fo * fo;
+      }
+    }
+    double out[2];
+    block_reduce<2, -1, kNHThreads>(v, out);
+    if (threadIdx.x == 0) {
+      double* slot = P.slots + (size_t)blockIdx.x * 4;
+      slot[0] = out[0];
+      slot[1] = out[1];
+    }
+  }
+  if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns, P.stall_extra)) return;
+  double red0[2];
+  grid_collect<2, -1, kNHThreads>(P.slots, 4, nb, red0);
+  double beta = red0[0];
+  const double bb = red0[1];
+  const double rtol2bb = P.rtol * P.rtol * bb;
+
+  const double eps = P.eps;
+  const int max_it = P.max_it;
+  double betamin = 0.0, step1 = 0.0, est = 0.0, bq = 0.0, alpha_prev = 0.0, rr_prev = beta;
+  int n = 0, status = PYOMGPU_OK, converged = 0;
+
+  if (beta == 0.0) {  // :177
+    n = 0;
+    goto done_ok;
+  }
+  if (max_it < 1) {
+    n = 1;
+    status = PYOMGPU_MAXITER;
+    goto done_err;
+  }
+
+  for (n = 1;; n++) {
+    const double* __restrict__ R = P.res[n & 1];
+    const double* __restrict__ S = P.s[n & 1];
+    // s_n at a cell: res + rsnew/rsold * p (:189), separately rounded
+    auto snew = [&](size_t qq) { return __dadd_rn(__ldcg(R + qq), __dmul_rn(bq, __ldcg(S + qq))); };
+    // -------------------------------------------------------------- sweep A
+    {
+      double acc_dot = 0.0, acc_max = 0.0;
+      for (uint32_t u = gw; u < nunits; u += tw) {
+        int i, j, k;
+        nh_unit(u, nch, ny, lane, i, j, k);
+        if (i > nx) continue;
+        const size_t q = G.at(i, j, k);
+        const uint32_t f = op.flags[q];
+        if (!(f & kNHMaskT)) continue;  // only masked products enter the sums
+        const double a = nh_apply(op, G, i, j, k, f,
+                                  [&](int di, int dj, int dk) { return snew(q + nh_off(G, di, dj, dk)); });
+        const double sc = snew(q);
+        acc_dot += sc * a;
+        acc_max = fmax(acc_max, fabs(sc));
+      }
+      double v[2] = {acc_dot, acc_max}, out[2];
+      block_reduce<2, 1, kNHThreads>(v, out);
+      if (threadIdx.x == 0) {
+        double* slot = P.slots + (size_t)((epoch & 1) * nb + blockIdx.x) * 4;
+        slot[0] = out[0];
+        slot[1] = out[1];
+      }
+    }
+    const unsigned long long ep_a = epoch;
+    if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
+    double sAs, smax;
+    {
+      double r2[2];
+      grid_collect<2, 1, kNHThreads>(P.slots + (size_t)((ep_a & 1) * nb) * 4, 4, nb, r2);
+      sAs = r2[0];
+      smax = r2[1];
+    }
+    if (n > 1) {  // convergence test of iteration n-1 (:215-226) with max|p| of its new p
+      const int m = n - 1;
+      const double step = fabs(alpha_prev) * smax;
+      if (m == 1) {
+        step1 = step;
+        est = step;
+        if (step < eps) {
+          n = m;
+          goto done_ok;
+        }
+      } else if (step < eps) {
+        const double rate = exp(log(step / step1) / (double)(m - 1));
+        est = step * rate / (1.0 - rate);
+        if (est < eps) {
+          n = m;
+          goto done_ok;
+        }
+      }
+      if (est != est) {
+        n = m;
+        status = PYOMGPU_NAN;
+        goto done_err;
+      }
+      if (P.rtol > 0.0 && (bb > 0.0 ? rr_prev <= rtol2bb : rr_prev == 0.0)) {
+        est = sqrt(rr_prev);
+        n = m;
+        goto done_ok;
+      }
+      if (m >= max_it) {  // :228
+        n = max_it + 1;
+        status = PYOMGPU_MAXITER;
+        goto done_err;
+      }
+    }
+    if (sAs == 0.0) goto done_ok;  // :185
+    {
+      const double alpha = beta / sAs;
+      double* __restrict__ Rn = P.res[(n + 1) & 1];
+      double* __restrict__ Sn = P.s[(n + 1) & 1];
+      // ------------------------------------------------------------ sweep B
+      double acc_r = 0.0;
+      for (uint32_t u = gw; u < nunits; u += tw) {
+        int i, j, k;
+        nh_unit(u, nch, ny, lane, i, j, k);
+        if (i > nx) continue;
+        const size_t q = G.at(i, j, k);
+        const uint32_t f = op.flags[q];
+        const double a = nh_apply(op, G, i, j, k, f,
+                                  [&](int di, int dj, int dk) { return snew(q + nh_off(G, di, dj, dk)); });
+        const double sc = snew(q);
+        const double r = __dsub_rn(__ldcg(R + q), __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
+        nh_add_cyclic(pnh, G, i, j, k, __dmul_rn(alpha, sc));             // p_non_hydro += alpha*p (:187)
+        nh_store_cyclic(Rn, G, i, j, k, r);
+        nh_store_cyclic(Sn, G, i, j, k, sc);
+        if (f & kNHMaskT) acc_r += r * r;
+      }
+      double v[1] = {acc_r}, out[1];
+      block_reduce<1, -1, kNHThreads>(v, out);
+      if (threadIdx.x == 0) P.slots[(size_t)((epoch & 1) * nb + blockIdx.x) * 4] = out[0];
+      const unsigned long long ep_b = epoch;
+      if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
+      double r1[1];
+      grid_collect<1, -1, kNHThreads>(P.slots + (size_t)((ep_b & 1) * nb) * 4, 4, nb, r1);
+      const double rsnew = r1[0];
+      bq = rsnew / beta;
+      beta = rsnew;
+      if (n == 1) {  // divergence test (:197-205)
+        betamin = fabs(rsnew);
+      } else if (n > 2) {
+        betamin = fmin(betamin, fabs(rsnew));
+        if (fabs(rsnew) > 100.0 * betamin) {
+          status = PYOMGPU_DIVERGED;
+          goto done_err;
+        }
+      }
+      alpha_prev = alpha;
+      rr_prev = rsnew;
+    }
+  }
+
+done_ok:
+  converged = 1;
+  status = PYOMGPU_OK;
+  goto done;
+done_err:
+  converged = 0;
+  if (est != est) status = PYOMGPU_NAN;
+done:
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.out->iterations = n;
+    P.out->converged = converged;
+    P.out->status = status;
+    P.out->est = est;
+  }
+}
+
+const void* nh_cg_kernel_ptr() { return (const void*)nh_cg_kernel; }
+
+namespace {
+
+__global__ void nh_apply_kernel(const NHGeo G, const NHOp op, const double* __restrict__ p, double* __restrict__ res) {
+  const int nx = G.g.nx, ny = G.g.ny;
+  const size_t ncell = (size_t)nx * ny * G.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ncell; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nx) + 1;
+    const size_t r = e / nx;
+    const int j = (int)(r % ny) + 1;
+    const int k = (int)(r / ny) + 1;
+    const size_t q = G.at(i, j, k);
+    res[q] = nh_apply(op, G, i, j, k, op.flags[q],
+                      [&](int di, int dj, int dk) { return p[q + nh_off(G, di, dj, dk)]; });
+  }
+}
+
+// Fortran (nx+4, ny+4, nz) <-> padded 3-D, whole arrays (halos included).
+__global__ void nh_pack_kernel(const NHGeo G, const double* __restrict__ user, double* __restrict__ pad, int dir) {
+  const int X = G.g.nx + 2 * kOnx, Y = G.g.ny + 2 * kOnx;
+  const size_t n = (size_t)X * Y * G.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int fi = (int)(e % X);
+    const size_t r = e / X;
+    const int fj = (int)(r % Y);
+    const int k = (int)(r / Y);
+    const size_t q = (size_t)k * G.plane + (size_t)fj * G.g.pitch + (size_t)(fi + kXOff);
+    if (dir == 0)
+      pad[q] = user[e];
+    else
+      const_cast<double*>(user)[e] = pad[q];
+  }
+}
+
+int grid_for(size_t n) { return (int)std::min<size_t>(4096, std::max<size_t>(1, (n + 255) / 256)); }
+
+}  // namespace
+
+void launch_nh_apply(const NHGeo& G, const NHOp& op, const double* p, double* res, cudaStream_t st) {
+  nh_apply_kernel<<<grid_for((size_t)G.g.nx * G.g.ny * G.nz), 256, 0, st>>>(G, op, p, res);
+}
+void launch_nh_pack(const NHGeo& G, const double* user, double* padded, cudaStream_t st) {
+  const size_t n = (size_t)(G.g.nx + 4) * (G.g.ny + 4) * G.nz;
+  nh_pack_kernel<<<grid_for(n), 256, 0, st>>>(G, user, padded, 0);
+}
+void launch_nh_unpack(const NHGeo& G, const double* padded, double* user, cudaStream_t st) {
+  const size_t n = (size_t)(G.g.nx + 4) * (G.g.ny + 4) * G.nz;
+  nh_pack_kernel<<<grid_for(n), 256, 0, st>>>(G, user, const_cast<double*>(padded), 1);
+}
+
+}  // namespace pyomgpu
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace pyomgpu;
+
+struct pyomgpu_nh {
+  int device = 0, nsm = 0;
+  NHGeo G{};
+  NHOp op{};
+  int cyclic_x = 0, cyclic_y = 0;
+  size_t nf = 0;  // Fortran-layout elements (nx+4)(ny+4)nz
+  uint8_t* flags = nullptr;
+  double *tE = nullptr, *tW = nullptr, *tN = nullptr, *tS = nullptr, *tT = nullptr, *tB = nullptr;
+  double *p = nullptr, *res[2] = {}, *s[2] = {}, *stage_f = nullptr, *stage_p = nullptr;
+  SyncCtl* ctl = nullptr;
+  double* slots = nullptr;
+  CGResult* d_result = nullptr;
+  CGResult* h_result = nullptr;
+  int* h_err = nullptr;
+  int max_blocks = 0;
+  int grid = 0;  // 0: automatic
+  double timeout_s = 2.0;
+  unsigned stall_next = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ~pyomgpu_nh() {
+    void* ptrs[] = {flags, tE, tW, tN, tS, tT, tB, p, res[0], res[1], s[0], s[1], stage_f, stage_p, ctl, slots,
+                    d_result};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    if (h_result) cudaFreeHost(h_result);
+    if (h_err) cudaFreeHost(h_err);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+namespace {
+
+int nfail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  pyomgpu::set_last_error(buf);
+  return code;
+}
+
+#define NCK(call)                                                                                       \
+  do {                                                                                                  \
+    cudaError_t e_ = (call);                                                                            \
+    if (e_ != cudaSuccess)                                                                              \
+      return nfail(PYOMGPU_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+bool nh_on_device(const void* q) {
+  if (!q) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+int nalloc(T** q, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)q, n * sizeof(T));
+  if (e != cudaSuccess) return nfail(PYOMGPU_ENOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  return 0;
+}
+
+template <typename T>
+int nupload(T** d, const std::vector<T>& h) {
+  if (int rc = nalloc(d, h.size())) return rc;
+  NCK(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// Fortran-layout input: device pointers pass through, host memory is copied
+// into `stage`.
+int nh_stage(pyomgpu_nh* h, const double* user, double* stage, const double** out, cudaStream_t st) {
+  if (nh_on_device(user)) {
+    *out = user;
+    return 0;
+  }
+  NCK(cudaMemcpyAsync(stage, user, h->nf * sizeof(double), cudaMemcpyHostToDevice, st));
+  *out = stage;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
+  if (!gr || !out) return nfail(PYOMGPU_EINVAL, "nh_create: null argument");
+  *out = nullptr;
+  const int nx = gr->nx, ny = gr->ny, nz = gr->nz;
+  if (gr->onx != 2) return nfail(PYOMGPU_EINVAL, "nh_create: onx must be 2");
+  if (nx < 4 || ny < 1 || nz < 2)
+    return nfail(PYOMGPU_EINVAL, "nh_create: need nx >= 4, ny >= 1, nz >= 2 (make_coeff_non_hydro reads maskW(nz-1))");
+  if (gr->enable_cyclic_y && ny < 4) return nfail(PYOMGPU_EINVAL, "nh_create: cyclic y needs ny >= 4");
+  if (!gr->dxt || !gr->dxu || !gr->dyt || !gr->dyu || !gr->cost || !gr->cosu || !gr->dzt || !gr->dzw ||
+      !gr->maskT || !gr->maskU || !gr->maskV || !gr->maskW)
+    return nfail(PYOMGPU_EINVAL, "nh_create: every grid array is required");
+  const size_t X = nx + 4, Y = ny + 4;
+  const size_t ncell = (size_t)nx * ny * nz;
+  if ((ncell + 31) / 32 + (size_t)ny * nz > 0xffffffffull / 2)
+    return nfail(PYOMGPU_EINVAL, "nh_create: grid too large");
+  auto* h = new pyomgpu_nh();
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
+  h->cyclic_x = gr->enable_cyclic_x != 0;
+  h->cyclic_y = gr->enable_cyclic_y != 0;
+  Geo g{};
+  g.nx = nx;
+  g.ny = ny;
+  g.pitch = (int)(((X + kXOff) + 31) / 32 * 32);
+  g.cyclic_x = h->cyclic_x;
+  g.cyclic_y = h->cyclic_y;
+  h->G.g = g;
+  h->G.nz = nz;
+  h->G.plane = g.size();
+  h->nf = X * Y * (size_t)nz;
+  const size_t np = h->G.size();
+
+  // ---- tables and flags, make_coeff_non_hydro's arithmetic (host IEEE double)
+  auto F3 = [&](const double* a, int i, int j, int k) {  // Fortran (i,j,k), 1-based k
+    return a[(size_t)(i + 1) + X * ((size_t)(j + 1) + Y * (size_t)(k - 1))];
+  };
+  auto I1 = [](int i) { return (size_t)(i + 1); };  // Fortran index -> [n+4] array index
+  std::vector<double> tE(g.size(), 0.0), tW(g.size(), 0.0), tN(Y, 0.0), tS(Y, 0.0), tT(nz, 0.0), tB(nz, 0.0);
+  std::vector<uint8_t> flags(np, 0);
+  int bad_mask = 0;
+  for (int j = 1; j <= ny; j++) {
+    const double c2 = gr->cost[I1(j)] * gr->cost[I1(j)];
+    for (int i = 1; i <= nx; i++) {
+      tE[g.at(i, j)] = 1.0 / gr->dxu[I1(i)] / gr->dxt[I1(i)] / c2;
+      tW[g.at(i, j)] = 1.0 / gr->dxu[I1(i - 1)] / gr->dxt[I1(i)] / c2;
+    }
+    tN[I1(j)] = 1.0 / gr->dyu[I1(j)] / gr->dyt[I1(j)] * gr->cosu[I1(j)] / gr->cost[I1(j)];
+    tS[I1(j)] = 1.0 / gr->dyu[I1(j - 1)] / gr->dyt[I1(j)] * gr->cosu[I1(j - 1)] / gr->cost[I1(j)];
+  }
+  for (int k = 1; k <= nz; k++) {
+    if (k < nz) tT[k - 1] = 1.0 / gr->dzw[k - 1] / gr->dzt[k - 1];
+    if (k > 1) tB[k - 1] = 1.0 / gr->dzw[k - 2] / gr->dzt[k - 1];
+  }
+  auto bit = [&](double m, uint32_t b) -> uint32_t {
+    if (m == 1.0) return b;
+    if (m != 0.0) bad_mask = 1;
+    return 0u;
+  };
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        uint32_t f = 0;
+        f |= bit(F3(gr->maskU, i, j, k), kNHE);
+        f |= bit(F3(gr->maskU, i - 1, j, k), kNHW);
+        f |= bit(F3(gr->maskV, i, j, k), kNHN);
+        f |= bit(F3(gr->maskV, i, j - 1, k), kNHS);
+        if (k < nz) f |= bit(F3(gr->maskW, i, j, k), kNHT);
+        if (k > 1) f |= bit(F3(gr->maskW, i, j, k - 1), kNHB);
+        f |= bit(F3(gr->maskT, i, j, k), kNHMaskT);
+        flags[h->G.at(i, j, k)] = (uint8_t)f;
+      }
+  if (bad_mask) {
+    delete h;
+    return nfail(PYOMGPU_EINVAL, "nh_create: masks must hold only 0 and 1");
+  }
+  int rc = 0;
+  if ((rc = nupload(&h->flags, flags)) || (rc = nupload(&h->tE, tE)) || (rc = nupload(&h->tW, tW)) ||
+      (rc = nupload(&h->tN, tN)) || (rc = nupload(&h->tS, tS)) || (rc = nupload(&h->tT, tT)) ||
+      (rc = nupload(&h->tB, tB)) || (rc = nalloc(&h->p, np)) || (rc = nalloc(&h->res[0], np)) ||
+      (rc = nalloc(&h->res[1], np)) || (rc = nalloc(&h->s[0], np)) || (rc = nalloc(&h->s[1], np)) ||
+      (rc = nalloc(&h->stage_f, h->nf)) || (rc = nalloc(&h->stage_p, h->nf)) || (rc = nalloc(&h->ctl, 1)) ||
+      (rc = nalloc(&h->d_result, 1))) {
+    delete h;
+    return rc;
+  }
+  h->op = NHOp{h->flags, h->tE, h->tW, h->tN, h->tS, h->tT, h->tB};
+  if (cudaMemset(h->p, 0, np * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return nfail(PYOMGPU_ECUDA, "nh_create: cudaMemset");
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nh_cg_kernel, kNHThreads, 0) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    delete h;
+    return nfail(PYOMGPU_ECUDA, "nh_create: occupancy query failed");
+  }
+  h->max_blocks = std::min(per_sm * h->nsm, 4 * kNHThreads);  // grid_collect reads <= 4 slots per thread
+  if ((rc = nalloc(&h->slots, (size_t)2 * h->max_blocks * 4))) {
+    delete h;
+    return rc;
+  }
+  if (cudaMallocHost((void**)&h->h_result, sizeof(CGResult)) != cudaSuccess ||
+      cudaMallocHost((void**)&h->h_err, sizeof(int)) != cudaSuccess || cudaEventCreate(&h->e0) != cudaSuccess ||
+      cudaEventCreate(&h->e1) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return nfail(PYOMGPU_ECUDA, "nh_create: host buffers / events");
+  }
+  *out = h;
+  return PYOMGPU_OK;
+}
+
+void pyomgpu_nh_destroy(pyomgpu_nh* h) { delete h; }
+
+int32_t pyomgpu_nh_set_sync_timeout(pyomgpu_nh* h, double seconds) {
+  if (!h || !(seconds > 0)) return nfail(PYOMGPU_EINVAL, "nh_set_sync_timeout: bad argument");
+  h->timeout_s = seconds;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_nh_inject_barrier_stall(pyomgpu_nh* h, int32_t enable) {
+  if (!h) return nfail(PYOMGPU_EINVAL, "nh_inject_barrier_stall: null handle");
+  h->stall_next = enable ? 1u : 0u;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_nh_set_grid(pyomgpu_nh* h, int32_t blocks) {
+  if (!h || blocks < 0) return nfail(PYOMGPU_EINVAL, "nh_set_grid: bad argument");
+  h->grid = std::min(blocks, h->max_blocks);
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_apply_op_3d(pyomgpu_nh* h, const double* p1, double* res, pyomgpu_stream stream) {
+  if (!h || !p1 || !res) return nfail(PYOMGPU_EINVAL, "apply_op_3d: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* pin = nullptr;
+  if (int rc = nh_stage(h, p1, h->stage_p, &pin, st)) return rc;
+  const size_t bytes = h->G.size() * sizeof(double);
+  launch_nh_pack(h->G, pin, h->p, st);
+  NCK(cudaMemsetAsync(h->res[0], 0, bytes, st));
+  launch_nh_apply(h->G, h->op, h->p, h->res[0], st);
+  const bool dev_out = nh_on_device(res);
+  double* dst = dev_out ? res : h->stage_f;
+  launch_nh_unpack(h->G, h->res[0], dst, st);
+  NCK(cudaGetLastError());
+  if (!dev_out) NCK(cudaMemcpyAsync(res, h->stage_f, h->nf * sizeof(double), cudaMemcpyDeviceToHost, st));
+  NCK(cudaStreamSynchronize(st));
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, double eps, int32_t max_it,
+                                  pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!h || !forc || !p) return nfail(PYOMGPU_EINVAL, "congrad_non_hydro: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* fdev = nullptr;
+  if (int rc = nh_stage(h, forc, h->stage_f, &fdev, st)) return rc;
+  const bool p_dev = nh_on_device(p);
+  const double* pin = nullptr;
+  if (int rc = nh_stage(h, p, h->stage_p, &pin, st)) return rc;
+  const size_t bytes = h->G.size() * sizeof(double);
+  launch_nh_pack(h->G, pin, h->p, st);
+  for (double* b : {h->res[0], h->res[1], h->s[0], h->s[1]}) NCK(cudaMemsetAsync(b, 0, bytes, st));
+  NCK(cudaMemsetAsync(h->ctl, 0, sizeof(SyncCtl), st));
+  NHParams P{};
+  P.G = h->G;
+  P.op = h->op;
+  P.forc = fdev;
+  P.p = h->p;
+  P.res[0] = h->res[0];
+  P.res[1] = h->res[1];
+  P.s[0] = h->s[0];
+  P.s[1] = h->s[1];
+  P.eps = eps;
+  P.max_it = max_it;
+  P.rtol = 0.0;
+  P.ctl = h->ctl;
+  P.slots = h->slots;
+  P.timeout_ns = (unsigned long long)(h->timeout_s * 1e9);
+  P.stall_extra = h->stall_next;
+  h->stall_next = 0;
+  P.out = h->d_result;
+  const size_t units = (size_t)((h->G.g.nx + 31) / 32) * h->G.g.ny * h->G.nz;
+  int grid = h->grid > 0 ? h->grid : (int)std::min<size_t>(h->max_blocks, (units + 7) / 8);
+  grid = std::max(1, grid);
+  void* args[] = {&P};
+  NCK(cudaEventRecord(h->e0, st));
+  NCK(cudaLaunchCooperativeKernel(nh_cg_kernel_ptr(), dim3(grid), dim3(kNHThreads), args, 0, st));
+  NCK(cudaEventRecord(h->e1, st));
+  NCK(cudaMemcpyAsync(h->h_result, h->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
+  NCK(cudaMemcpyAsync(h->h_err, &h->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  double* pout = p_dev ? p : h->stage_p;
+  launch_nh_unpack(h->G, h->p, pout, st);
+  NCK(cudaGetLastError());
+  if (!p_dev) NCK(cudaMemcpyAsync(p, h->stage_p, h->nf * sizeof(double), cudaMemcpyDeviceToHost, st));
+  NCK(cudaStreamSynchronize(st));
+  const int err = *h->h_err;
+  float ms = 0.f;
+  NCK(cudaEventElapsedTime(&ms, h->e0, h->e1));
+  if (info) {
+    info->iterations = h->h_result->iterations;
+    info->converged = h->h_result->converged;
+    info->status = h->h_result->status;
+    info->outer_iterations = 1;
+    info->estimated_error = h->h_result->est;
+    info->rel_residual = -1.0;
+    info->device_ms = ms;
+    info->kernel_launches = 1;
+    info->fcg_iterations = 0;
+    if (err) {
+      info->status = PYOMGPU_TIMEOUT;
+      info->converged = 0;
+    }
+  }
+  if (err) return nfail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded %.3f s", h->timeout_s);
+  return h->h_result->status;
+}
+
+}  // extern "C"

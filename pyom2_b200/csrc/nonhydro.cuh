@@ -1,0 +1,120 @@
+// Non-hydrostatic pressure operator (non_hydrostatic.f90:70-138, 247-276) in
+// compact device form.
+//
+// make_coeff_non_hydro stores a 3x3x3 stencil per cell (27 doubles), of which
+// at most seven entries are nonzero: the six faces and the centre.  Every face
+// coefficient is a 0/1 face mask times a metric factor that depends on one or
+// two of (i, j, k) only:
+//
+//   east   maskU(i,j,k)   * tE(i,j) = ((1/dxu(i)  )/dxt(i))/cost(j)**2
+//   west   maskU(i-1,j,k) * tW(i,j) = ((1/dxu(i-1))/dxt(i))/cost(j)**2
+//   north  maskV(i,j,k)   * tN(j)   = (((1/dyu(j)  )/dyt(j))*cosu(j)  )/cost(j)
+//   south  maskV(i,j-1,k) * tS(j)   = (((1/dyu(j-1))/dyt(j))*cosu(j-1))/cost(j)
+//   top    maskW(i,j,k)   * tT(k)   = (1/dzw(k)  )/dzt(k)      (k < nz)
+//   bottom maskW(i,j,k-1) * tB(k)   = (1/dzw(k-1))/dzt(k)      (k > 1)
+//
+// (mp/a/b/c with mp = 1 rounds exactly like 1/a/b/c, and with mp = 0 gives 0.)
+// The device keeps one flag byte per cell (the six face masks and maskT) plus
+// the 2-D tables tE, tW and the 1-D tables tN, tS, tT, tB, i.e. 1 byte per
+// cell instead of 216.  The centre coefficient is rebuilt in the order the
+// reference accumulates it (east, west, north, south, top, bottom), and the
+// products are summed in apply_op_3D's (kk, jj, ii) order with separately
+// rounded multiplies and adds, so A p is bit-identical to the reference's.
+#pragma once
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace pyomgpu {
+
+constexpr int kNHThreads = 256;
+
+enum : uint32_t { kNHE = 1u, kNHW = 2u, kNHN = 4u, kNHS = 8u, kNHT = 16u, kNHB = 32u, kNHMaskT = 64u };
+
+// Padded 3-D layout: level k (1..nz) is a padded 2-D field of the Geo layout.
+struct NHGeo {
+  Geo g;
+  int nz;
+  size_t plane;  // g.size()
+  __host__ __device__ __forceinline__ size_t at(int i, int j, int k) const {
+    return (size_t)(k - 1) * plane + g.at(i, j);
+  }
+  __host__ __device__ __forceinline__ size_t size() const { return plane * (size_t)nz; }
+};
+
+struct NHOp {
+  const uint8_t* flags;  // padded 3-D
+  const double* tE;      // padded 2-D
+  const double* tW;      // padded 2-D
+  const double* tN;      // [ny+4], index j+1
+  const double* tS;      // [ny+4], index j+1
+  const double* tT;      // [nz], index k-1
+  const double* tB;      // [nz], index k-1
+};
+
+// Operator row of cell (i,j,k) applied to a field given by fetch(di, dj, dk).
+template <class Fetch>
+__device__ __forceinline__ double nh_apply(const NHOp& op, const NHGeo& G, int i, int j, int k, uint32_t f,
+                                           const Fetch& fetch) {
+  const size_t q2 = G.g.at(i, j);
+  const double tE = (f & kNHE) ? op.tE[q2] : 0.0;
+  const double tW = (f & kNHW) ? op.tW[q2] : 0.0;
+  const double tN = (f & kNHN) ? op.tN[j + 1] : 0.0;
+  const double tS = (f & kNHS) ? op.tS[j + 1] : 0.0;
+  const double tT = (f & kNHT) ? op.tT[k - 1] : 0.0;
+  const double tB = (f & kNHB) ? op.tB[k - 1] : 0.0;
+  double c = 0.0;  // make_coeff_non_hydro's accumulation order
+  if (f & kNHE) c = __dsub_rn(c, tE);
+  if (f & kNHW) c = __dsub_rn(c, tW);
+  if (f & kNHN) c = __dsub_rn(c, tN);
+  if (f & kNHS) c = __dsub_rn(c, tS);
+  if (f & kNHT) c = __dsub_rn(c, tT);
+  if (f & kNHB) c = __dsub_rn(c, tB);
+  // apply_op_3D: kk outermost, then jj, then ii; zero coefficients add nothing
+  double a = 0.0;
+  if (f & kNHB) a = __dadd_rn(a, __dmul_rn(tB, fetch(0, 0, -1)));
+  if (f & kNHS) a = __dadd_rn(a, __dmul_rn(tS, fetch(0, -1, 0)));
+  if (f & kNHW) a = __dadd_rn(a, __dmul_rn(tW, fetch(-1, 0, 0)));
+  a = __dadd_rn(a, __dmul_rn(c, fetch(0, 0, 0)));
+  if (f & kNHE) a = __dadd_rn(a, __dmul_rn(tE, fetch(1, 0, 0)));
+  if (f & kNHN) a = __dadd_rn(a, __dmul_rn(tN, fetch(0, 1, 0)));
+  if (f & kNHT) a = __dadd_rn(a, __dmul_rn(tT, fetch(0, 0, 1)));
+  return a;
+}
+
+// setcyclic_xyz (parallel_none.f90) applied per level: store v at (i,j,k) and
+// at the halo copies of (i,j) on that level.
+template <typename T>
+__device__ __forceinline__ void nh_store_cyclic(T* __restrict__ a, const NHGeo& G, int i, int j, int k, T v) {
+  store_cyclic(a + (size_t)(k - 1) * G.plane, G.g, i, j, v);
+}
+template <typename T>
+__device__ __forceinline__ void nh_add_cyclic(T* __restrict__ a, const NHGeo& G, int i, int j, int k, T d) {
+  add_cyclic(a + (size_t)(k - 1) * G.plane, G.g, i, j, d);
+}
+
+struct CGResult;
+
+struct NHParams {
+  NHGeo G;
+  NHOp op;
+  const double* forc;  // Fortran layout (nx+4, ny+4, nz), device
+  double* p;           // padded p_non_hydro(:,:,:,taup1), in/out
+  double* res[2];      // padded residual, double-buffered (halo = cyclic copies)
+  double* s[2];        // padded search direction, double-buffered
+  double eps;          // congr_epsilon_non_hydro
+  int max_it;          // congr_max_itts_non_hydro
+  double rtol;         // > 0: extra stop on the recursive residual, sqrt(sum r^2 maskT / sum forc^2 maskT)
+  SyncCtl* ctl;
+  double* slots;       // 2 * gridDim.x * 4 doubles
+  unsigned long long timeout_ns;
+  unsigned stall_extra;
+  CGResult* out;
+};
+
+const void* nh_cg_kernel_ptr();
+void launch_nh_apply(const NHGeo& G, const NHOp& op, const double* p, double* res, cudaStream_t st);
+void launch_nh_pack(const NHGeo& G, const double* user, double* padded, cudaStream_t st);
+void launch_nh_unpack(const NHGeo& G, const double* padded, double* user, cudaStream_t st);
+
+}  // namespace pyomgpu

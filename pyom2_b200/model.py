@@ -38,6 +38,8 @@ GRAV = f32(9.81)                                     # main_module.f90:19
 AB_EPS = f32(0.1)                                    # main_module.f90:52
 CONGR_EPSILON = f32(1e-12)                           # main_module.f90:189
 CONGR_MAX_ITERATIONS = 1000                          # main_module.f90:190
+CONGR_EPSILON_NON_HYDRO = f32(1e-12)                 # main_module.f90:222, default-real literal
+CONGR_MAX_ITTS_NON_HYDRO = 1000                      # main_module.f90:223
 
 
 def zeros_f(*shape, dtype=np.float64):
@@ -69,6 +71,9 @@ class ModelState:
         self.congr_epsilon = CONGR_EPSILON
         self.congr_max_iterations = CONGR_MAX_ITERATIONS
         self.congr_itts = 0
+        self.congr_epsilon_non_hydro = CONGR_EPSILON_NON_HYDRO
+        self.congr_max_itts_non_hydro = CONGR_MAX_ITTS_NON_HYDRO
+        self.congr_itts_non_hydro = 0
         self.taum1, self.tau, self.taup1 = 1, 2, 3
         self.itt = 0
         X, Y = self.nx + 2 * ONX, self.ny + 2 * ONX
@@ -90,13 +95,14 @@ class ModelState:
         for name in ("ht", "hu", "hv", "hur", "hvr"):
             setattr(self, name, zeros_f(X, Y))
         # 3-D masks
-        for name in ("maskT", "maskU", "maskV", "maskZ"):
+        for name in ("maskT", "maskU", "maskV", "maskZ", "maskW"):
             setattr(self, name, zeros_f(X, Y, nz))
         # dynamics (main_module.f90:298-311)
         for name in ("u", "v", "du", "dv", "rho"):
             setattr(self, name, zeros_f(X, Y, nz, 3))
         for name in ("du_mix", "dv_mix", "p_hydro"):
             setattr(self, name, zeros_f(X, Y, nz))
+        self.p_non_hydro = zeros_f(X, Y, nz, 3)          # main_module.f90:337
         self.psi = zeros_f(X, Y, 3)
         self.dpsi = zeros_f(X, Y, 3)
         # island variables, allocated by streamfunction_init (streamfct_init.f90:87-93)

@@ -130,7 +130,7 @@ def setcyclic_xy(M: ModelState, a):
 
 
 def calc_topo(M: ModelState):
-    """numerics.f90:187-261: close the domain, build masks T/U/V/Z and the
+    """numerics.f90:187-261: close the domain, build masks T/U/V/Z/W and the
     column depths ``hu, hv`` with reciprocals ``hur, hvr``."""
     nx, ny, nz = M.nx, M.ny, M.nz
     kbot = M.kbot
@@ -158,6 +158,9 @@ def calc_topo(M: ModelState):
     M.maskU[...] = maskU
     M.maskV[...] = maskV
     M.maskZ[...] = maskZ
+    maskW = maskT.copy()                          # numerics.f90:246-249
+    maskW[:, :, :-1] = np.minimum(maskT[:, :, :-1], maskT[:, :, 1:])
+    M.maskW[...] = maskW
     dzt = M.dzt[None, None, :]
     M.ht[...] = (maskT * dzt).sum(axis=2)
     M.hu[...] = 0.0
@@ -463,6 +466,88 @@ def config2(seed: int = 1002, count: int = 64, scale: float = 1.0):
         ni = int(rng.integers(0, 13))
         out.append(basin(nx, ny, seed * 1000 + m, lf, ni))
     return out
+
+
+# ----------------------------------------------------------------------------
+# non-hydrostatic pressure (non_hydrostatic.f90)
+# ----------------------------------------------------------------------------
+def nonhydro_forcing(M: ModelState, u, v, w, dt_mom):
+    """Forcing of the non-hydrostatic pressure solve from the provisional
+    velocities (u, v, w) at taup1, non_hydrostatic.f90:26-36: horizontal
+    divergence on the interior, plus the vertical difference of w, over dt_mom."""
+    nx, ny, nz = M.nx, M.ny, M.nz
+    forc = np.zeros(M.shape2d + (nz,), order="F")
+    I = slice(2, nx + 2)
+    J = slice(2, ny + 2)
+    cost = M.cost[J][None, :, None]
+    cosu = M.cosu[J][None, :, None]
+    cosum = M.cosu[1:ny + 1][None, :, None]
+    dxt = M.dxt[I][:, None, None]
+    dyt = M.dyt[J][None, :, None]
+    forc[I, J] = ((u[I, J] - u[1:nx + 1, J]) / (cost * dxt)
+                  + (cosu * v[I, J] - cosum * v[I, 1:ny + 1]) / (cost * dyt))
+    forc[:, :, 0] = forc[:, :, 0] + w[:, :, 0] / M.dzt[0]
+    for k in range(1, nz):
+        forc[:, :, k] = forc[:, :, k] + (w[:, :, k] - w[:, :, k - 1]) / M.dzt[k]
+    return np.asfortranarray(forc / dt_mom)
+
+
+class Workload3D:
+    """A model state with the forcing and first guess of one non-hydrostatic
+    pressure solve."""
+
+    def __init__(self, name, M, forc, p0, seed, meta=None):
+        self.name, self.M, self.forc, self.p0, self.seed = name, M, forc, p0, seed
+        self.meta = meta or {}
+
+
+def nonhydro_tank(nx, ny, nz, seed, cyclic_x=False, dx=0.01, slope=True, vel_rms=1e-3, first_guess=False):
+    """Cartesian tank (dx = dy = dz), closed walls (or re-entrant in x), a
+    shelf over the first quarter in x falling linearly to the full depth, with
+    seeded smooth roughness on the slope.  The forcing is the divergence of a
+    seeded smooth masked velocity field (rigid lid, w(nz) = 0), so it lies in
+    the range of the operator.  ``first_guess`` adds a smooth nonzero start
+    (the reference starts from 2 p(tau) - p(taum1))."""
+    rng = np.random.default_rng(np.random.PCG64(seed))
+    M = ModelState(nx, ny, nz, enable_cyclic_x=cyclic_x, coord_degree=False)
+    M.dxt[2:nx + 2] = dx
+    M.dyt[2:ny + 2] = dx
+    M.dzt[:] = dx
+    M.dt_mom = 0.25 * dx / 0.01
+    calc_grid(M)
+    H0 = dx * nz
+    if slope and nz > 2:
+        i = np.arange(1, nx + 1, dtype=np.float64)
+        shelf = 0.25 * H0
+        edge = max(1, nx // 4)
+        H = np.where(i <= edge, shelf, shelf + (H0 - shelf) * (i - edge) / max(1, nx - edge))
+        rough = smooth_field(rng, (nx, ny), max(2.0, nx / 16.0), (cyclic_x, False))
+        rough = rough / (np.abs(rough).max() + 1e-300)
+        Hij = np.clip(H[:, None] + 0.1 * H0 * rough * (i[:, None] > edge), dx, H0)
+        kb = _kbot_from_depth(Hij, dx, nz)
+    else:
+        kb = np.ones((nx, ny), dtype=np.int32)
+    M.kbot[2:nx + 2, 2:ny + 2] = kb
+    calc_topo(M)
+    shape3 = M.shape2d + (nz,)
+    cyc = (cyclic_x, False, False)
+    sig = (max(1.0, nx / 16.0), max(1.0, ny / 16.0), max(1.0, nz / 8.0))
+    vel = []
+    for m in (M.maskU, M.maskV, M.maskW):
+        f = smooth_field(rng, shape3, sig, cyc)
+        f *= vel_rms / (np.sqrt(np.mean(f ** 2)) + 1e-300)
+        vel.append(np.asfortranarray(f * m))
+    u, v, w = vel
+    w[:, :, nz - 1] = 0.0
+    for a in (u, v, w):
+        setcyclic_xy(M, a)
+    forc = nonhydro_forcing(M, u, v, w, M.dt_mom)
+    p0 = np.zeros(shape3, order="F")
+    if first_guess:
+        g = smooth_field(rng, shape3, sig, cyc)
+        p0 = np.asfortranarray(g * M.maskT * 1e-3)
+        setcyclic_xy(M, p0)
+    return Workload3D(f"tank_{nx}x{ny}x{nz}", M, forc, p0, seed)
 
 
 WORKLOADS = {"c0": config0, "c1": config1, "c3": config3}
