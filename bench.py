@@ -204,6 +204,86 @@ def c2_batch(steps, warmup, count=64):
             "note": "one launch for all 64 grids vs one launch per grid; FP64 Jacobi-PCG, same stop"}
 
 
+NH_BYTES_PER_CELL_ITER = 66  # res, s read twice (32), p read + write (16), res, s written (16), flags twice (2)
+
+
+def nh_bench(steps, warmup, peak, grid=(240, 240, 80), eps=1e-8, max_it=5000, cpu=True):
+    """Non-hydrostatic pressure solve (congrad_non_hydro, non_hydrostatic.f90:146):
+    a Cartesian tank of grid[0] x grid[1] x grid[2] cells (shelf, slope,
+    rough bottom, closed walls) with the divergence of a seeded velocity
+    field as forcing, solved from zero to the reference's stopping estimate
+    eps (1e-8, as in the 3-D overflow set-up of the reference).  Device time by
+    CUDA events with the L2 flushed before each solve; e2e through the C ABI
+    with host arrays."""
+    import torch
+    from pyom2_b200 import synth
+    from pyom2_b200.non_hydrostatic import NonHydrostatic
+
+    nx, ny, nz = grid
+    W = synth.nonhydro_tank(nx, ny, nz, 1)
+    M = W.M
+    nh = NonHydrostatic(M)
+    to_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).cuda().T
+    f_d, p0_d = to_dev(W.forc), to_dev(W.p0)
+    p_d = p0_d.clone()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    times, kern, its = [], [], []
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for k in range(warmup + steps):
+            p_d.copy_(p0_d)
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            it, info = nh.congrad_non_hydro(f_d, p_d, eps=eps, max_it=max_it)
+            e1.record(stream)
+            e1.synchronize()
+            if k >= warmup:
+                times.append(e0.elapsed_time(e1))
+                kern.append(info["device_ms"])
+                its.append(it)
+    cells = nx * ny * nz
+    it_med = int(statistics.median(its))
+    kern_med = statistics.median(kern)
+    alg = NH_BYTES_PER_CELL_ITER * cells * it_med
+    ach = alg / (kern_med * 1e-3) / 1e9
+    e2e = []
+    for k in range(2 + max(2, steps // 2)):
+        p_h = np.asfortranarray(W.p0.copy())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nh.congrad_non_hydro(W.forc, p_h, eps=eps, max_it=max_it)
+        if k >= 2:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    nf = M.shape2d[0] * M.shape2d[1] * nz
+    out = {"workload": f"tank_{nx}x{ny}x{nz}", "cells": cells, "eps": eps, "iterations": it_med,
+           "ms_per_solve": statistics.median(times), "kernel": "nh_cg_kernel", "kernel_ms": kern_med,
+           "us_per_iteration": 1e3 * kern_med / max(1, it_med), "status": info["status"],
+           "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "bytes_per_cell_iter": NH_BYTES_PER_CELL_ITER, "algorithmic_bytes": alg},
+           "e2e": {"value": statistics.median(e2e), "unit": "ms/solve", "h2d_bytes_per_step": 2 * nf * 8,
+                   "d2h_bytes_per_step": nf * 8},
+           "l2": "flushed (256 MiB write) per solve", "clocks": clk.summary()}
+    if cpu:
+        from oracle.oracle import Oracle3D
+        O = Oracle3D(M)
+        cf = O.make_coeff()
+        p = W.p0.copy(order="F")
+        t0 = time.perf_counter()
+        O.congrad(cf, W.forc, p, eps=0.0, max_it=3)
+        per = (time.perf_counter() - t0) / 3
+        n = max(5, min(it_med, int(10.0 / max(per, 1e-6))))
+        p = W.p0.copy(order="F")
+        t0 = time.perf_counter()
+        O.congrad(cf, W.forc, p, eps=0.0, max_it=n)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": dt / n * it_med * 1e3, "unit": "ms/solve", "cores": 1, "kind": "port",
+                               "sample": f"{n} CG iterations of the {nx}x{ny}x{nz} solve timed ({dt:.1f} s), "
+                                         f"x {it_med} iterations per solve"}
+    nh.close()
+    return out
+
+
 METHODS = {
     # name: (precision code, dtype label, algorithmic bytes key, dominant kernel)
     "pcg64": ("PREC_F64", "f64", "f64", "cg_ref_kernel<false>"),
@@ -226,6 +306,12 @@ def main():
     ap.add_argument("--with-c2", action="store_true",
                     help="also time config 2 (64 basins in one work-queue launch vs 64 sequential solves)")
     ap.add_argument("--c2-count", type=int, default=64, help="basins of config 2 (fewer for profiling)")
+    ap.add_argument("--with-nh", action="store_true",
+                    help="also time the non-hydrostatic 3-D pressure solve (congrad_non_hydro)")
+    ap.add_argument("--nh-only", action="store_true",
+                    help="time only the non-hydrostatic solve and print its object (profiling runs)")
+    ap.add_argument("--nh-grid", default="240x240x80", help="tank size of the non-hydrostatic solve")
+    ap.add_argument("--nh-max-it", type=int, default=5000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
@@ -243,6 +329,14 @@ def main():
 
     from pyom2_b200 import _abi
     from pyom2_b200.external import ExternalMode, _ptr
+
+    nh_grid = tuple(int(v) for v in args.nh_grid.split("x"))
+    if args.nh_only:
+        r = nh_bench(args.steps, args.warmup, peaks()[0], nh_grid, max_it=args.nh_max_it,
+                     cpu=not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps({"non_hydrostatic": r}), flush=True)
+        return
 
     W = build_workload()
     M = W.M
@@ -365,6 +459,9 @@ def main():
                                      "fcg_iterations": results["fcg"]["iterations"],
                                      "pcg64_iterations": results["pcg64"]["iterations"],
                                      "speedup": results["pcg64"]["value"] / results["fcg"]["value"]}
+    if args.with_nh and rank == 0:
+        out["non_hydrostatic"] = nh_bench(max(2, args.steps // 3), 3, peak, nh_grid, max_it=args.nh_max_it,
+                                          cpu=world == 1 and not args.no_cpu_baseline)
     if args.with_c2 and rank == 0:
         out["c2_batch"] = c2_batch(max(1, args.steps // 3), 1, args.c2_count)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -304,10 +304,13 @@ void pyomgpu_nh_destroy(pyomgpu_nh* nh);
 int32_t pyomgpu_nh_set_sync_timeout(pyomgpu_nh* nh, double seconds);
 /* Failure-detection test hook, as pyomgpu_inject_barrier_stall. */
 int32_t pyomgpu_nh_inject_barrier_stall(pyomgpu_nh* nh, int32_t enable);
-/* Blocks of the CG launch (0 = one 8-warp block per 256 cells' worth of
- * 32-cell rows, capped at the co-resident maximum).  Reduction order follows
- * the grid, so results change at rounding level. */
+/* Blocks of the CG launch (0 = one per brick, capped at the co-resident
+ * maximum).  Reduction order follows the grid, so results change at rounding
+ * level. */
 int32_t pyomgpu_nh_set_grid(pyomgpu_nh* nh, int32_t blocks);
+/* Brick shape of the CG sweeps: 32 x ty x kc cells staged with their halo in
+ * shared memory (0, 0 = automatic: ty = min(8, ny), kc from a 26 KB box). */
+int32_t pyomgpu_nh_set_brick(pyomgpu_nh* nh, int32_t ty, int32_t kc);
 /* res = A p1 over the interior, zero halo (apply_op_3D).  (nx+4, ny+4, nz)
  * Fortran-layout arrays, host or device. */
 int32_t pyomgpu_apply_op_3d(pyomgpu_nh* nh, const double* p1, double* res, pyomgpu_stream stream);

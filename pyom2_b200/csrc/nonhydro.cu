@@ -2,20 +2,23 @@
 // (non_hydrostatic.f90:146-242) as one persistent, grid-synchronised kernel,
 // apply_op_3D (:247-276) as a stand-alone kernel, and their C ABI.
 //
-// Per CG iteration the kernel makes two sweeps over the cells, separated by
-// grid barriers that carry the reductions (dot_3D / absmax_3D, :279-322):
+// Per CG iteration the kernel makes two sweeps over bricks of 32 x ty x kc
+// cells, separated by grid barriers that carry the reductions (dot_3D /
+// absmax_3D, :279-322).  Each brick's res and s boxes (brick + one-cell halo)
+// come into shared memory by TMA through a two-stage pipeline (the next
+// brick loads while this one is computed), and s_n = res + bq s_{n-1} is
+// formed in the box, so s_n is never stored before it is complete:
 //
-//   sweep A  s_n = res + bq s_{n-1} at each cell and its six neighbours
-//            (recomputed where needed, so s_n is never stored before it is
-//            complete), partial sums of (s_n, A s_n) and max|s_n| over maskT
+//   sweep A  partial sums of (s_n, A s_n) and max|s_n| over maskT
 //   sweep B  the same s_n and A s_n again, then res -= alpha A s_n,
 //            p += alpha s_n; res and s_n go to the other buffer of their
 //            double-buffered pair; partial sums of (res, res)
 //
-// so an iteration streams 64 bytes per cell (read res and s twice, read and
-// write p, write res and s) and stores no A s vector.  The convergence test of
-// iteration n needs max|s_{n+1}|, so it runs after sweep A of iteration n+1,
-// exactly as the reference evaluates it after forming the new direction.
+// so an iteration streams 64 bytes per cell from HBM (read res and s twice,
+// read and write p, write res and s) plus the flag byte twice, and stores no
+// A s vector.  The convergence test of iteration n needs max|s_{n+1}|, so it
+// runs after sweep A of iteration n+1, exactly as the reference evaluates it
+// after forming the new direction.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -28,6 +31,7 @@
 #include "../../include/pyomgpu.h"
 #include "cg_ref.cuh"
 #include "nonhydro.cuh"
+#include "tma.cuh"
 
 namespace pyomgpu {
 
@@ -55,7 +59,107 @@ __device__ __forceinline__ ptrdiff_t nh_off(const NHGeo& G, int di, int dj, int 
 
 }  // namespace
 
+// p += d at the setcyclic_xyz halo copies of (i,j) on level k (not at (i,j) itself).
+__device__ __forceinline__ void nh_add_copies(double* __restrict__ a, const NHGeo& G, int i, int j, int k, double d) {
+  double* lv = a + (size_t)(k - 1) * G.plane;
+  int xc, yc;
+  cyclic_copies(G.g, i, j, xc, yc);
+  if (xc != 0x7fffffff) lv[G.g.at(xc, j)] += d;
+  if (yc != 0x7fffffff) {
+    lv[G.g.at(i, yc)] += d;
+    if (xc != 0x7fffffff) lv[G.g.at(xc, yc)] += d;
+  }
+}
+
+// One sweep of this block over its bricks (brick b = blockIdx.x + m gridDim.x).
+// TMA brings the res/s boxes of buffer `cur`, the flags and (sweep B) p into
+// one of two pipeline stages while the other stage is computed; s_n = res +
+// bq s is formed in the box; then every warp marches up its column of the
+// brick, keeping s_n below/at/above the cell in registers, and calls
+// cell(i, j, k, f, A s_n, s_n, res, p) for each interior cell (sweep A: only
+// cells with maskT).  Returns false after a time-out (error recorded, the
+// other stage's copy waited for).
+template <bool kB, class Cell>
+__device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, unsigned char* smem, uint64_t* bar,
+                                         uint32_t (&phase)[2], const Cell& cell) {
+  const int TY = P.ty, KW = P.kw, KC = P.kc, BY = TY + 2, BXY = kNHBoxX * BY;
+  const int nbox = BXY * (KC + 2);
+  const size_t rs = nh_al(nh_rs_bytes(TY, KC)), pb = nh_al(nh_p_bytes(TY, KC)), stage = nh_stage_bytes(TY, KC);
+  const uint32_t tx_bytes =
+      (uint32_t)(2 * nh_rs_bytes(TY, KC) + nh_f_bytes(TY, KC) + (kB ? nh_p_bytes(TY, KC) : 0));
+  const int nbr = P.nbx * P.nby * P.nbz;
+  const int nx = P.G.g.nx, ny = P.G.g.ny, nz = P.G.nz;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int jj = warp % TY, kk0 = (warp / TY) * KW;
+  auto issue = [&](int b, int st) {
+    const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
+    unsigned char* B = smem + (size_t)st * stage;
+    fence_proxy_async_smem();
+    fence_proxy_async_global();
+    mbar_arrive_expect_tx(&bar[st], tx_bytes);
+    // res/s boxes: padded column of Fortran i0-2 (even, 16-byte aligned), row of j0-1, level index of k0-1
+    const int x = 32 * bx + 2, y = TY * by + 1, z = KC * bz - 1;
+    tma_load_3d(B, &P.map_res[cur], x, y, z, &bar[st]);
+    tma_load_3d(B + rs, &P.map_s[cur], x, y, z, &bar[st]);
+    // p: padded column of i0 (even), row of j0, level index of k0
+    if (kB) tma_load_3d(B + 2 * rs, &P.map_p, 32 * bx + 4, TY * by + 2, KC * bz, &bar[st]);
+    // flags: column i0-1 (a multiple of 32 bytes), row j0-1, level k0-1
+    tma_load_3d(B + 2 * rs + pb, &P.map_f, 32 * bx, TY * by, KC * bz, &bar[st]);
+  };
+  int c = 0;
+  if ((int)blockIdx.x < nbr && threadIdx.x == 0) issue(blockIdx.x, 0);
+  for (int b = blockIdx.x; b < nbr; b += gridDim.x, c++) {
+    const int st = c & 1;
+    const int bn = b + (int)gridDim.x;
+    if (bn < nbr && threadIdx.x == 0) issue(bn, st ^ 1);
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar[st], phase[st], P.timeout_ns));
+    phase[st] ^= 1u;
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+        if (bn < nbr) mbar_wait_bounded(&bar[st ^ 1], phase[st ^ 1], P.timeout_ns);
+      }
+      __syncthreads();
+      return false;
+    }
+    unsigned char* B = smem + (size_t)st * stage;
+    const double* R = reinterpret_cast<const double*>(B);
+    double* S = reinterpret_cast<double*>(B + rs);
+    const double* Pb = reinterpret_cast<const double*>(B + 2 * rs);
+    const uint8_t* F = B + 2 * rs + pb;
+    for (int e = threadIdx.x; e < nbox; e += kNHThreads) S[e] = __dadd_rn(R[e], __dmul_rn(bq, S[e]));
+    __syncthreads();
+    const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
+    const int i = 1 + 32 * bx + lane, j = 1 + TY * by + jj;
+    if (i <= nx && j <= ny) {
+      const size_t q2 = P.G.g.at(i, j);
+      const double tE = __ldg(P.op.tE + q2), tW = __ldg(P.op.tW + q2);
+      const double tN = __ldg(P.op.tN + j + 1), tS = __ldg(P.op.tS + j + 1);
+      int cc = ((kk0 + 1) * BY + jj + 1) * kNHBoxX + lane + 2;
+      double sdn = S[cc - BXY], sc = S[cc];
+      int k = 1 + KC * bz + kk0;
+      for (int m = 0; m < KW && k <= nz; m++, k++, cc += BXY) {
+        const double sup = S[cc + BXY];
+        const int fl = ((kk0 + m) * TY + jj) * 32 + lane;
+        const uint32_t f = F[fl];
+        if (kB || (f & kNHMaskT)) {
+          const double tT = (f & kNHT) ? __ldg(P.op.tT + k - 1) : 0.0;
+          const double tB = (f & kNHB) ? __ldg(P.op.tB + k - 1) : 0.0;
+          const double a = nh_row(f, tE, tW, tN, tS, tT, tB, sdn, S[cc - kNHBoxX], S[cc - 1], sc, S[cc + 1],
+                                  S[cc + kNHBoxX], sup);
+          cell(i, j, k, f, a, sc, R[cc], kB ? Pb[fl] : 0.0);
+        }
+        sdn = sc;
+        sc = sup;
+      }
+    }
+    __syncthreads();  // stage st is free for the copy issued next iteration
+  }
+  return true;
+}
+
 __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_constant__ NHParams P) {
+  extern __shared__ __align__(128) unsigned char smem[];
   const NHGeo G = P.G;
   const NHOp op = P.op;
   const int nx = G.g.nx;
@@ -67,8 +171,17 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
   const uint32_t gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
   const uint32_t tw = gridDim.x * kWarps;
   const unsigned nb = gridDim.x;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * nh_stage_bytes(P.ty, P.kc));
+  uint32_t phase[2] = {0u, 0u};
   unsigned long long epoch = 0;
   double* __restrict__ pnh = P.p;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
 
   // ------------------------------------------------------------------ init
   // res = forc - A p (interior), rsold = dot_3D(res, res)  (:163-176)
@@ -79,7 +192,7 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
       nh_unit(u, nch, ny, lane, i, j, k);
       if (i > nx) continue;
       const size_t q = G.at(i, j, k);
-      const uint32_t f = op.flags[q];
+      const uint32_t f = __ldg(op.flags + op.fidx((int)ny, i, j, k));
       const double a = nh_apply(op, G, i, j, k, f,
                                 [&](int di, int dj, int dk) { return __ldcg(pnh + q + nh_off(G, di, dj, dk)); });
       const double fo = P.forc[fidx3(nx, (int)ny, i, j, k)];
@@ -121,26 +234,16 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
   }
 
   for (n = 1;; n++) {
-    const double* __restrict__ R = P.res[n & 1];
-    const double* __restrict__ S = P.s[n & 1];
-    // s_n at a cell: res + rsnew/rsold * p (:189), separately rounded
-    auto snew = [&](size_t qq) { return __dadd_rn(__ldcg(R + qq), __dmul_rn(bq, __ldcg(S + qq))); };
+    const int cur = n & 1;
     // -------------------------------------------------------------- sweep A
     {
       double acc_dot = 0.0, acc_max = 0.0;
-      for (uint32_t u = gw; u < nunits; u += tw) {
-        int i, j, k;
-        nh_unit(u, nch, ny, lane, i, j, k);
-        if (i > nx) continue;
-        const size_t q = G.at(i, j, k);
-        const uint32_t f = op.flags[q];
-        if (!(f & kNHMaskT)) continue;  // only masked products enter the sums
-        const double a = nh_apply(op, G, i, j, k, f,
-                                  [&](int di, int dj, int dk) { return snew(q + nh_off(G, di, dj, dk)); });
-        const double sc = snew(q);
-        acc_dot += sc * a;
-        acc_max = fmax(acc_max, fabs(sc));
-      }
+      const bool ok = nh_sweep<false>(P, cur, bq, smem, bar, phase,
+                                      [&](int, int, int, uint32_t, double a, double sc, double, double) {
+                                        acc_dot += sc * a;
+                                        acc_max = fmax(acc_max, fabs(sc));
+                                      });
+      if (!ok) return;
       double v[2] = {acc_dot, acc_max}, out[2];
       block_reduce<2, 1, kNHThreads>(v, out);
       if (threadIdx.x == 0) {
@@ -195,25 +298,21 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
     if (sAs == 0.0) goto done_ok;  // :185
     {
       const double alpha = beta / sAs;
-      double* __restrict__ Rn = P.res[(n + 1) & 1];
-      double* __restrict__ Sn = P.s[(n + 1) & 1];
+      double* __restrict__ Rn = P.res[cur ^ 1];
+      double* __restrict__ Sn = P.s[cur ^ 1];
       // ------------------------------------------------------------ sweep B
       double acc_r = 0.0;
-      for (uint32_t u = gw; u < nunits; u += tw) {
-        int i, j, k;
-        nh_unit(u, nch, ny, lane, i, j, k);
-        if (i > nx) continue;
-        const size_t q = G.at(i, j, k);
-        const uint32_t f = op.flags[q];
-        const double a = nh_apply(op, G, i, j, k, f,
-                                  [&](int di, int dj, int dk) { return snew(q + nh_off(G, di, dj, dk)); });
-        const double sc = snew(q);
-        const double r = __dsub_rn(__ldcg(R + q), __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
-        nh_add_cyclic(pnh, G, i, j, k, __dmul_rn(alpha, sc));             // p_non_hydro += alpha*p (:187)
-        nh_store_cyclic(Rn, G, i, j, k, r);
-        nh_store_cyclic(Sn, G, i, j, k, sc);
-        if (f & kNHMaskT) acc_r += r * r;
-      }
+      const bool ok = nh_sweep<true>(
+          P, cur, bq, smem, bar, phase, [&](int i, int j, int k, uint32_t f, double a, double sc, double rc, double pc) {
+            const double r = __dsub_rn(rc, __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
+            const double d = __dmul_rn(alpha, sc);                // p_non_hydro + alpha*p (:187)
+            pnh[G.at(i, j, k)] = __dadd_rn(pc, d);
+            nh_add_copies(pnh, G, i, j, k, d);
+            nh_store_cyclic(Rn, G, i, j, k, r);
+            nh_store_cyclic(Sn, G, i, j, k, sc);
+            if (f & kNHMaskT) acc_r += r * r;
+          });
+      if (!ok) return;
       double v[1] = {acc_r}, out[1];
       block_reduce<1, -1, kNHThreads>(v, out);
       if (threadIdx.x == 0) P.slots[(size_t)((epoch & 1) * nb + blockIdx.x) * 4] = out[0];
@@ -222,7 +321,7 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
       double r1[1];
       grid_collect<1, -1, kNHThreads>(P.slots + (size_t)((ep_b & 1) * nb) * 4, 4, nb, r1);
       const double rsnew = r1[0];
-      bq = rsnew / beta;
+      bq = rsnew / beta;  // p = res + rsnew/rsold*p (:189)
       beta = rsnew;
       if (n == 1) {  // divergence test (:197-205)
         betamin = fabs(rsnew);
@@ -267,7 +366,7 @@ __global__ void nh_apply_kernel(const NHGeo G, const NHOp op, const double* __re
     const int j = (int)(r % ny) + 1;
     const int k = (int)(r / ny) + 1;
     const size_t q = G.at(i, j, k);
-    res[q] = nh_apply(op, G, i, j, k, op.flags[q],
+    res[q] = nh_apply(op, G, i, j, k, op.flags[op.fidx(ny, i, j, k)],
                       [&](int di, int dj, int dk) { return p[q + nh_off(G, di, dj, dk)]; });
   }
 }
@@ -326,8 +425,9 @@ struct pyomgpu_nh {
   CGResult* d_result = nullptr;
   CGResult* h_result = nullptr;
   int* h_err = nullptr;
-  int max_blocks = 0;
-  int grid = 0;  // 0: automatic
+  int max_blocks = 0;  // slots reserved for this many blocks
+  int grid = 0;        // 0: automatic
+  int ty = 0, kc = 0;  // brick shape (0: automatic)
   double timeout_s = 2.0;
   unsigned stall_next = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -441,7 +541,8 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
   };
   auto I1 = [](int i) { return (size_t)(i + 1); };  // Fortran index -> [n+4] array index
   std::vector<double> tE(g.size(), 0.0), tW(g.size(), 0.0), tN(Y, 0.0), tS(Y, 0.0), tT(nz, 0.0), tB(nz, 0.0);
-  std::vector<uint8_t> flags(np, 0);
+  const int fx = (nx + 31) / 32 * 32;
+  std::vector<uint8_t> flags((size_t)fx * ny * nz, 0);
   int bad_mask = 0;
   for (int j = 1; j <= ny; j++) {
     const double c2 = gr->cost[I1(j)] * gr->cost[I1(j)];
@@ -472,7 +573,7 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
         if (k < nz) f |= bit(F3(gr->maskW, i, j, k), kNHT);
         if (k > 1) f |= bit(F3(gr->maskW, i, j, k - 1), kNHB);
         f |= bit(F3(gr->maskT, i, j, k), kNHMaskT);
-        flags[h->G.at(i, j, k)] = (uint8_t)f;
+        flags[((size_t)(k - 1) * ny + (j - 1)) * fx + (i - 1)] = (uint8_t)f;
       }
   if (bad_mask) {
     delete h;
@@ -488,20 +589,19 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
     delete h;
     return rc;
   }
-  h->op = NHOp{h->flags, h->tE, h->tW, h->tN, h->tS, h->tT, h->tB};
+  h->op = NHOp{h->flags, h->tE, h->tW, h->tN, h->tS, h->tT, h->tB, fx};
   if (cudaMemset(h->p, 0, np * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     delete h;
     return nfail(PYOMGPU_ECUDA, "nh_create: cudaMemset");
   }
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nh_cg_kernel, kNHThreads, 0) != cudaSuccess ||
-      per_sm < 1) {
+  if (cudaFuncSetAttribute(nh_cg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNHSmemMax) !=
+      cudaSuccess) {
     cudaGetLastError();
     delete h;
-    return nfail(PYOMGPU_ECUDA, "nh_create: occupancy query failed");
+    return nfail(PYOMGPU_ECUDA, "nh_create: shared-memory attribute");
   }
-  h->max_blocks = std::min(per_sm * h->nsm, 4 * kNHThreads);  // grid_collect reads <= 4 slots per thread
+  h->max_blocks = 4 * kNHThreads;  // grid_collect reads <= 4 slots per thread
   if ((rc = nalloc(&h->slots, (size_t)2 * h->max_blocks * 4))) {
     delete h;
     return rc;
@@ -534,6 +634,18 @@ int32_t pyomgpu_nh_inject_barrier_stall(pyomgpu_nh* h, int32_t enable) {
 int32_t pyomgpu_nh_set_grid(pyomgpu_nh* h, int32_t blocks) {
   if (!h || blocks < 0) return nfail(PYOMGPU_EINVAL, "nh_set_grid: bad argument");
   h->grid = std::min(blocks, h->max_blocks);
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_nh_set_brick(pyomgpu_nh* h, int32_t ty, int32_t kc) {
+  if (!h || ty < 0 || kc < 0 || (ty > 0) != (kc > 0))
+    return nfail(PYOMGPU_EINVAL, "nh_set_brick: ty and kc both positive (or both 0 = automatic)");
+  if (ty > 0 && ((ty != 1 && ty != 2 && ty != 4 && ty != 8) || kc % (8 / ty) != 0 || kc > 248 ||
+                 nh_smem_bytes(ty, kc) > kNHSmemMax))
+    return nfail(PYOMGPU_EINVAL,
+                 "nh_set_brick: ty in {1,2,4,8}, kc a multiple of 8/ty, and the staged boxes within shared memory");
+  h->ty = ty;
+  h->kc = kc;
   return PYOMGPU_OK;
 }
 
@@ -586,12 +698,49 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
   P.stall_extra = h->stall_next;
   h->stall_next = 0;
   P.out = h->d_result;
-  const size_t units = (size_t)((h->G.g.nx + 31) / 32) * h->G.g.ny * h->G.nz;
-  int grid = h->grid > 0 ? h->grid : (int)std::min<size_t>(h->max_blocks, (units + 7) / 8);
+  // brick shape: 32 x ty x kc, ty the largest power of two <= min(8, ny), kc = (8/ty) kw with kw the
+  // largest level count per warp whose two pipeline stages leave room for two blocks per SM
+  int ty = h->ty, kc = h->kc;
+  if (ty == 0) {
+    ty = h->G.g.ny >= 8 ? 8 : h->G.g.ny >= 4 ? 4 : h->G.g.ny >= 2 ? 2 : 1;
+    const int seg = 8 / ty;
+    const int kw_need = (h->G.nz + seg - 1) / seg;
+    int kw = 1;
+    while (kw < kw_need && nh_smem_bytes(ty, seg * (kw + 1)) <= (size_t)113 * 1024) kw++;
+    kc = seg * kw;
+  }
+  const size_t smem = nh_smem_bytes(ty, kc);
+  P.ty = ty;
+  P.kc = kc;
+  P.kw = kc / (8 / ty);
+  P.nbx = (h->G.g.nx + 31) / 32;
+  P.nby = (h->G.g.ny + ty - 1) / ty;
+  P.nbz = (h->G.nz + kc - 1) / kc;
+  {
+    const uint64_t dims[3] = {(uint64_t)h->G.g.pitch, (uint64_t)(h->G.g.ny + 2 * kOnx), (uint64_t)h->G.nz};
+    const uint64_t strides[2] = {(uint64_t)h->G.g.pitch * 8, (uint64_t)h->G.plane * 8};
+    const uint32_t box[3] = {(uint32_t)kNHBoxX, (uint32_t)(ty + 2), (uint32_t)(kc + 2)};
+    const uint32_t pbox[3] = {32u, (uint32_t)ty, (uint32_t)kc};
+    const uint64_t fdims[3] = {(uint64_t)h->op.fx, (uint64_t)h->G.g.ny, (uint64_t)h->G.nz};
+    const uint64_t fstrides[2] = {(uint64_t)h->op.fx, (uint64_t)h->op.fx * h->G.g.ny};
+    int bad = 0;
+    for (int b = 0; b < 2; b++)
+      bad |= encode_map(&P.map_res[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->res[b], dims, strides, box) |
+             encode_map(&P.map_s[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->s[b], dims, strides, box);
+    bad |= encode_map(&P.map_p, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->p, dims, strides, pbox);
+    bad |= encode_map(&P.map_f, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->flags, fdims, fstrides, pbox);
+    if (bad) return nfail(PYOMGPU_ECUDA, "congrad_non_hydro: cuTensorMapEncodeTiled failed");
+  }
+  int per_sm = 0;
+  NCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nh_cg_kernel, kNHThreads, smem));
+  if (per_sm < 1) return nfail(PYOMGPU_EINVAL, "congrad_non_hydro: brick does not fit on an SM");
+  const int coresident = std::min(per_sm * h->nsm, h->max_blocks);
+  const int nbricks = P.nbx * P.nby * P.nbz;
+  int grid = h->grid > 0 ? std::min(h->grid, coresident) : std::min(coresident, nbricks);
   grid = std::max(1, grid);
   void* args[] = {&P};
   NCK(cudaEventRecord(h->e0, st));
-  NCK(cudaLaunchCooperativeKernel(nh_cg_kernel_ptr(), dim3(grid), dim3(kNHThreads), args, 0, st));
+  NCK(cudaLaunchCooperativeKernel(nh_cg_kernel_ptr(), dim3(grid), dim3(kNHThreads), args, smem, st));
   NCK(cudaEventRecord(h->e1, st));
   NCK(cudaMemcpyAsync(h->h_result, h->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
   NCK(cudaMemcpyAsync(h->h_err, &h->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -21,6 +21,7 @@
 // products are summed in apply_op_3D's (kk, jj, ii) order with separately
 // rounded multiplies and adds, so A p is bit-identical to the reference's.
 #pragma once
+#include <cuda.h>
 #include <stdint.h>
 
 #include "common.cuh"
@@ -43,26 +44,24 @@ struct NHGeo {
 };
 
 struct NHOp {
-  const uint8_t* flags;  // padded 3-D
+  const uint8_t* flags;  // [nz][ny][fx], cell (i,j,k) at ((k-1)*ny + j-1)*fx + i-1
   const double* tE;      // padded 2-D
   const double* tW;      // padded 2-D
   const double* tN;      // [ny+4], index j+1
   const double* tS;      // [ny+4], index j+1
   const double* tT;      // [nz], index k-1
   const double* tB;      // [nz], index k-1
+  int fx;                // flag row pitch, nx rounded up to 32
+  __host__ __device__ __forceinline__ size_t fidx(int ny, int i, int j, int k) const {
+    return ((size_t)(k - 1) * (size_t)ny + (size_t)(j - 1)) * (size_t)fx + (size_t)(i - 1);
+  }
 };
 
-// Operator row of cell (i,j,k) applied to a field given by fetch(di, dj, dk).
-template <class Fetch>
-__device__ __forceinline__ double nh_apply(const NHOp& op, const NHGeo& G, int i, int j, int k, uint32_t f,
-                                           const Fetch& fetch) {
-  const size_t q2 = G.g.at(i, j);
-  const double tE = (f & kNHE) ? op.tE[q2] : 0.0;
-  const double tW = (f & kNHW) ? op.tW[q2] : 0.0;
-  const double tN = (f & kNHN) ? op.tN[j + 1] : 0.0;
-  const double tS = (f & kNHS) ? op.tS[j + 1] : 0.0;
-  const double tT = (f & kNHT) ? op.tT[k - 1] : 0.0;
-  const double tB = (f & kNHB) ? op.tB[k - 1] : 0.0;
+// Operator row with the seven field values given: bottom, south, west,
+// centre, east, north, top; t* are the face factors (read only where the
+// face flag is set).
+__device__ __forceinline__ double nh_row(uint32_t f, double tE, double tW, double tN, double tS, double tT, double tB,
+                                         double vb, double vs, double vw, double vc, double ve, double vn, double vt) {
   double c = 0.0;  // make_coeff_non_hydro's accumulation order
   if (f & kNHE) c = __dsub_rn(c, tE);
   if (f & kNHW) c = __dsub_rn(c, tW);
@@ -72,14 +71,30 @@ __device__ __forceinline__ double nh_apply(const NHOp& op, const NHGeo& G, int i
   if (f & kNHB) c = __dsub_rn(c, tB);
   // apply_op_3D: kk outermost, then jj, then ii; zero coefficients add nothing
   double a = 0.0;
-  if (f & kNHB) a = __dadd_rn(a, __dmul_rn(tB, fetch(0, 0, -1)));
-  if (f & kNHS) a = __dadd_rn(a, __dmul_rn(tS, fetch(0, -1, 0)));
-  if (f & kNHW) a = __dadd_rn(a, __dmul_rn(tW, fetch(-1, 0, 0)));
-  a = __dadd_rn(a, __dmul_rn(c, fetch(0, 0, 0)));
-  if (f & kNHE) a = __dadd_rn(a, __dmul_rn(tE, fetch(1, 0, 0)));
-  if (f & kNHN) a = __dadd_rn(a, __dmul_rn(tN, fetch(0, 1, 0)));
-  if (f & kNHT) a = __dadd_rn(a, __dmul_rn(tT, fetch(0, 0, 1)));
+  if (f & kNHB) a = __dadd_rn(a, __dmul_rn(tB, vb));
+  if (f & kNHS) a = __dadd_rn(a, __dmul_rn(tS, vs));
+  if (f & kNHW) a = __dadd_rn(a, __dmul_rn(tW, vw));
+  a = __dadd_rn(a, __dmul_rn(c, vc));
+  if (f & kNHE) a = __dadd_rn(a, __dmul_rn(tE, ve));
+  if (f & kNHN) a = __dadd_rn(a, __dmul_rn(tN, vn));
+  if (f & kNHT) a = __dadd_rn(a, __dmul_rn(tT, vt));
   return a;
+}
+
+// Operator row of cell (i,j,k) applied to a field given by fetch(di, dj, dk).
+template <class Fetch>
+__device__ __forceinline__ double nh_apply(const NHOp& op, const NHGeo& G, int i, int j, int k, uint32_t f,
+                                           const Fetch& fetch) {
+  const size_t q2 = G.g.at(i, j);  // the tables are read-only for the life of the operator
+  const double tE = (f & kNHE) ? __ldg(op.tE + q2) : 0.0;
+  const double tW = (f & kNHW) ? __ldg(op.tW + q2) : 0.0;
+  const double tN = (f & kNHN) ? __ldg(op.tN + j + 1) : 0.0;
+  const double tS = (f & kNHS) ? __ldg(op.tS + j + 1) : 0.0;
+  const double tT = (f & kNHT) ? __ldg(op.tT + k - 1) : 0.0;
+  const double tB = (f & kNHB) ? __ldg(op.tB + k - 1) : 0.0;
+  return nh_row(f, tE, tW, tN, tS, tT, tB, (f & kNHB) ? fetch(0, 0, -1) : 0.0, (f & kNHS) ? fetch(0, -1, 0) : 0.0,
+                (f & kNHW) ? fetch(-1, 0, 0) : 0.0, fetch(0, 0, 0), (f & kNHE) ? fetch(1, 0, 0) : 0.0,
+                (f & kNHN) ? fetch(0, 1, 0) : 0.0, (f & kNHT) ? fetch(0, 0, 1) : 0.0);
 }
 
 // setcyclic_xyz (parallel_none.f90) applied per level: store v at (i,j,k) and
@@ -95,9 +110,32 @@ __device__ __forceinline__ void nh_add_cyclic(T* __restrict__ a, const NHGeo& G,
 
 struct CGResult;
 
-struct NHParams {
+// Bricks of the CG sweeps: 32 cells in i (one per lane) x ty in j x kc in k,
+// kc = (8/ty) * kw.  Warp w works on row jj = w % ty and marches over kw
+// levels from (w / ty) * kw.  Per brick and pipeline stage, shared memory
+// holds the res and s boxes (brick + one-cell halo: i0-2..i0+33, i.e. 36
+// doubles starting on a 16-byte boundary of the padded layout, j0-1..j0+ty,
+// k0-1..k0+kc), the brick's p (sweep B) and its flag bytes.
+constexpr int kNHBoxX = 36;
+__host__ __device__ constexpr size_t nh_al(size_t b) { return (b + 127) / 128 * 128; }
+__host__ __device__ constexpr size_t nh_rs_bytes(int ty, int kc) { return (size_t)kNHBoxX * (ty + 2) * (kc + 2) * 8; }
+__host__ __device__ constexpr size_t nh_p_bytes(int ty, int kc) { return (size_t)32 * ty * kc * 8; }
+__host__ __device__ constexpr size_t nh_f_bytes(int ty, int kc) { return (size_t)32 * ty * kc; }
+__host__ __device__ constexpr size_t nh_stage_bytes(int ty, int kc) {
+  return 2 * nh_al(nh_rs_bytes(ty, kc)) + nh_al(nh_p_bytes(ty, kc)) + nh_al(nh_f_bytes(ty, kc));
+}
+// two pipeline stages + two mbarriers
+__host__ __device__ constexpr size_t nh_smem_bytes(int ty, int kc) { return 2 * nh_stage_bytes(ty, kc) + 128; }
+constexpr size_t kNHSmemMax = 220 * 1024;
+
+struct alignas(64) NHParams {
+  CUtensorMap map_res[2], map_s[2];  // 3-D (pitch, ny+4, nz) maps, box 36 x (ty+2) x (kc+2)
+  CUtensorMap map_p;                 // 3-D (pitch, ny+4, nz) map of p, box 32 x ty x kc
+  CUtensorMap map_f;                 // 3-D (fx, ny, nz) map of the flags, box 32 x ty x kc
   NHGeo G;
   NHOp op;
+  int ty, kw, kc;                    // brick shape
+  int nbx, nby, nbz;                 // bricks per dimension
   const double* forc;  // Fortran layout (nx+4, ny+4, nz), device
   double* p;           // padded p_non_hydro(:,:,:,taup1), in/out
   double* res[2];      // padded residual, double-buffered (halo = cyclic copies)

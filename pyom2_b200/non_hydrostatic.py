@@ -75,6 +75,10 @@ class NonHydrostatic:
         """Blocks of the CG launch (0 = automatic)."""
         _abi.check(self._L.pyomgpu_nh_set_grid(self._h, int(blocks)))
 
+    def set_brick(self, ty: int, kc: int):
+        """Brick shape 32 x ty x kc of the CG sweeps ((0, 0) = automatic)."""
+        _abi.check(self._L.pyomgpu_nh_set_brick(self._h, int(ty), int(kc)))
+
     def apply_op_3d(self, p):
         """non_hydrostatic.f90:247-276: ``res = A p`` over the interior, zero halo."""
         res = np.zeros(self.shape, order="F") if not _is_torch(p) else _torch_like(p)
