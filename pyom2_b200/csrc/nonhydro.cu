@@ -4,21 +4,28 @@
 //
 // Per CG iteration the kernel makes two sweeps over bricks of 32 x ty x kc
 // cells, separated by grid barriers that carry the reductions (dot_3D /
-// absmax_3D, :279-322).  Each brick's res and s boxes (brick + one-cell halo)
-// come into shared memory by TMA through a two-stage pipeline (the next
-// brick loads while this one is computed), and s_n = res + bq s_{n-1} is
-// formed in the box, so s_n is never stored before it is complete:
+// absmax_3D, :279-322).  A brick's operands come into shared memory by TMA
+// through a two-stage pipeline (the next brick loads while this one is
+// computed), and every warp marches up one column of the brick with the
+// field below, at and above its cell in registers:
 //
-//   sweep A  partial sums of (s_n, A s_n) and max|s_n| over maskT
-//   sweep B  the same s_n and A s_n again, then res -= alpha A s_n,
-//            p += alpha s_n; res and s_n go to the other buffer of their
-//            double-buffered pair; partial sums of (res, res)
+//   sweep A  boxes (brick + one-cell halo) of res and s_{n-1}; forms
+//            s_n = res + bq s_{n-1} in the box; partial sums of
+//            (s_n, A s_n) and max|s_n| over maskT; writes s_n
+//   sweep B  the s_n box, res and p of the brick; A s_n again;
+//            res -= alpha A s_n (in place), p += alpha s_n; partial
+//            sums of (res, res)
 //
-// so an iteration streams 64 bytes per cell from HBM (read res and s twice,
-// read and write p, write res and s) plus the flag byte twice, and stores no
-// A s vector.  The convergence test of iteration n needs max|s_{n+1}|, so it
+// An iteration streams 64 bytes per cell from HBM (res and s_{n-1} read, s_n
+// written and read back, res and p read and written) plus the flag byte
+// twice, and stores no A s vector.  The search direction alternates between
+// two buffers (s_{n-1} is still read by neighbouring bricks while s_n is
+// written).  The convergence test of iteration n needs max|s_{n+1}|, so it
 // runs after sweep A of iteration n+1, exactly as the reference evaluates it
-// after forming the new direction.
+// after forming the new direction.  Cyclic halos are written by the owner of
+// the source cell (setcyclic_xyz); the kernel is compiled for each
+// combination of cyclic x / cyclic y so that closed domains carry no halo
+// logic.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -57,38 +64,56 @@ __device__ __forceinline__ ptrdiff_t nh_off(const NHGeo& G, int di, int dj, int 
   return (ptrdiff_t)di + (ptrdiff_t)dj * G.g.pitch + (ptrdiff_t)dk * (ptrdiff_t)G.plane;
 }
 
-}  // namespace
-
-// p += d at the setcyclic_xyz halo copies of (i,j) on level k (not at (i,j) itself).
-__device__ __forceinline__ void nh_add_copies(double* __restrict__ a, const NHGeo& G, int i, int j, int k, double d) {
-  double* lv = a + (size_t)(k - 1) * G.plane;
-  int xc, yc;
-  cyclic_copies(G.g, i, j, xc, yc);
-  if (xc != 0x7fffffff) lv[G.g.at(xc, j)] += d;
-  if (yc != 0x7fffffff) {
-    lv[G.g.at(i, yc)] += d;
-    if (xc != 0x7fffffff) lv[G.g.at(xc, yc)] += d;
+// Offsets (relative to cell (i,j) on the same level) of the setcyclic_xyz halo
+// copies of (i,j); 0 = none.  At most three: x, y and the corner.
+template <bool CX, bool CY>
+__device__ __forceinline__ void nh_copy_offsets(const Geo& g, int i, int j, ptrdiff_t& ox, ptrdiff_t& oy) {
+  ox = 0;
+  oy = 0;
+  if (CX) ox = (i <= kOnx) ? (ptrdiff_t)g.nx : ((i > g.nx - kOnx) ? -(ptrdiff_t)g.nx : 0);
+  if (CY) oy = (j <= kOnx) ? (ptrdiff_t)g.ny * g.pitch : ((j > g.ny - kOnx) ? -(ptrdiff_t)g.ny * g.pitch : 0);
+}
+template <bool CX, bool CY>
+__device__ __forceinline__ void nh_put(double* __restrict__ a, size_t q, ptrdiff_t ox, ptrdiff_t oy, double v) {
+  a[q] = v;
+  if (CX && ox) a[q + ox] = v;
+  if (CY && oy) {
+    a[q + oy] = v;
+    if (CX && ox) a[q + ox + oy] = v;
+  }
+}
+template <bool CX, bool CY>
+__device__ __forceinline__ void nh_add_halo(double* __restrict__ a, size_t q, ptrdiff_t ox, ptrdiff_t oy, double d) {
+  if (CX && ox) a[q + ox] += d;
+  if (CY && oy) {
+    a[q + oy] += d;
+    if (CX && ox) a[q + ox + oy] += d;
   }
 }
 
+}  // namespace
+
 // One sweep of this block over its bricks (brick b = blockIdx.x + m gridDim.x).
-// TMA brings the res/s boxes of buffer `cur`, the flags and (sweep B) p into
-// one of two pipeline stages while the other stage is computed; s_n = res +
-// bq s is formed in the box; then every warp marches up its column of the
-// brick, keeping s_n below/at/above the cell in registers, and calls
-// cell(i, j, k, f, A s_n, s_n, res, p) for each interior cell (sweep A: only
-// cells with maskT).  Returns false after a time-out (error recorded, the
-// other stage's copy waited for).
+//   sweep A (kB false): stage = res box, s box (buffer cur), flags; s = res +
+//     bq s is formed in the box;
+//   sweep B (kB true):  stage = s box (buffer cur ^ 1), the brick's res and p,
+//     flags.
+// Then every warp marches up its column and calls
+// cell(i, j, k, f, q, A s, s, res, p) for each interior cell (sweep A: only
+// cells with maskT; q = padded index; res and p only in sweep B).  Returns
+// false after a time-out (error recorded, the other stage's copy waited for).
 template <bool kB, class Cell>
 __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, unsigned char* smem, uint64_t* bar,
                                          uint32_t (&phase)[2], const Cell& cell) {
   const int TY = P.ty, KW = P.kw, KC = P.kc, BY = TY + 2, BXY = kNHBoxX * BY;
   const int nbox = BXY * (KC + 2);
   const size_t rs = nh_al(nh_rs_bytes(TY, KC)), pb = nh_al(nh_p_bytes(TY, KC)), stage = nh_stage_bytes(TY, KC);
-  const uint32_t tx_bytes =
-      (uint32_t)(2 * nh_rs_bytes(TY, KC) + nh_f_bytes(TY, KC) + (kB ? nh_p_bytes(TY, KC) : 0));
+  const size_t fo = nh_flags_off(TY, KC);
+  const uint32_t tx_bytes = (uint32_t)(kB ? nh_rs_bytes(TY, KC) + 2 * nh_p_bytes(TY, KC) + nh_f_bytes(TY, KC)
+                                          : 2 * nh_rs_bytes(TY, KC) + nh_f_bytes(TY, KC));
   const int nbr = P.nbx * P.nby * P.nbz;
   const int nx = P.G.g.nx, ny = P.G.g.ny, nz = P.G.nz;
+  const size_t plane = P.G.plane;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int jj = warp % TY, kk0 = (warp / TY) * KW;
   auto issue = [&](int b, int st) {
@@ -97,14 +122,20 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
     fence_proxy_async_smem();
     fence_proxy_async_global();
     mbar_arrive_expect_tx(&bar[st], tx_bytes);
-    // res/s boxes: padded column of Fortran i0-2 (even, 16-byte aligned), row of j0-1, level index of k0-1
+    // boxes: padded column of Fortran i0-2 (even, 16-byte aligned), row of j0-1, level index of k0-1;
+    // brick arrays: padded column of i0 (even), row of j0, level index of k0
     const int x = 32 * bx + 2, y = TY * by + 1, z = KC * bz - 1;
-    tma_load_3d(B, &P.map_res[cur], x, y, z, &bar[st]);
-    tma_load_3d(B + rs, &P.map_s[cur], x, y, z, &bar[st]);
-    // p: padded column of i0 (even), row of j0, level index of k0
-    if (kB) tma_load_3d(B + 2 * rs, &P.map_p, 32 * bx + 4, TY * by + 2, KC * bz, &bar[st]);
+    const int xb = 32 * bx + 4, yb = TY * by + 2, zb = KC * bz;
+    if (!kB) {  // box 0 = s_{n-1}, box 1 = res
+      tma_load_3d(B, &P.map_s[cur], x, y, z, &bar[st]);
+      tma_load_3d(B + rs, &P.map_res, x, y, z, &bar[st]);
+    } else {  // box 0 = s_n, then the brick's res and p
+      tma_load_3d(B, &P.map_s[cur ^ 1], x, y, z, &bar[st]);
+      tma_load_3d(B + rs, &P.map_res_brick, xb, yb, zb, &bar[st]);
+      tma_load_3d(B + rs + pb, &P.map_p, xb, yb, zb, &bar[st]);
+    }
     // flags: column i0-1 (a multiple of 32 bytes), row j0-1, level k0-1
-    tma_load_3d(B + 2 * rs + pb, &P.map_f, 32 * bx, TY * by, KC * bz, &bar[st]);
+    tma_load_3d(B + fo, &P.map_f, 32 * bx, TY * by, KC * bz, &bar[st]);
   };
   int c = 0;
   if ((int)blockIdx.x < nbr && threadIdx.x == 0) issue(blockIdx.x, 0);
@@ -123,34 +154,47 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
       return false;
     }
     unsigned char* B = smem + (size_t)st * stage;
-    const double* R = reinterpret_cast<const double*>(B);
-    double* S = reinterpret_cast<double*>(B + rs);
-    const double* Pb = reinterpret_cast<const double*>(B + 2 * rs);
-    const uint8_t* F = B + 2 * rs + pb;
-    for (int e = threadIdx.x; e < nbox; e += kNHThreads) S[e] = __dadd_rn(R[e], __dmul_rn(bq, S[e]));
-    __syncthreads();
+    double* S = reinterpret_cast<double*>(B);
+    const double* Rb = reinterpret_cast<const double*>(B + rs);       // sweep A: res box; B: the brick's res
+    const double* Pb = reinterpret_cast<const double*>(B + rs + pb);  // sweep B: the brick's p
+    const uint8_t* F = B + fo;
+    if (!kB) {
+      // s_n = res + rsnew/rsold * p (:189), separately rounded, over the box (box 0 = s, box 1 = res)
+      const double* R = Rb;
+      for (int e = threadIdx.x; e < nbox; e += kNHThreads) S[e] = __dadd_rn(R[e], __dmul_rn(bq, S[e]));
+      __syncthreads();
+    }
     const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
     const int i = 1 + 32 * bx + lane, j = 1 + TY * by + jj;
     if (i <= nx && j <= ny) {
       const size_t q2 = P.G.g.at(i, j);
       const double tE = __ldg(P.op.tE + q2), tW = __ldg(P.op.tW + q2);
       const double tN = __ldg(P.op.tN + j + 1), tS = __ldg(P.op.tS + j + 1);
-      int cc = ((kk0 + 1) * BY + jj + 1) * kNHBoxX + lane + 2;
-      double sdn = S[cc - BXY], sc = S[cc];
       int k = 1 + KC * bz + kk0;
-      for (int m = 0; m < KW && k <= nz; m++, k++, cc += BXY) {
+      size_t q = (size_t)(k - 1) * plane + q2;
+      int cc = ((kk0 + 1) * BY + jj + 1) * kNHBoxX + lane + 2;
+      int fl = (kk0 * TY + jj) * 32 + lane;
+      double sdn = S[cc - BXY], sc = S[cc];
+      const int mend = min(KW, nz - k + 1);
+#pragma unroll 2
+      for (int m = 0; m < mend; m++) {
         const double sup = S[cc + BXY];
-        const int fl = ((kk0 + m) * TY + jj) * 32 + lane;
         const uint32_t f = F[fl];
         if (kB || (f & kNHMaskT)) {
           const double tT = (f & kNHT) ? __ldg(P.op.tT + k - 1) : 0.0;
           const double tB = (f & kNHB) ? __ldg(P.op.tB + k - 1) : 0.0;
           const double a = nh_row(f, tE, tW, tN, tS, tT, tB, sdn, S[cc - kNHBoxX], S[cc - 1], sc, S[cc + 1],
                                   S[cc + kNHBoxX], sup);
-          cell(i, j, k, f, a, sc, R[cc], kB ? Pb[fl] : 0.0);
+          cell(i, j, k, f, q, a, sc, kB ? Rb[fl] : 0.0, kB ? Pb[fl] : 0.0);
+        } else if (!kB) {
+          cell(i, j, k, f, q, 0.0, sc, 0.0, 0.0);  // sweep A stores s_n everywhere
         }
         sdn = sc;
         sc = sup;
+        k++;
+        q += plane;
+        cc += BXY;
+        fl += 32 * TY;
       }
     }
     __syncthreads();  // stage st is free for the copy issued next iteration
@@ -158,6 +202,7 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
   return true;
 }
 
+template <bool CX, bool CY>
 __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_constant__ NHParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
   const NHGeo G = P.G;
@@ -175,6 +220,7 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
   uint32_t phase[2] = {0u, 0u};
   unsigned long long epoch = 0;
   double* __restrict__ pnh = P.p;
+  double* __restrict__ res = P.res;
 
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
@@ -197,7 +243,9 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
                                 [&](int di, int dj, int dk) { return __ldcg(pnh + q + nh_off(G, di, dj, dk)); });
       const double fo = P.forc[fidx3(nx, (int)ny, i, j, k)];
       const double r = __dsub_rn(fo, a);
-      nh_store_cyclic(P.res[1], G, i, j, k, r);
+      ptrdiff_t ox, oy;
+      nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
+      nh_put<CX, CY>(res, q, ox, oy, r);
       if (f & kNHMaskT) {
         v[0] += r * r;
         v[1] += fo * fo;
@@ -237,12 +285,19 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
     const int cur = n & 1;
     // -------------------------------------------------------------- sweep A
     {
+      double* __restrict__ Sn = P.s[cur ^ 1];
       double acc_dot = 0.0, acc_max = 0.0;
-      const bool ok = nh_sweep<false>(P, cur, bq, smem, bar, phase,
-                                      [&](int, int, int, uint32_t, double a, double sc, double, double) {
-                                        acc_dot += sc * a;
-                                        acc_max = fmax(acc_max, fabs(sc));
-                                      });
+      const bool ok = nh_sweep<false>(
+          P, cur, bq, smem, bar, phase,
+          [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double, double) {
+            ptrdiff_t ox, oy;
+            nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
+            nh_put<CX, CY>(Sn, q, ox, oy, sc);
+            if (f & kNHMaskT) {  // only masked products enter the sums
+              acc_dot += sc * a;
+              acc_max = fmax(acc_max, fabs(sc));
+            }
+          });
       if (!ok) return;
       double v[2] = {acc_dot, acc_max}, out[2];
       block_reduce<2, 1, kNHThreads>(v, out);
@@ -298,18 +353,18 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
     if (sAs == 0.0) goto done_ok;  // :185
     {
       const double alpha = beta / sAs;
-      double* __restrict__ Rn = P.res[cur ^ 1];
-      double* __restrict__ Sn = P.s[cur ^ 1];
       // ------------------------------------------------------------ sweep B
       double acc_r = 0.0;
       const bool ok = nh_sweep<true>(
-          P, cur, bq, smem, bar, phase, [&](int i, int j, int k, uint32_t f, double a, double sc, double rc, double pc) {
+          P, cur, bq, smem, bar, phase,
+          [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double rc, double pc) {
             const double r = __dsub_rn(rc, __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
             const double d = __dmul_rn(alpha, sc);                // p_non_hydro + alpha*p (:187)
-            pnh[G.at(i, j, k)] = __dadd_rn(pc, d);
-            nh_add_copies(pnh, G, i, j, k, d);
-            nh_store_cyclic(Rn, G, i, j, k, r);
-            nh_store_cyclic(Sn, G, i, j, k, sc);
+            ptrdiff_t ox, oy;
+            nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
+            pnh[q] = __dadd_rn(pc, d);
+            nh_add_halo<CX, CY>(pnh, q, ox, oy, d);
+            nh_put<CX, CY>(res, q, ox, oy, r);
             if (f & kNHMaskT) acc_r += r * r;
           });
       if (!ok) return;
@@ -353,7 +408,10 @@ done:
   }
 }
 
-const void* nh_cg_kernel_ptr() { return (const void*)nh_cg_kernel; }
+const void* nh_cg_kernel_ptr(bool cx, bool cy) {
+  if (cx) return cy ? (const void*)nh_cg_kernel<true, true> : (const void*)nh_cg_kernel<true, false>;
+  return cy ? (const void*)nh_cg_kernel<false, true> : (const void*)nh_cg_kernel<false, false>;
+}
 
 namespace {
 
@@ -419,7 +477,7 @@ struct pyomgpu_nh {
   size_t nf = 0;  // Fortran-layout elements (nx+4)(ny+4)nz
   uint8_t* flags = nullptr;
   double *tE = nullptr, *tW = nullptr, *tN = nullptr, *tS = nullptr, *tT = nullptr, *tB = nullptr;
-  double *p = nullptr, *res[2] = {}, *s[2] = {}, *stage_f = nullptr, *stage_p = nullptr;
+  double *p = nullptr, *res = nullptr, *s[2] = {}, *stage_f = nullptr, *stage_p = nullptr;
   SyncCtl* ctl = nullptr;
   double* slots = nullptr;
   CGResult* d_result = nullptr;
@@ -432,7 +490,7 @@ struct pyomgpu_nh {
   unsigned stall_next = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   ~pyomgpu_nh() {
-    void* ptrs[] = {flags, tE, tW, tN, tS, tT, tB, p, res[0], res[1], s[0], s[1], stage_f, stage_p, ctl, slots,
+    void* ptrs[] = {flags, tE, tW, tN, tS, tT, tB, p, res, s[0], s[1], stage_f, stage_p, ctl, slots,
                     d_result};
     for (void* q : ptrs)
       if (q) cudaFree(q);
@@ -582,8 +640,8 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
   int rc = 0;
   if ((rc = nupload(&h->flags, flags)) || (rc = nupload(&h->tE, tE)) || (rc = nupload(&h->tW, tW)) ||
       (rc = nupload(&h->tN, tN)) || (rc = nupload(&h->tS, tS)) || (rc = nupload(&h->tT, tT)) ||
-      (rc = nupload(&h->tB, tB)) || (rc = nalloc(&h->p, np)) || (rc = nalloc(&h->res[0], np)) ||
-      (rc = nalloc(&h->res[1], np)) || (rc = nalloc(&h->s[0], np)) || (rc = nalloc(&h->s[1], np)) ||
+      (rc = nupload(&h->tB, tB)) || (rc = nalloc(&h->p, np)) || (rc = nalloc(&h->res, np)) ||
+      (rc = nalloc(&h->s[0], np)) || (rc = nalloc(&h->s[1], np)) ||
       (rc = nalloc(&h->stage_f, h->nf)) || (rc = nalloc(&h->stage_p, h->nf)) || (rc = nalloc(&h->ctl, 1)) ||
       (rc = nalloc(&h->d_result, 1))) {
     delete h;
@@ -595,8 +653,12 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
     delete h;
     return nfail(PYOMGPU_ECUDA, "nh_create: cudaMemset");
   }
-  if (cudaFuncSetAttribute(nh_cg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNHSmemMax) !=
-      cudaSuccess) {
+  bool attr_ok = true;
+  for (int v = 0; v < 4; v++)
+    attr_ok = attr_ok && cudaFuncSetAttribute(nh_cg_kernel_ptr(v & 1, v >> 1),
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kNHSmemMax) == cudaSuccess;
+  if (!attr_ok) {
     cudaGetLastError();
     delete h;
     return nfail(PYOMGPU_ECUDA, "nh_create: shared-memory attribute");
@@ -656,11 +718,11 @@ int32_t pyomgpu_apply_op_3d(pyomgpu_nh* h, const double* p1, double* res, pyomgp
   if (int rc = nh_stage(h, p1, h->stage_p, &pin, st)) return rc;
   const size_t bytes = h->G.size() * sizeof(double);
   launch_nh_pack(h->G, pin, h->p, st);
-  NCK(cudaMemsetAsync(h->res[0], 0, bytes, st));
-  launch_nh_apply(h->G, h->op, h->p, h->res[0], st);
+  NCK(cudaMemsetAsync(h->res, 0, bytes, st));
+  launch_nh_apply(h->G, h->op, h->p, h->res, st);
   const bool dev_out = nh_on_device(res);
   double* dst = dev_out ? res : h->stage_f;
-  launch_nh_unpack(h->G, h->res[0], dst, st);
+  launch_nh_unpack(h->G, h->res, dst, st);
   NCK(cudaGetLastError());
   if (!dev_out) NCK(cudaMemcpyAsync(res, h->stage_f, h->nf * sizeof(double), cudaMemcpyDeviceToHost, st));
   NCK(cudaStreamSynchronize(st));
@@ -678,15 +740,14 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
   if (int rc = nh_stage(h, p, h->stage_p, &pin, st)) return rc;
   const size_t bytes = h->G.size() * sizeof(double);
   launch_nh_pack(h->G, pin, h->p, st);
-  for (double* b : {h->res[0], h->res[1], h->s[0], h->s[1]}) NCK(cudaMemsetAsync(b, 0, bytes, st));
+  for (double* b : {h->res, h->s[0], h->s[1]}) NCK(cudaMemsetAsync(b, 0, bytes, st));
   NCK(cudaMemsetAsync(h->ctl, 0, sizeof(SyncCtl), st));
   NHParams P{};
   P.G = h->G;
   P.op = h->op;
   P.forc = fdev;
   P.p = h->p;
-  P.res[0] = h->res[0];
-  P.res[1] = h->res[1];
+  P.res = h->res;
   P.s[0] = h->s[0];
   P.s[1] = h->s[1];
   P.eps = eps;
@@ -724,15 +785,17 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
     const uint64_t fdims[3] = {(uint64_t)h->op.fx, (uint64_t)h->G.g.ny, (uint64_t)h->G.nz};
     const uint64_t fstrides[2] = {(uint64_t)h->op.fx, (uint64_t)h->op.fx * h->G.g.ny};
     int bad = 0;
+    bad |= encode_map(&P.map_res, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->res, dims, strides, box);
+    bad |= encode_map(&P.map_res_brick, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->res, dims, strides, pbox);
     for (int b = 0; b < 2; b++)
-      bad |= encode_map(&P.map_res[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->res[b], dims, strides, box) |
-             encode_map(&P.map_s[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->s[b], dims, strides, box);
+      bad |= encode_map(&P.map_s[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->s[b], dims, strides, box);
     bad |= encode_map(&P.map_p, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->p, dims, strides, pbox);
     bad |= encode_map(&P.map_f, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->flags, fdims, fstrides, pbox);
     if (bad) return nfail(PYOMGPU_ECUDA, "congrad_non_hydro: cuTensorMapEncodeTiled failed");
   }
   int per_sm = 0;
-  NCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nh_cg_kernel, kNHThreads, smem));
+  const void* kfn = nh_cg_kernel_ptr(h->cyclic_x != 0, h->cyclic_y != 0);
+  NCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kNHThreads, smem));
   if (per_sm < 1) return nfail(PYOMGPU_EINVAL, "congrad_non_hydro: brick does not fit on an SM");
   const int coresident = std::min(per_sm * h->nsm, h->max_blocks);
   const int nbricks = P.nbx * P.nby * P.nbz;
@@ -740,7 +803,7 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
   grid = std::max(1, grid);
   void* args[] = {&P};
   NCK(cudaEventRecord(h->e0, st));
-  NCK(cudaLaunchCooperativeKernel(nh_cg_kernel_ptr(), dim3(grid), dim3(kNHThreads), args, smem, st));
+  NCK(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kNHThreads), args, smem, st));
   NCK(cudaEventRecord(h->e1, st));
   NCK(cudaMemcpyAsync(h->h_result, h->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
   NCK(cudaMemcpyAsync(h->h_err, &h->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -113,23 +113,33 @@ struct CGResult;
 // Bricks of the CG sweeps: 32 cells in i (one per lane) x ty in j x kc in k,
 // kc = (8/ty) * kw.  Warp w works on row jj = w % ty and marches over kw
 // levels from (w / ty) * kw.  Per brick and pipeline stage, shared memory
-// holds the res and s boxes (brick + one-cell halo: i0-2..i0+33, i.e. 36
-// doubles starting on a 16-byte boundary of the padded layout, j0-1..j0+ty,
-// k0-1..k0+kc), the brick's p (sweep B) and its flag bytes.
+// holds two boxes (brick + one-cell halo: i0-2..i0+33, i.e. 36 doubles
+// starting on a 16-byte boundary of the padded layout, j0-1..j0+ty,
+// k0-1..k0+kc) -- sweep A: res and s; sweep B: s and, in the second box's
+// place, the brick's res and p -- and the brick's flag bytes.
 constexpr int kNHBoxX = 36;
 __host__ __device__ constexpr size_t nh_al(size_t b) { return (b + 127) / 128 * 128; }
 __host__ __device__ constexpr size_t nh_rs_bytes(int ty, int kc) { return (size_t)kNHBoxX * (ty + 2) * (kc + 2) * 8; }
 __host__ __device__ constexpr size_t nh_p_bytes(int ty, int kc) { return (size_t)32 * ty * kc * 8; }
 __host__ __device__ constexpr size_t nh_f_bytes(int ty, int kc) { return (size_t)32 * ty * kc; }
+// stage layout: [box 0][region 1: box 1, or the brick's res then p][flags]
+__host__ __device__ constexpr size_t nh_region1_bytes(int ty, int kc) {
+  return nh_al(nh_rs_bytes(ty, kc)) > 2 * nh_al(nh_p_bytes(ty, kc)) ? nh_al(nh_rs_bytes(ty, kc))
+                                                                       : 2 * nh_al(nh_p_bytes(ty, kc));
+}
+__host__ __device__ constexpr size_t nh_flags_off(int ty, int kc) {
+  return nh_al(nh_rs_bytes(ty, kc)) + nh_region1_bytes(ty, kc);
+}
 __host__ __device__ constexpr size_t nh_stage_bytes(int ty, int kc) {
-  return 2 * nh_al(nh_rs_bytes(ty, kc)) + nh_al(nh_p_bytes(ty, kc)) + nh_al(nh_f_bytes(ty, kc));
+  return nh_flags_off(ty, kc) + nh_al(nh_f_bytes(ty, kc));
 }
 // two pipeline stages + two mbarriers
 __host__ __device__ constexpr size_t nh_smem_bytes(int ty, int kc) { return 2 * nh_stage_bytes(ty, kc) + 128; }
 constexpr size_t kNHSmemMax = 220 * 1024;
 
 struct alignas(64) NHParams {
-  CUtensorMap map_res[2], map_s[2];  // 3-D (pitch, ny+4, nz) maps, box 36 x (ty+2) x (kc+2)
+  CUtensorMap map_res, map_s[2];     // 3-D (pitch, ny+4, nz) maps, box 36 x (ty+2) x (kc+2)
+  CUtensorMap map_res_brick;         // the same array as map_res, box 32 x ty x kc
   CUtensorMap map_p;                 // 3-D (pitch, ny+4, nz) map of p, box 32 x ty x kc
   CUtensorMap map_f;                 // 3-D (fx, ny, nz) map of the flags, box 32 x ty x kc
   NHGeo G;
@@ -138,7 +148,7 @@ struct alignas(64) NHParams {
   int nbx, nby, nbz;                 // bricks per dimension
   const double* forc;  // Fortran layout (nx+4, ny+4, nz), device
   double* p;           // padded p_non_hydro(:,:,:,taup1), in/out
-  double* res[2];      // padded residual, double-buffered (halo = cyclic copies)
+  double* res;         // padded residual (halo = cyclic copies), updated in place
   double* s[2];        // padded search direction, double-buffered
   double eps;          // congr_epsilon_non_hydro
   int max_it;          // congr_max_itts_non_hydro
@@ -150,7 +160,7 @@ struct alignas(64) NHParams {
   CGResult* out;
 };
 
-const void* nh_cg_kernel_ptr();
+const void* nh_cg_kernel_ptr(bool cyclic_x, bool cyclic_y);
 void launch_nh_apply(const NHGeo& G, const NHOp& op, const double* p, double* res, cudaStream_t st);
 void launch_nh_pack(const NHGeo& G, const double* user, double* padded, cudaStream_t st);
 void launch_nh_unpack(const NHGeo& G, const double* padded, double* user, cudaStream_t st);
