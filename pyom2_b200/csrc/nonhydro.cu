@@ -142,17 +142,22 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
   for (int b = blockIdx.x; b < nbr; b += gridDim.x, c++) {
     const int st = c & 1;
     const int bn = b + (int)gridDim.x;
-    if (bn < nbr && threadIdx.x == 0) issue(bn, st ^ 1);
+    const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
+    const int i = 1 + 32 * bx + lane, j = 1 + TY * by + jj;
+    const bool col = i <= nx && j <= ny;
+    // the column's metric factors load while the brick's copy is in flight
+    const size_t q2 = col ? P.G.g.at(i, j) : 0;
+    const double tE = col ? __ldg(P.op.tE + q2) : 0.0, tW = col ? __ldg(P.op.tW + q2) : 0.0;
+    const double tN = col ? __ldg(P.op.tN + j + 1) : 0.0, tS = col ? __ldg(P.op.tS + j + 1) : 0.0;
+    // every thread is past brick c-1 here, so its stage can take brick c+1
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bar[st], phase[st], P.timeout_ns));
     phase[st] ^= 1u;
     if (!ok) {
-      if (threadIdx.x == 0) {
-        atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
-        if (bn < nbr) mbar_wait_bounded(&bar[st ^ 1], phase[st ^ 1], P.timeout_ns);
-      }
+      if (threadIdx.x == 0) atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
       __syncthreads();
       return false;
     }
+    if (bn < nbr && threadIdx.x == 0) issue(bn, st ^ 1);
     unsigned char* B = smem + (size_t)st * stage;
     double* S = reinterpret_cast<double*>(B);
     const double* Rb = reinterpret_cast<const double*>(B + rs);       // sweep A: res box; B: the brick's res
@@ -164,25 +169,20 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
       for (int e = threadIdx.x; e < nbox; e += kNHThreads) S[e] = __dadd_rn(R[e], __dmul_rn(bq, S[e]));
       __syncthreads();
     }
-    const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
-    const int i = 1 + 32 * bx + lane, j = 1 + TY * by + jj;
-    if (i <= nx && j <= ny) {
-      const size_t q2 = P.G.g.at(i, j);
-      const double tE = __ldg(P.op.tE + q2), tW = __ldg(P.op.tW + q2);
-      const double tN = __ldg(P.op.tN + j + 1), tS = __ldg(P.op.tS + j + 1);
-      int k = 1 + KC * bz + kk0;
+    int k = 1 + KC * bz + kk0;
+    const int mend = col ? min(KW, nz - k + 1) : 0;
+    if (mend > 0) {
       size_t q = (size_t)(k - 1) * plane + q2;
       int cc = ((kk0 + 1) * BY + jj + 1) * kNHBoxX + lane + 2;
       int fl = (kk0 * TY + jj) * 32 + lane;
       double sdn = S[cc - BXY], sc = S[cc];
-      const int mend = min(KW, nz - k + 1);
+      double tT = __ldg(P.op.tT + k - 1), tB = __ldg(P.op.tB + k - 1);  // vertical factors, one level ahead
 #pragma unroll 2
       for (int m = 0; m < mend; m++) {
         const double sup = S[cc + BXY];
         const uint32_t f = F[fl];
+        const double tTn = k < nz ? __ldg(P.op.tT + k) : 0.0, tBn = k < nz ? __ldg(P.op.tB + k) : 0.0;
         if (kB || (f & kNHMaskT)) {
-          const double tT = (f & kNHT) ? __ldg(P.op.tT + k - 1) : 0.0;
-          const double tB = (f & kNHB) ? __ldg(P.op.tB + k - 1) : 0.0;
           const double a = nh_row(f, tE, tW, tN, tS, tT, tB, sdn, S[cc - kNHBoxX], S[cc - 1], sc, S[cc + 1],
                                   S[cc + kNHBoxX], sup);
           cell(i, j, k, f, q, a, sc, kB ? Rb[fl] : 0.0, kB ? Pb[fl] : 0.0);
@@ -191,14 +191,16 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
         }
         sdn = sc;
         sc = sup;
+        tT = tTn;
+        tB = tBn;
         k++;
         q += plane;
         cc += BXY;
         fl += 32 * TY;
       }
     }
-    __syncthreads();  // stage st is free for the copy issued next iteration
   }
+  __syncthreads();  // the last stage is read to the end before the next sweep reuses it
   return true;
 }
 
