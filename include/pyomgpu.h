@@ -311,6 +311,8 @@ int32_t pyomgpu_nh_set_grid(pyomgpu_nh* nh, int32_t blocks);
 /* Brick shape of the CG sweeps: 32 x ty x kc cells staged with their halo in
  * shared memory (0, 0 = automatic: ty = min(8, ny), kc from a 26 KB box). */
 int32_t pyomgpu_nh_set_brick(pyomgpu_nh* nh, int32_t ty, int32_t kc);
+/* TMA pipeline depth of the CG sweeps: 2..4 stages (0 = automatic, 2). */
+int32_t pyomgpu_nh_set_stages(pyomgpu_nh* nh, int32_t stages);
 /* res = A p1 over the interior, zero halo (apply_op_3D).  (nx+4, ny+4, nz)
  * Fortran-layout arrays, host or device. */
 int32_t pyomgpu_apply_op_3d(pyomgpu_nh* nh, const double* p1, double* res, pyomgpu_stream stream);

@@ -93,20 +93,33 @@ __device__ __forceinline__ void nh_add_halo(double* __restrict__ a, size_t q, pt
 
 }  // namespace
 
+// Pipeline state of a block: per stage a "full" mbarrier (the TMA copy
+// landed) and an "empty" one (all eight warps are done with the stage).
+struct NHPipe {
+  uint64_t* full;
+  uint64_t* empty;
+  uint32_t fph;   // per stage: parity of the next full phase to wait for (all threads)
+  uint32_t eph;   // per stage: parity of the next empty phase to wait for (thread 0)
+  uint32_t used;  // per stage: filled at least once (thread 0)
+};
+
 // One sweep of this block over its bricks (brick b = blockIdx.x + m gridDim.x).
-//   sweep A (kB false): stage = res box, s box (buffer cur), flags; s = res +
-//     bq s is formed in the box;
-//   sweep B (kB true):  stage = s box (buffer cur ^ 1), the brick's res and p,
-//     flags.
-// Then every warp marches up its column and calls
-// cell(i, j, k, f, q, A s, s, res, p) for each interior cell (sweep A: only
-// cells with maskT; q = padded index; res and p only in sweep B).  Returns
-// false after a time-out (error recorded, the other stage's copy waited for).
+//   sweep A (kB false): stage = s_{n-1} box (buffer cur), res box, flags;
+//   sweep B (kB true):  stage = s_n box (buffer cur ^ 1), the brick's res
+//     and p, flags.
+// Thread 0 keeps ns - 1 bricks in flight ahead of the one computed, reusing a
+// stage once all eight warps have arrived on its empty barrier; warps run
+// through the bricks without block-wide barriers.  Each warp marches up its
+// column with the direction below, at and above its cell in registers
+// (sweep A forms s_n = res + bq s_{n-1} where it reads it) and calls
+// cell(i, j, k, f, q, A s, s, res, p) for each interior cell (sweep A: A s
+// only for cells with maskT, else 0; q = padded index; res and p only in
+// sweep B).  Returns false, the same in every thread, after a time-out
+// (error recorded).
 template <bool kB, class Cell>
-__device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, unsigned char* smem, uint64_t* bar,
-                                         uint32_t (&phase)[2], const Cell& cell) {
-  const int TY = P.ty, KW = P.kw, KC = P.kc, BY = TY + 2, BXY = kNHBoxX * BY;
-  const int nbox = BXY * (KC + 2);
+__device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, unsigned char* smem, NHPipe& pp,
+                                         const Cell& cell) {
+  const int TY = P.ty, KW = P.kw, KC = P.kc, NS = P.ns, BY = TY + 2, BXY = kNHBoxX * BY;
   const size_t rs = nh_al(nh_rs_bytes(TY, KC)), pb = nh_al(nh_p_bytes(TY, KC)), stage = nh_stage_bytes(TY, KC);
   const size_t fo = nh_flags_off(TY, KC);
   const uint32_t tx_bytes = (uint32_t)(kB ? nh_rs_bytes(TY, KC) + 2 * nh_p_bytes(TY, KC) + nh_f_bytes(TY, KC)
@@ -116,32 +129,44 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
   const size_t plane = P.G.plane;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int jj = warp % TY, kk0 = (warp / TY) * KW;
-  auto issue = [&](int b, int st) {
+  const int nmine = (int)blockIdx.x < nbr ? (nbr - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  // thread 0: put brick number m of this block into stage st once the stage is free
+  auto produce = [&](int m, int st) -> bool {
+    if (pp.used & (1u << st)) {
+      if (!mbar_wait_bounded(&pp.empty[st], (pp.eph >> st) & 1u, P.timeout_ns)) return false;
+      pp.eph ^= 1u << st;
+    }
+    pp.used |= 1u << st;
+    const int b = (int)blockIdx.x + m * (int)gridDim.x;
     const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
     unsigned char* B = smem + (size_t)st * stage;
     fence_proxy_async_smem();
     fence_proxy_async_global();
-    mbar_arrive_expect_tx(&bar[st], tx_bytes);
+    mbar_arrive_expect_tx(&pp.full[st], tx_bytes);
     // boxes: padded column of Fortran i0-2 (even, 16-byte aligned), row of j0-1, level index of k0-1;
     // brick arrays: padded column of i0 (even), row of j0, level index of k0
     const int x = 32 * bx + 2, y = TY * by + 1, z = KC * bz - 1;
     const int xb = 32 * bx + 4, yb = TY * by + 2, zb = KC * bz;
     if (!kB) {  // box 0 = s_{n-1}, box 1 = res
-      tma_load_3d(B, &P.map_s[cur], x, y, z, &bar[st]);
-      tma_load_3d(B + rs, &P.map_res, x, y, z, &bar[st]);
+      tma_load_3d(B, &P.map_s[cur], x, y, z, &pp.full[st]);
+      tma_load_3d(B + rs, &P.map_res, x, y, z, &pp.full[st]);
     } else {  // box 0 = s_n, then the brick's res and p
-      tma_load_3d(B, &P.map_s[cur ^ 1], x, y, z, &bar[st]);
-      tma_load_3d(B + rs, &P.map_res_brick, xb, yb, zb, &bar[st]);
-      tma_load_3d(B + rs + pb, &P.map_p, xb, yb, zb, &bar[st]);
+      tma_load_3d(B, &P.map_s[cur ^ 1], x, y, z, &pp.full[st]);
+      tma_load_3d(B + rs, &P.map_res_brick, xb, yb, zb, &pp.full[st]);
+      tma_load_3d(B + rs + pb, &P.map_p, xb, yb, zb, &pp.full[st]);
     }
     // flags: column i0-1 (a multiple of 32 bytes), row j0-1, level k0-1
-    tma_load_3d(B + fo, &P.map_f, 32 * bx, TY * by, KC * bz, &bar[st]);
+    tma_load_3d(B + fo, &P.map_f, 32 * bx, TY * by, KC * bz, &pp.full[st]);
+    return true;
   };
-  int c = 0;
-  if ((int)blockIdx.x < nbr && threadIdx.x == 0) issue(blockIdx.x, 0);
-  for (int b = blockIdx.x; b < nbr; b += gridDim.x, c++) {
-    const int st = c & 1;
-    const int bn = b + (int)gridDim.x;
+  // a producer time-out stops the copies; the consumers then time out on the stage that never fills
+  bool ok = true, prod_ok = true;
+  if (threadIdx.x == 0)
+    for (int m = 0; m < NS - 1 && m < nmine && prod_ok; m++) prod_ok = produce(m, m);
+  for (int m = 0; m < nmine; m++) {
+    const int st = m % NS;
+    if (threadIdx.x == 0 && prod_ok && m + NS - 1 < nmine) prod_ok = produce(m + NS - 1, (m + NS - 1) % NS);
+    const int b = (int)blockIdx.x + m * (int)gridDim.x;
     const int bx = b % P.nbx, t = b / P.nbx, by = t % P.nby, bz = t / P.nby;
     const int i = 1 + 32 * bx + lane, j = 1 + TY * by + jj;
     const bool col = i <= nx && j <= ny;
@@ -149,44 +174,36 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
     const size_t q2 = col ? P.G.g.at(i, j) : 0;
     const double tE = col ? __ldg(P.op.tE + q2) : 0.0, tW = col ? __ldg(P.op.tW + q2) : 0.0;
     const double tN = col ? __ldg(P.op.tN + j + 1) : 0.0, tS = col ? __ldg(P.op.tS + j + 1) : 0.0;
-    // every thread is past brick c-1 here, so its stage can take brick c+1
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar[st], phase[st], P.timeout_ns));
-    phase[st] ^= 1u;
-    if (!ok) {
-      if (threadIdx.x == 0) atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
-      __syncthreads();
-      return false;
-    }
-    if (bn < nbr && threadIdx.x == 0) issue(bn, st ^ 1);
+    // every lane waits, then the warp agrees, so all its lanes leave the loop together
+    ok = __all_sync(0xffffffffu, mbar_wait_bounded(&pp.full[st], (pp.fph >> st) & 1u, P.timeout_ns));
+    pp.fph ^= 1u << st;
+    if (!ok) break;
     unsigned char* B = smem + (size_t)st * stage;
-    double* S = reinterpret_cast<double*>(B);
-    const double* Rb = reinterpret_cast<const double*>(B + rs);       // sweep A: res box; B: the brick's res
+    const double* S = reinterpret_cast<const double*>(B);
+    const double* R1 = reinterpret_cast<const double*>(B + rs);       // sweep A: res box; B: the brick's res
     const double* Pb = reinterpret_cast<const double*>(B + rs + pb);  // sweep B: the brick's p
     const uint8_t* F = B + fo;
-    if (!kB) {
-      // s_n = res + rsnew/rsold * p (:189), separately rounded, over the box (box 0 = s, box 1 = res)
-      const double* R = Rb;
-      for (int e = threadIdx.x; e < nbox; e += kNHThreads) S[e] = __dadd_rn(R[e], __dmul_rn(bq, S[e]));
-      __syncthreads();
-    }
+    // the direction at box index x: sweep A forms s_n = res + rsnew/rsold * p (:189), separately
+    // rounded; sweep B reads the stored s_n
+    auto sv = [&](int x) { return kB ? S[x] : __dadd_rn(R1[x], __dmul_rn(bq, S[x])); };
     int k = 1 + KC * bz + kk0;
     const int mend = col ? min(KW, nz - k + 1) : 0;
     if (mend > 0) {
       size_t q = (size_t)(k - 1) * plane + q2;
       int cc = ((kk0 + 1) * BY + jj + 1) * kNHBoxX + lane + 2;
       int fl = (kk0 * TY + jj) * 32 + lane;
-      double sdn = S[cc - BXY], sc = S[cc];
+      double sdn = sv(cc - BXY), sc = sv(cc);
       double tT = __ldg(P.op.tT + k - 1), tB = __ldg(P.op.tB + k - 1);  // vertical factors, one level ahead
 #pragma unroll 2
-      for (int m = 0; m < mend; m++) {
-        const double sup = S[cc + BXY];
+      for (int mm = 0; mm < mend; mm++) {
+        const double sup = sv(cc + BXY);
         const uint32_t f = F[fl];
         const double tTn = k < nz ? __ldg(P.op.tT + k) : 0.0, tBn = k < nz ? __ldg(P.op.tB + k) : 0.0;
         if (kB || (f & kNHMaskT)) {
-          const double a = nh_row(f, tE, tW, tN, tS, tT, tB, sdn, S[cc - kNHBoxX], S[cc - 1], sc, S[cc + 1],
-                                  S[cc + kNHBoxX], sup);
-          cell(i, j, k, f, q, a, sc, kB ? Rb[fl] : 0.0, kB ? Pb[fl] : 0.0);
-        } else if (!kB) {
+          const double a = nh_row(f, tE, tW, tN, tS, tT, tB, sdn, sv(cc - kNHBoxX), sv(cc - 1), sc, sv(cc + 1),
+                                  sv(cc + kNHBoxX), sup);
+          cell(i, j, k, f, q, a, sc, kB ? R1[fl] : 0.0, kB ? Pb[fl] : 0.0);
+        } else {
           cell(i, j, k, f, q, 0.0, sc, 0.0, 0.0);  // sweep A stores s_n everywhere
         }
         sdn = sc;
@@ -199,9 +216,11 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
         fl += 32 * TY;
       }
     }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&pp.empty[st]);
   }
-  __syncthreads();  // the last stage is read to the end before the next sweep reuses it
-  return true;
+  if (!ok || !prod_ok) atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+  return __syncthreads_and(ok && prod_ok) != 0;  // also: every stage is read to the end before the next sweep
 }
 
 template <bool CX, bool CY>
@@ -218,15 +237,17 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
   const uint32_t gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
   const uint32_t tw = gridDim.x * kWarps;
   const unsigned nb = gridDim.x;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * nh_stage_bytes(P.ty, P.kc));
-  uint32_t phase[2] = {0u, 0u};
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)P.ns * nh_stage_bytes(P.ty, P.kc));
+  NHPipe pp{bars, bars + kNHMaxStages, 0u, 0u, 0u};
   unsigned long long epoch = 0;
   double* __restrict__ pnh = P.p;
   double* __restrict__ res = P.res;
 
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int st = 0; st < P.ns; st++) {
+      mbar_init(&pp.full[st], 1);
+      mbar_init(&pp.empty[st], kNHThreads / 32);
+    }
     fence_mbar_init();
   }
   __syncthreads();
@@ -290,7 +311,7 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
       double* __restrict__ Sn = P.s[cur ^ 1];
       double acc_dot = 0.0, acc_max = 0.0;
       const bool ok = nh_sweep<false>(
-          P, cur, bq, smem, bar, phase,
+          P, cur, bq, smem, pp,
           [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double, double) {
             ptrdiff_t ox, oy;
             nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
@@ -358,7 +379,7 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
       // ------------------------------------------------------------ sweep B
       double acc_r = 0.0;
       const bool ok = nh_sweep<true>(
-          P, cur, bq, smem, bar, phase,
+          P, cur, bq, smem, pp,
           [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double rc, double pc) {
             const double r = __dsub_rn(rc, __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
             const double d = __dmul_rn(alpha, sc);                // p_non_hydro + alpha*p (:187)
@@ -488,6 +509,7 @@ struct pyomgpu_nh {
   int max_blocks = 0;  // slots reserved for this many blocks
   int grid = 0;        // 0: automatic
   int ty = 0, kc = 0;  // brick shape (0: automatic)
+  int ns = 0;          // pipeline stages (0: automatic)
   double timeout_s = 2.0;
   unsigned stall_next = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -705,11 +727,18 @@ int32_t pyomgpu_nh_set_brick(pyomgpu_nh* h, int32_t ty, int32_t kc) {
   if (!h || ty < 0 || kc < 0 || (ty > 0) != (kc > 0))
     return nfail(PYOMGPU_EINVAL, "nh_set_brick: ty and kc both positive (or both 0 = automatic)");
   if (ty > 0 && ((ty != 1 && ty != 2 && ty != 4 && ty != 8) || kc % (8 / ty) != 0 || kc > 248 ||
-                 nh_smem_bytes(ty, kc) > kNHSmemMax))
+                 nh_smem_bytes(ty, kc, 2) > kNHSmemMax))
     return nfail(PYOMGPU_EINVAL,
                  "nh_set_brick: ty in {1,2,4,8}, kc a multiple of 8/ty, and the staged boxes within shared memory");
   h->ty = ty;
   h->kc = kc;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_nh_set_stages(pyomgpu_nh* h, int32_t stages) {
+  if (!h || stages < 0 || stages == 1 || stages > kNHMaxStages)
+    return nfail(PYOMGPU_EINVAL, "nh_set_stages: 2..%d stages (0 = automatic)", kNHMaxStages);
+  h->ns = stages;
   return PYOMGPU_OK;
 }
 
@@ -762,17 +791,20 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
   h->stall_next = 0;
   P.out = h->d_result;
   // brick shape: 32 x ty x kc, ty the largest power of two <= min(8, ny), kc = (8/ty) kw with kw the
-  // largest level count per warp whose two pipeline stages leave room for two blocks per SM
-  int ty = h->ty, kc = h->kc;
+  // largest level count per warp whose pipeline stages leave room for two blocks per SM
+  int ty = h->ty, kc = h->kc, ns = h->ns > 0 ? h->ns : 2;
   if (ty == 0) {
     ty = h->G.g.ny >= 8 ? 8 : h->G.g.ny >= 4 ? 4 : h->G.g.ny >= 2 ? 2 : 1;
     const int seg = 8 / ty;
     const int kw_need = (h->G.nz + seg - 1) / seg;
     int kw = 1;
-    while (kw < kw_need && nh_smem_bytes(ty, seg * (kw + 1)) <= (size_t)113 * 1024) kw++;
+    while (kw < kw_need && nh_smem_bytes(ty, seg * (kw + 1), ns) <= (size_t)113 * 1024) kw++;
     kc = seg * kw;
   }
-  const size_t smem = nh_smem_bytes(ty, kc);
+  while (ns > 2 && nh_smem_bytes(ty, kc, ns) > kNHSmemMax) ns--;
+  const size_t smem = nh_smem_bytes(ty, kc, ns);
+  if (smem > kNHSmemMax) return nfail(PYOMGPU_EINVAL, "congrad_non_hydro: brick boxes exceed shared memory");
+  P.ns = ns;
   P.ty = ty;
   P.kc = kc;
   P.kw = kc / (8 / ty);

@@ -133,8 +133,11 @@ __host__ __device__ constexpr size_t nh_flags_off(int ty, int kc) {
 __host__ __device__ constexpr size_t nh_stage_bytes(int ty, int kc) {
   return nh_flags_off(ty, kc) + nh_al(nh_f_bytes(ty, kc));
 }
-// two pipeline stages + two mbarriers
-__host__ __device__ constexpr size_t nh_smem_bytes(int ty, int kc) { return 2 * nh_stage_bytes(ty, kc) + 128; }
+// ns pipeline stages (2..4) + a full and an empty mbarrier per stage
+constexpr int kNHMaxStages = 4;
+__host__ __device__ constexpr size_t nh_smem_bytes(int ty, int kc, int ns) {
+  return (size_t)ns * nh_stage_bytes(ty, kc) + 128;
+}
 constexpr size_t kNHSmemMax = 220 * 1024;
 
 struct alignas(64) NHParams {
@@ -145,6 +148,7 @@ struct alignas(64) NHParams {
   NHGeo G;
   NHOp op;
   int ty, kw, kc;                    // brick shape
+  int ns;                            // pipeline stages
   int nbx, nby, nbz;                 // bricks per dimension
   const double* forc;  // Fortran layout (nx+4, ny+4, nz), device
   double* p;           // padded p_non_hydro(:,:,:,taup1), in/out

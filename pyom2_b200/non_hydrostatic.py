@@ -79,6 +79,10 @@ class NonHydrostatic:
         """Brick shape 32 x ty x kc of the CG sweeps ((0, 0) = automatic)."""
         _abi.check(self._L.pyomgpu_nh_set_brick(self._h, int(ty), int(kc)))
 
+    def set_stages(self, stages: int):
+        """TMA pipeline depth of the CG sweeps (2..4; 0 = automatic)."""
+        _abi.check(self._L.pyomgpu_nh_set_stages(self._h, int(stages)))
+
     def apply_op_3d(self, p):
         """non_hydrostatic.f90:247-276: ``res = A p`` over the interior, zero halo."""
         res = np.zeros(self.shape, order="F") if not _is_torch(p) else _torch_like(p)
