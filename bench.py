@@ -306,8 +306,8 @@ def main():
     ap.add_argument("--with-c2", action="store_true",
                     help="also time config 2 (64 basins in one work-queue launch vs 64 sequential solves)")
     ap.add_argument("--c2-count", type=int, default=64, help="basins of config 2 (fewer for profiling)")
-    ap.add_argument("--with-nh", action="store_true",
-                    help="also time the non-hydrostatic 3-D pressure solve (congrad_non_hydro)")
+    ap.add_argument("--no-nh", action="store_true",
+                    help="skip the non-hydrostatic 3-D pressure solve (congrad_non_hydro) leg")
     ap.add_argument("--nh-only", action="store_true",
                     help="time only the non-hydrostatic solve and print its object (profiling runs)")
     ap.add_argument("--nh-grid", default="240x240x80", help="tank size of the non-hydrostatic solve")
@@ -459,7 +459,7 @@ def main():
                                      "fcg_iterations": results["fcg"]["iterations"],
                                      "pcg64_iterations": results["pcg64"]["iterations"],
                                      "speedup": results["pcg64"]["value"] / results["fcg"]["value"]}
-    if args.with_nh and rank == 0:
+    if not args.no_nh and rank == 0:
         out["non_hydrostatic"] = nh_bench(max(2, args.steps // 3), 3, peak, nh_grid, max_it=args.nh_max_it,
                                           cpu=world == 1 and not args.no_cpu_baseline)
     if args.with_c2 and rank == 0:

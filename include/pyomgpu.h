@@ -23,6 +23,7 @@
  *   congrad_non_hydro          non_hydrostatic.f90:146  pyomgpu_congrad_non_hydro
  *   apply_op_3D                non_hydrostatic.f90:247  pyomgpu_apply_op_3d
  *   dot_3D/absmax_3D           non_hydrostatic.f90:279-322 (fused into the CG kernel)
+ *   solve_non_hydrostatic      non_hydrostatic.f90:5    pyomgpu_solve_non_hydrostatic
  *
  * Array conventions: every 2-D field has the Fortran extents of
  * main_module.f90 for one PE, (1-onx:nx+onx, 1-onx:ny+onx) with onx = 2, in
@@ -325,6 +326,26 @@ int32_t pyomgpu_apply_op_3d(pyomgpu_nh* nh, const double* p1, double* res, pyomg
  * immediate stop (zero initial residual) reports 0 iterations. */
 int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* nh, const double* forc, double* p, double eps, int32_t max_it,
                                   pyomgpu_solve_info* info, pyomgpu_stream stream);
+
+/* Model arrays of solve_non_hydrostatic (all DEVICE pointers, Fortran layout). */
+typedef struct pyomgpu_state3d {
+  int32_t taum1, tau, taup1;       /* 1-based time levels */
+  int32_t itt;                     /* time step counter (itt == 0 copies p to tau and taum1) */
+  int32_t congr_max_itts_non_hydro;
+  int32_t congr_itts_non_hydro;    /* out */
+  double dt_mom, AB_eps, congr_epsilon_non_hydro;
+  double *u, *v, *w;               /* (nx+4, ny+4, nz, 3) */
+  const double* dw;                /* (nx+4, ny+4, nz, 3) */
+  const double* dw_mix;            /* (nx+4, ny+4, nz) */
+  double* p_non_hydro;             /* (nx+4, ny+4, nz, 3) */
+} pyomgpu_state3d;
+/* solve_non_hydrostatic (non_hydrostatic.f90:5-63) on device-resident model
+ * arrays: w(taup1) integrated, u/v/w(taup1) made cyclic, the divergence
+ * forcing, the first guess 2 p(tau) - p(taum1), congrad_non_hydro, p made
+ * cyclic (and copied to tau, taum1 when itt == 0), and the pressure-gradient
+ * correction of u, v, w(taup1). */
+int32_t pyomgpu_solve_non_hydrostatic(pyomgpu_nh* nh, pyomgpu_state3d* st, pyomgpu_solve_info* info,
+                                      pyomgpu_stream stream);
 
 /* ---- learned preconditioner (no counterpart in the reference) ----------------- */
 /* Building block of the U-Net preconditioner: one 3x3 convolution (stride 1,

@@ -43,6 +43,14 @@ class OGrid3(C.Structure):
                 ("maskU", C.c_void_p), ("maskV", C.c_void_p), ("maskW", C.c_void_p)]
 
 
+class OState3(C.Structure):
+    _fields_ = [("taum1", C.c_int), ("tau", C.c_int), ("taup1", C.c_int), ("itt", C.c_int),
+                ("dt_mom", C.c_double), ("AB_eps", C.c_double), ("congr_epsilon_non_hydro", C.c_double),
+                ("congr_max_itts_non_hydro", C.c_int), ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+                ("dw", C.c_void_p), ("dw_mix", C.c_void_p), ("p_non_hydro", C.c_void_p),
+                ("congr_itts_non_hydro", C.c_int), ("status", C.c_int)]
+
+
 class OIslands(C.Structure):
     _fields_ = [("nisle", C.c_int), ("max_boundary", C.c_int), ("boundary", C.c_void_p),
                 ("line_dir", C.c_void_p), ("nr_boundary", C.c_void_p)]
@@ -104,6 +112,7 @@ def lib():
             "o_dot_3d": (d, [p, p, p]),
             "o_absmax_3d": (d, [p, p]),
             "o_congrad_non_hydro": (i, [p, p, p, p, d, i, p]),
+            "o_solve_non_hydrostatic": (i, [p, p, p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(_lib, name)
@@ -358,3 +367,26 @@ class Oracle3D:
                                   int(M.congr_max_itts_non_hydro if max_it is None else max_it), C.byref(info))
         return dict(iterations=info.iterations, converged=bool(info.converged), status=info.status,
                     estimated_error=info.estimated_error)
+
+    def solve_non_hydrostatic(self, M=None, cf=None):
+        """non_hydrostatic.f90:5-63 in place on M's u, v, w, p_non_hydro;
+        sets M.congr_itts_non_hydro and returns the solver status."""
+        M = M or self.M
+        cf = self.make_coeff() if cf is None else cf
+        keep = []
+
+        def P(a):
+            assert a.dtype == np.float64 and a.flags.f_contiguous
+            keep.append(a)
+            return a.ctypes.data
+
+        s = OState3()
+        s.taum1, s.tau, s.taup1, s.itt = M.taum1, M.tau, M.taup1, int(M.itt)
+        s.dt_mom, s.AB_eps = float(M.dt_mom), float(M.AB_eps)
+        s.congr_epsilon_non_hydro = float(M.congr_epsilon_non_hydro)
+        s.congr_max_itts_non_hydro = int(M.congr_max_itts_non_hydro)
+        for n in ("u", "v", "w", "dw", "dw_mix", "p_non_hydro"):
+            setattr(s, n, P(getattr(M, n)))
+        rc = lib().o_solve_non_hydrostatic(self.gp, _p(cf), C.byref(s))
+        M.congr_itts_non_hydro = s.congr_itts_non_hydro
+        return rc

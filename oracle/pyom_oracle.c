@@ -1285,3 +1285,77 @@ done:
   free(Ap);
   return status;
 }
+
+/* non_hydrostatic.f90:5-63.  forc's halo is never read by the solve (the
+ * reference leaves it uninitialised); it is zero here. */
+int o_solve_non_hydrostatic(const o_grid3 *g3, const double *cf, o_state3 *s) {
+  const o_grid *g = &g3->g;
+  const int nx = g->nx, ny = g->ny, nz = g3->nz;
+  const size_t n3 = N3(g3);
+  const int X = nx + 4, Y = ny + 4;
+  double *u = s->u + (size_t)(s->taup1 - 1) * n3;
+  double *v = s->v + (size_t)(s->taup1 - 1) * n3;
+  double *w = s->w + (size_t)(s->taup1 - 1) * n3;
+  const double *w_tau = s->w + (size_t)(s->tau - 1) * n3;
+  const double *dw_tau = s->dw + (size_t)(s->tau - 1) * n3;
+  const double *dw_taum1 = s->dw + (size_t)(s->taum1 - 1) * n3;
+  double *p1 = s->p_non_hydro + (size_t)(s->taup1 - 1) * n3;
+  double *p0 = s->p_non_hydro + (size_t)(s->tau - 1) * n3;
+  double *pm = s->p_non_hydro + (size_t)(s->taum1 - 1) * n3;
+  /* :13-15 integrate w forward (whole levels k < nz) */
+  for (int k = 1; k < nz; k++)
+    for (int jj = 0; jj < Y; jj++)
+      for (int ii = 0; ii < X; ii++) {
+        const size_t q = (size_t)ii + (size_t)X * ((size_t)jj + (size_t)Y * (size_t)(k - 1));
+        w[q] = w_tau[q] + s->dt_mom *
+                              (s->dw_mix[q] + (1.5 + s->AB_eps) * dw_tau[q] - (0.5 + s->AB_eps) * dw_taum1[q]) *
+                              g3->maskW[q];
+      }
+  /* :19-24 */
+  o_setcyclic_xyz(g3, u);
+  o_setcyclic_xyz(g3, v);
+  o_setcyclic_xyz(g3, w);
+  /* :25-36 */
+  double *forc = (double *)calloc(n3, sizeof(double));
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        const double cj = g->cost[Y1(g, j)];
+        forc[IX3(g3, i, j, k)] = (u[IX3(g3, i, j, k)] - u[IX3(g3, i - 1, j, k)]) / (cj * g->dxt[X1(g, i)]) +
+                                 (g->cosu[Y1(g, j)] * v[IX3(g3, i, j, k)] -
+                                  g->cosu[Y1(g, j - 1)] * v[IX3(g3, i, j - 1, k)]) /
+                                     (cj * g->dyt[Y1(g, j)]);
+      }
+  for (size_t q = 0; q < N2(g); q++) forc[q] = forc[q] + w[q] / g3->dzt[0];
+  for (int k = 2; k <= nz; k++) {
+    const size_t o = (size_t)(k - 1) * N2(g), om = (size_t)(k - 2) * N2(g);
+    for (size_t q = 0; q < N2(g); q++) forc[o + q] = forc[o + q] + (w[o + q] - w[om + q]) / g3->dzt[k - 1];
+  }
+  for (size_t q = 0; q < n3; q++) forc[q] = forc[q] / s->dt_mom;
+  /* :40-48 */
+  for (size_t q = 0; q < n3; q++) p1[q] = 2 * p0[q] - pm[q];
+  o_info info;
+  s->status = o_congrad_non_hydro(g3, cf, forc, p1, s->congr_epsilon_non_hydro, s->congr_max_itts_non_hydro, &info);
+  s->congr_itts_non_hydro = info.iterations;
+  free(forc);
+  o_setcyclic_xyz(g3, p1);
+  if (s->itt == 0) {
+    memcpy(p0, p1, n3 * sizeof(double));
+    memcpy(pm, p1, n3 * sizeof(double));
+  }
+  /* :52-61 */
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        const size_t q = IX3(g3, i, j, k);
+        u[q] = u[q] - s->dt_mom * (p1[IX3(g3, i + 1, j, k)] - p1[q]) / (g->dxu[X1(g, i)] * g->cost[Y1(g, j)]) *
+                          g3->maskU[q];
+        v[q] = v[q] - s->dt_mom * (p1[IX3(g3, i, j + 1, k)] - p1[q]) / g->dyu[Y1(g, j)] * g3->maskV[q];
+      }
+  for (int k = 1; k < nz; k++) {
+    const size_t o = (size_t)(k - 1) * N2(g), op = (size_t)k * N2(g);
+    for (size_t q = 0; q < N2(g); q++)
+      w[o + q] = w[o + q] - s->dt_mom * (p1[op + q] - p1[o + q]) / g3->dzw[k - 1] * g3->maskW[o + q];
+  }
+  return s->status;
+}

@@ -118,6 +118,22 @@ double o_absmax_3d(const o_grid3 *g, const double *p1);
 int o_congrad_non_hydro(const o_grid3 *g, const double *cf, const double *forc, double *p, double eps, int max_it,
                         o_info *info);
 
+/* model arrays of solve_non_hydrostatic (non_hydrostatic.f90:5-63) */
+typedef struct o_state3 {
+  int taum1, tau, taup1;            /* 1-based time levels */
+  int itt;
+  double dt_mom, AB_eps;
+  double congr_epsilon_non_hydro;
+  int congr_max_itts_non_hydro;
+  double *u, *v, *w;                /* (nx+4, ny+4, nz, 3) */
+  const double *dw;                 /* (nx+4, ny+4, nz, 3) */
+  const double *dw_mix;             /* (nx+4, ny+4, nz) */
+  double *p_non_hydro;              /* (nx+4, ny+4, nz, 3) */
+  int congr_itts_non_hydro;         /* out */
+  int status;                       /* out */
+} o_state3;
+int o_solve_non_hydrostatic(const o_grid3 *g, const double *cf, o_state3 *s);
+
 int o_solve_streamfunction(const o_grid *g, const double *cf, const o_islands *isl, o_state *s);
 int o_solve_pressure(const o_grid *g, const double *cf, o_state *s);
 

@@ -39,7 +39,7 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_unet_forward_backward", "pyomgpu_solve_fcg",
            "pyomgpu_nh_create", "pyomgpu_nh_destroy", "pyomgpu_nh_set_sync_timeout",
            "pyomgpu_nh_inject_barrier_stall", "pyomgpu_nh_set_grid", "pyomgpu_nh_set_brick", "pyomgpu_nh_set_stages", "pyomgpu_apply_op_3d",
-           "pyomgpu_congrad_non_hydro")
+           "pyomgpu_congrad_non_hydro", "pyomgpu_solve_non_hydrostatic")
 
 
 class PyOMGPUError(RuntimeError):
@@ -64,6 +64,14 @@ class Grid3D(C.Structure):
                 ("dxt", C.c_void_p), ("dxu", C.c_void_p), ("dyt", C.c_void_p), ("dyu", C.c_void_p),
                 ("cost", C.c_void_p), ("cosu", C.c_void_p), ("dzt", C.c_void_p), ("dzw", C.c_void_p),
                 ("maskT", C.c_void_p), ("maskU", C.c_void_p), ("maskV", C.c_void_p), ("maskW", C.c_void_p)]
+
+
+class State3D(C.Structure):
+    _fields_ = [("taum1", C.c_int32), ("tau", C.c_int32), ("taup1", C.c_int32), ("itt", C.c_int32),
+                ("congr_max_itts_non_hydro", C.c_int32), ("congr_itts_non_hydro", C.c_int32),
+                ("dt_mom", C.c_double), ("AB_eps", C.c_double), ("congr_epsilon_non_hydro", C.c_double),
+                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p), ("dw", C.c_void_p),
+                ("dw_mix", C.c_void_p), ("p_non_hydro", C.c_void_p)]
 
 
 class Islands(C.Structure):
@@ -150,6 +158,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_nh_set_stages": (i32, [vp, i32]),
         "pyomgpu_apply_op_3d": (i32, [vp, vp, vp, vp]),
         "pyomgpu_congrad_non_hydro": (i32, [vp, vp, vp, d, i32, P(SolveInfo), vp]),
+        "pyomgpu_solve_non_hydrostatic": (i32, [vp, P(State3D), P(SolveInfo), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

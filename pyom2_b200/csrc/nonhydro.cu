@@ -471,7 +471,112 @@ __global__ void nh_pack_kernel(const NHGeo G, const double* __restrict__ user, d
 
 int grid_for(size_t n) { return (int)std::min<size_t>(4096, std::max<size_t>(1, (n + 255) / 256)); }
 
+// ---- solve_non_hydrostatic step (non_hydrostatic.f90:5-63), Fortran layout -----------------
+__device__ __forceinline__ size_t nh_f(const NHGeo& G, int fi, int fj, int k0) {  // 0-based indices
+  return (size_t)fi + (size_t)(G.g.nx + 2 * kOnx) * ((size_t)fj + (size_t)(G.g.ny + 2 * kOnx) * (size_t)k0);
+}
+
+// w(:,:,k,taup1) = w(tau) + dt_mom*(dw_mix + (1.5+AB_eps) dw(tau) - (0.5+AB_eps) dw(taum1)) * maskW, k < nz (:13-15)
+__global__ void nh_w_kernel(const NHStep S) {
+  const size_t n = (size_t)(S.G.g.nx + 4) * (S.G.g.ny + 4) * (S.G.nz - 1);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    S.w[q] = __dadd_rn(S.w_tau[q],
+                       __dmul_rn(__dmul_rn(S.dt_mom, __dsub_rn(__dadd_rn(S.dw_mix[q], __dmul_rn(1.5 + S.AB_eps,
+                                                                                               S.dw_tau[q])),
+                                                               __dmul_rn(0.5 + S.AB_eps, S.dw_taum1[q]))),
+                                 (double)S.maskW[q]));
+}
+
+// setcyclic_xyz (parallel_none.f90:188-211) of up to three arrays: every halo position the reference
+// fills takes the interior value it ends up with (x copies, then y copies over the x-filled rows).
+__global__ void nh_setcyclic_kernel(const NHGeo G, double* a, double* b, double* c) {
+  const int X = G.g.nx + 4, Y = G.g.ny + 4;
+  const size_t n = (size_t)X * Y * G.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int fi = (int)(e % X);
+    const size_t r = e / X;
+    const int fj = (int)(r % Y);
+    const int k0 = (int)(r / Y);
+    int si = fi, sj = fj;  // Fortran index = 0-based index - 1
+    if (G.g.cyclic_x) {
+      if (fi - 1 > G.g.nx) si = fi - G.g.nx;
+      else if (fi - 1 < 1) si = fi + G.g.nx;
+    }
+    if (G.g.cyclic_y) {
+      if (fj - 1 > G.g.ny) sj = fj - G.g.ny;
+      else if (fj - 1 < 1) sj = fj + G.g.ny;
+    }
+    if (si == fi && sj == fj) continue;
+    const size_t src = nh_f(G, si, sj, k0);
+    for (double* x : {a, b, c})
+      if (x) x[e] = x[src];
+  }
+}
+
+// forc = (div_h(u, v) + dw/dz) / dt_mom on the interior (:25-36); p(taup1) = 2 p(tau) - p(taum1) (:40)
+__global__ void nh_forc_kernel(const NHStep S) {
+  const int nx = S.G.g.nx, ny = S.G.g.ny, X = nx + 4;
+  const size_t n = (size_t)X * (ny + 4) * S.G.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    S.p1[e] = __dsub_rn(2.0 * S.p0[e], S.pm[e]);
+    const int fi = (int)(e % X);
+    const size_t r = e / X;
+    const int fj = (int)(r % (ny + 4));
+    const int k0 = (int)(r / (ny + 4));
+    const int i = fi - 1, j = fj - 1;  // Fortran indices
+    if (i < 1 || i > nx || j < 1 || j > ny) {
+      S.forc[e] = 0.0;
+      continue;
+    }
+    const double cj = S.cost[fj];
+    double f = __dadd_rn(__ddiv_rn(__dsub_rn(S.u[e], S.u[e - 1]), __dmul_rn(cj, S.dxt[fi])),
+                         __ddiv_rn(__dsub_rn(__dmul_rn(S.cosu[fj], S.v[e]), __dmul_rn(S.cosu[fj - 1], S.v[e - X])),
+                                   __dmul_rn(cj, S.dyt[fj])));
+    const size_t pl = (size_t)X * (ny + 4);
+    const double wt = k0 == 0 ? S.w[e] : __dsub_rn(S.w[e], S.w[e - pl]);
+    f = __dadd_rn(f, __ddiv_rn(wt, S.dzt[k0]));
+    S.forc[e] = __ddiv_rn(f, S.dt_mom);
+  }
+}
+
+// u, v -= dt_mom * grad p (interior), w -= dt_mom * dp/dz * maskW (whole levels k < nz)  (:52-61)
+__global__ void nh_correct_kernel(const NHStep S) {
+  const int nx = S.G.g.nx, ny = S.G.g.ny, X = nx + 4;
+  const size_t pl = (size_t)X * (ny + 4);
+  const size_t n = pl * S.G.nz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int fi = (int)(e % X);
+    const size_t r = e / X;
+    const int fj = (int)(r % (ny + 4));
+    const int k0 = (int)(r / (ny + 4));
+    const int i = fi - 1, j = fj - 1;
+    if (i >= 1 && i <= nx && j >= 1 && j <= ny) {
+      const double dpx = __dsub_rn(S.p1[e + 1], S.p1[e]);
+      S.u[e] = __dsub_rn(S.u[e], __dmul_rn(__ddiv_rn(__dmul_rn(S.dt_mom, dpx), __dmul_rn(S.dxu[fi], S.cost[fj])),
+                                           (double)S.maskU[e]));
+      const double dpy = __dsub_rn(S.p1[e + X], S.p1[e]);
+      S.v[e] = __dsub_rn(S.v[e], __dmul_rn(__ddiv_rn(__dmul_rn(S.dt_mom, dpy), S.dyu[fj]), (double)S.maskV[e]));
+    }
+    if (k0 < S.G.nz - 1) {
+      const double dpz = __dsub_rn(S.p1[e + pl], S.p1[e]);
+      S.w[e] = __dsub_rn(S.w[e], __dmul_rn(__ddiv_rn(__dmul_rn(S.dt_mom, dpz), S.dzw[k0]), (double)S.maskW[e]));
+    }
+  }
+}
+
 }  // namespace
+
+void launch_nh_step_pre(const NHStep& S, cudaStream_t st) {
+  const size_t n = (size_t)(S.G.g.nx + 4) * (S.G.g.ny + 4) * S.G.nz;
+  nh_w_kernel<<<grid_for(n), 256, 0, st>>>(S);
+  if (S.G.g.cyclic_x || S.G.g.cyclic_y) nh_setcyclic_kernel<<<grid_for(n), 256, 0, st>>>(S.G, S.u, S.v, S.w);
+  nh_forc_kernel<<<grid_for(n), 256, 0, st>>>(S);
+}
+void launch_nh_step_post(const NHStep& S, cudaStream_t st) {
+  const size_t n = (size_t)(S.G.g.nx + 4) * (S.G.g.ny + 4) * S.G.nz;
+  if (S.G.g.cyclic_x || S.G.g.cyclic_y) nh_setcyclic_kernel<<<grid_for(n), 256, 0, st>>>(S.G, S.p1, nullptr, nullptr);
+  nh_correct_kernel<<<grid_for(n), 256, 0, st>>>(S);
+}
 
 void launch_nh_apply(const NHGeo& G, const NHOp& op, const double* p, double* res, cudaStream_t st) {
   nh_apply_kernel<<<grid_for((size_t)G.g.nx * G.g.ny * G.nz), 256, 0, st>>>(G, op, p, res);
@@ -500,6 +605,10 @@ struct pyomgpu_nh {
   size_t nf = 0;  // Fortran-layout elements (nx+4)(ny+4)nz
   uint8_t* flags = nullptr;
   double *tE = nullptr, *tW = nullptr, *tN = nullptr, *tS = nullptr, *tT = nullptr, *tB = nullptr;
+  // grid arrays of the full step (solve_non_hydrostatic)
+  double *dxt = nullptr, *dxu = nullptr, *dyt = nullptr, *dyu = nullptr, *cost = nullptr, *cosu = nullptr;
+  double *dzt = nullptr, *dzw = nullptr;
+  uint8_t *mU = nullptr, *mV = nullptr, *mW = nullptr;
   double *p = nullptr, *res = nullptr, *s[2] = {}, *stage_f = nullptr, *stage_p = nullptr;
   SyncCtl* ctl = nullptr;
   double* slots = nullptr;
@@ -514,7 +623,8 @@ struct pyomgpu_nh {
   unsigned stall_next = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   ~pyomgpu_nh() {
-    void* ptrs[] = {flags, tE, tW, tN, tS, tT, tB, p, res, s[0], s[1], stage_f, stage_p, ctl, slots,
+    void* ptrs[] = {flags, tE, tW, tN, tS, tT, tB, dxt, dxu, dyt, dyu, cost, cosu, dzt, dzw, mU, mV, mW,
+                    p, res, s[0], s[1], stage_f, stage_p, ctl, slots,
                     d_result};
     for (void* q : ptrs)
       if (q) cudaFree(q);
@@ -657,6 +767,9 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
         f |= bit(F3(gr->maskT, i, j, k), kNHMaskT);
         flags[((size_t)(k - 1) * ny + (j - 1)) * fx + (i - 1)] = (uint8_t)f;
       }
+  for (const double* m : {gr->maskT, gr->maskU, gr->maskV, gr->maskW})
+    for (size_t q = 0; q < h->nf; q++)
+      if (m[q] != 0.0 && m[q] != 1.0) bad_mask = 1;
   if (bad_mask) {
     delete h;
     return nfail(PYOMGPU_EINVAL, "nh_create: masks must hold only 0 and 1");
@@ -670,6 +783,23 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
       (rc = nalloc(&h->d_result, 1))) {
     delete h;
     return rc;
+  }
+  {
+    auto v1 = [](const double* a, size_t n) { return std::vector<double>(a, a + n); };
+    auto m8 = [&](const double* a) {
+      std::vector<uint8_t> m(h->nf);
+      for (size_t q = 0; q < h->nf; q++) m[q] = a[q] == 1.0 ? 1 : 0;
+      return m;
+    };
+    if ((rc = nupload(&h->dxt, v1(gr->dxt, X))) || (rc = nupload(&h->dxu, v1(gr->dxu, X))) ||
+        (rc = nupload(&h->dyt, v1(gr->dyt, Y))) || (rc = nupload(&h->dyu, v1(gr->dyu, Y))) ||
+        (rc = nupload(&h->cost, v1(gr->cost, Y))) || (rc = nupload(&h->cosu, v1(gr->cosu, Y))) ||
+        (rc = nupload(&h->dzt, v1(gr->dzt, nz))) || (rc = nupload(&h->dzw, v1(gr->dzw, nz))) ||
+        (rc = nupload(&h->mU, m8(gr->maskU))) || (rc = nupload(&h->mV, m8(gr->maskV))) ||
+        (rc = nupload(&h->mW, m8(gr->maskW)))) {
+      delete h;
+      return rc;
+    }
   }
   h->op = NHOp{h->flags, h->tE, h->tW, h->tN, h->tS, h->tT, h->tB, fx};
   if (cudaMemset(h->p, 0, np * sizeof(double)) != cudaSuccess) {
@@ -760,17 +890,16 @@ int32_t pyomgpu_apply_op_3d(pyomgpu_nh* h, const double* p1, double* res, pyomgp
   return PYOMGPU_OK;
 }
 
-int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, double eps, int32_t max_it,
-                                  pyomgpu_solve_info* info, pyomgpu_stream stream) {
-  if (!h || !forc || !p) return nfail(PYOMGPU_EINVAL, "congrad_non_hydro: null argument");
-  cudaStream_t st = (cudaStream_t)stream;
-  const double* fdev = nullptr;
-  if (int rc = nh_stage(h, forc, h->stage_f, &fdev, st)) return rc;
-  const bool p_dev = nh_on_device(p);
-  const double* pin = nullptr;
-  if (int rc = nh_stage(h, p, h->stage_p, &pin, st)) return rc;
+}  // extern "C"
+
+namespace {
+
+// congrad_non_hydro on device arrays: fdev (forcing) and pdev (p_non_hydro(:,:,:,taup1), in/out), both
+// Fortran layout.  pdev may be a staging buffer whose result the caller copies out.
+int nh_run_cg(pyomgpu_nh* h, const double* fdev, double* pdev, double eps, int max_it, pyomgpu_solve_info* info,
+              cudaStream_t st) {
   const size_t bytes = h->G.size() * sizeof(double);
-  launch_nh_pack(h->G, pin, h->p, st);
+  launch_nh_pack(h->G, pdev, h->p, st);
   for (double* b : {h->res, h->s[0], h->s[1]}) NCK(cudaMemsetAsync(b, 0, bytes, st));
   NCK(cudaMemsetAsync(h->ctl, 0, sizeof(SyncCtl), st));
   NHParams P{};
@@ -841,10 +970,8 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
   NCK(cudaEventRecord(h->e1, st));
   NCK(cudaMemcpyAsync(h->h_result, h->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
   NCK(cudaMemcpyAsync(h->h_err, &h->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
-  double* pout = p_dev ? p : h->stage_p;
-  launch_nh_unpack(h->G, h->p, pout, st);
+  launch_nh_unpack(h->G, h->p, pdev, st);
   NCK(cudaGetLastError());
-  if (!p_dev) NCK(cudaMemcpyAsync(p, h->stage_p, h->nf * sizeof(double), cudaMemcpyDeviceToHost, st));
   NCK(cudaStreamSynchronize(st));
   const int err = *h->h_err;
   float ms = 0.f;
@@ -866,6 +993,81 @@ int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, 
   }
   if (err) return nfail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded %.3f s", h->timeout_s);
   return h->h_result->status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t pyomgpu_congrad_non_hydro(pyomgpu_nh* h, const double* forc, double* p, double eps, int32_t max_it,
+                                  pyomgpu_solve_info* info, pyomgpu_stream stream) {
+  if (!h || !forc || !p) return nfail(PYOMGPU_EINVAL, "congrad_non_hydro: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* fdev = nullptr;
+  if (int rc = nh_stage(h, forc, h->stage_f, &fdev, st)) return rc;
+  const bool p_dev = nh_on_device(p);
+  if (!p_dev) NCK(cudaMemcpyAsync(h->stage_p, p, h->nf * sizeof(double), cudaMemcpyHostToDevice, st));
+  const int rc = nh_run_cg(h, fdev, p_dev ? p : h->stage_p, eps, max_it, info, st);
+  if (rc < 0 && rc != PYOMGPU_TIMEOUT) return rc;
+  if (!p_dev) {
+    NCK(cudaMemcpyAsync(p, h->stage_p, h->nf * sizeof(double), cudaMemcpyDeviceToHost, st));
+    NCK(cudaStreamSynchronize(st));
+  }
+  return rc;
+}
+
+int32_t pyomgpu_solve_non_hydrostatic(pyomgpu_nh* h, pyomgpu_state3d* s, pyomgpu_solve_info* info,
+                                      pyomgpu_stream stream) {
+  if (!h || !s || !s->u || !s->v || !s->w || !s->dw || !s->dw_mix || !s->p_non_hydro)
+    return nfail(PYOMGPU_EINVAL, "solve_non_hydrostatic: null argument");
+  for (int t : {s->taum1, s->tau, s->taup1})
+    if (t < 1 || t > 3) return nfail(PYOMGPU_EINVAL, "solve_non_hydrostatic: time levels are 1..3");
+  for (const void* q : {(const void*)s->u, (const void*)s->v, (const void*)s->w, (const void*)s->dw,
+                        (const void*)s->dw_mix, (const void*)s->p_non_hydro})
+    if (!nh_on_device(q)) return nfail(PYOMGPU_EINVAL, "solve_non_hydrostatic: model arrays must be device memory");
+  cudaStream_t st = (cudaStream_t)stream;
+  NHStep S{};
+  S.G = h->G;
+  S.dxt = h->dxt;
+  S.dxu = h->dxu;
+  S.dyt = h->dyt;
+  S.dyu = h->dyu;
+  S.cost = h->cost;
+  S.cosu = h->cosu;
+  S.dzt = h->dzt;
+  S.dzw = h->dzw;
+  S.maskU = h->mU;
+  S.maskV = h->mV;
+  S.maskW = h->mW;
+  const size_t n3 = h->nf;
+  S.u = s->u + (size_t)(s->taup1 - 1) * n3;
+  S.v = s->v + (size_t)(s->taup1 - 1) * n3;
+  S.w = s->w + (size_t)(s->taup1 - 1) * n3;
+  S.w_tau = s->w + (size_t)(s->tau - 1) * n3;
+  S.dw_tau = s->dw + (size_t)(s->tau - 1) * n3;
+  S.dw_taum1 = s->dw + (size_t)(s->taum1 - 1) * n3;
+  S.dw_mix = s->dw_mix;
+  S.p1 = s->p_non_hydro + (size_t)(s->taup1 - 1) * n3;
+  S.p0 = s->p_non_hydro + (size_t)(s->tau - 1) * n3;
+  S.pm = s->p_non_hydro + (size_t)(s->taum1 - 1) * n3;
+  S.forc = h->stage_f;
+  S.dt_mom = s->dt_mom;
+  S.AB_eps = s->AB_eps;
+  launch_nh_step_pre(S, st);   // w(taup1), setcyclic u/v/w, forcing, first guess
+  NCK(cudaGetLastError());
+  const int rc = nh_run_cg(h, h->stage_f, S.p1, s->congr_epsilon_non_hydro, s->congr_max_itts_non_hydro, info, st);
+  if (rc < 0) return rc;
+  s->congr_itts_non_hydro = info ? info->iterations : h->h_result->iterations;
+  launch_nh_step_post(S, st);  // setcyclic p, velocity correction
+  if (s->itt == 0) {           // :44-47
+    double* p_tau = s->p_non_hydro + (size_t)(s->tau - 1) * n3;
+    double* p_taum1 = s->p_non_hydro + (size_t)(s->taum1 - 1) * n3;
+    NCK(cudaMemcpyAsync(p_tau, S.p1, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    NCK(cudaMemcpyAsync(p_taum1, S.p1, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  NCK(cudaGetLastError());
+  NCK(cudaStreamSynchronize(st));
+  return rc;
 }
 
 }  // extern "C"

@@ -164,6 +164,24 @@ struct alignas(64) NHParams {
   CGResult* out;
 };
 
+// Arrays of one solve_non_hydrostatic step (non_hydrostatic.f90:5-63), all
+// device memory in Fortran layout; the u, v, w, p pointers are already offset
+// to their time level.
+struct NHStep {
+  NHGeo G;
+  const double *dxt, *dxu, *dyt, *dyu, *cost, *cosu;  // [nx+4] / [ny+4]
+  const double *dzt, *dzw;                            // [nz]
+  const uint8_t *maskU, *maskV, *maskW;               // (nx+4, ny+4, nz), 0/1
+  double *u, *v, *w;                                  // taup1
+  const double *w_tau, *dw_tau, *dw_taum1, *dw_mix;
+  double *p1;                                         // p_non_hydro(:,:,:,taup1)
+  const double *p0, *pm;                              // tau, taum1
+  double* forc;                                       // (nx+4, ny+4, nz) scratch
+  double dt_mom, AB_eps;
+};
+void launch_nh_step_pre(const NHStep& S, cudaStream_t st);
+void launch_nh_step_post(const NHStep& S, cudaStream_t st);
+
 const void* nh_cg_kernel_ptr(bool cyclic_x, bool cyclic_y);
 void launch_nh_apply(const NHGeo& G, const NHOp& op, const double* p, double* res, cudaStream_t st);
 void launch_nh_pack(const NHGeo& G, const double* user, double* padded, cudaStream_t st);

@@ -176,24 +176,20 @@ def random_field(shape_f, sigma, gen):
     return f.T  # Fortran view
 
 
-def generate_and_train(pc: LearnedPreconditioner, W, em: ExternalMode, basis, steps, lr, seed, log=None,
-                       pairs_per_rhs=24, restart_range=(0, 40), lr_final=None):
-    """``steps`` Adam steps on fresh pairs.  A right-hand side b is a random
-    combination of ``basis``; its tight solution x* comes from Jacobi-PCG.
-    Each pair starts the plain solver from x* plus a smooth random
-    perturbation (random correlation length 1-96 cells) and runs a random
-    number of restarted PCG iterations; the iterate x gives r = b - A x and
-    e = x* - x."""
+def pair_stream(W, em: ExternalMode, basis, seed, pairs_per_rhs=24, restart_range=(0, 40)):
+    """Endless stream of training pairs (r, e).  A right-hand side b is a
+    random combination of ``basis``; its tight solution x* comes from
+    Jacobi-PCG.  Each pair starts the plain solver from x* plus a smooth
+    random perturbation (random correlation length 1-96 cells) and runs a
+    random number of restarted PCG iterations; the iterate x gives r = b - A x
+    and e = x* - x."""
     import torch
     rng = np.random.default_rng(np.random.PCG64(seed))
     gen = torch.Generator(device="cuda")
     gen.manual_seed(int(seed) * 7919 + 1)
     B = [_dev(b) for b in basis]
     mask = _dev((em.make_inv_sfc() != 0).astype(np.float64))
-    losses = []
-    step = 0
-    lr0 = lr
-    while step < steps:
+    while True:
         c = rng.standard_normal(len(B))
         b = sum(float(ck) * Bk for ck, Bk in zip(c, B))
         b = b.T.contiguous().T  # Fortran order
@@ -201,8 +197,6 @@ def generate_and_train(pc: LearnedPreconditioner, W, em: ExternalMode, basis, st
         em.solve_rtol(b, xs, rtol=1e-12, precision=_abi.PREC_F64)
         xs_rms = float(xs[mask > 0].pow(2).mean().sqrt())
         for _ in range(pairs_per_rhs):
-            if step >= steps:
-                break
             sigma = float(np.exp(rng.uniform(np.log(1.0), np.log(96.0))))
             amp = xs_rms * float(np.exp(rng.uniform(np.log(1e-3), np.log(1.0))))
             d = random_field(em.shape, sigma, gen) * mask * amp
@@ -214,11 +208,21 @@ def generate_and_train(pc: LearnedPreconditioner, W, em: ExternalMode, basis, st
                     em.congrad_streamfunction(b, x, eps=0.0, max_it=m)
             r = ((b - em.apply_op(x)) * mask).T.contiguous().T
             e = (xs - x).T.contiguous().T
-            if lr_final is not None:
-                lr = lr0 * (lr_final / lr0) ** (step / max(1, steps - 1))
-            loss = pc.train_step(r, e, lr)
-            losses.append(loss)
-            step += 1
-            if log and step % 200 == 0:
-                log(f"step {step} loss(avg200) {np.mean(losses[-200:]):.4f}")
+            yield r, e
+
+
+def generate_and_train(pc: LearnedPreconditioner, W, em: ExternalMode, basis, steps, lr, seed, log=None,
+                       pairs_per_rhs=24, restart_range=(0, 40), lr_final=None):
+    """``steps`` Adam steps on fresh pairs from :func:`pair_stream`; with
+    ``lr_final`` the learning rate decays geometrically from ``lr`` to it."""
+    losses = []
+    lr0 = lr
+    stream = pair_stream(W, em, basis, seed, pairs_per_rhs, restart_range)
+    for step in range(steps):
+        r, e = next(stream)
+        if lr_final is not None:
+            lr = lr0 * (lr_final / lr0) ** (step / max(1, steps - 1))
+        losses.append(pc.train_step(r, e, lr))
+        if log and (step + 1) % 200 == 0:
+            log(f"step {step + 1} loss(avg200) {np.mean(losses[-200:]):.4f}")
     return losses

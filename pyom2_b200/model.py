@@ -103,6 +103,9 @@ class ModelState:
         for name in ("du_mix", "dv_mix", "p_hydro"):
             setattr(self, name, zeros_f(X, Y, nz))
         self.p_non_hydro = zeros_f(X, Y, nz, 3)          # main_module.f90:337
+        self.w = zeros_f(X, Y, nz, 3)                    # main_module.f90:298-311
+        self.dw = zeros_f(X, Y, nz, 3)
+        self.dw_mix = zeros_f(X, Y, nz)
         self.psi = zeros_f(X, Y, 3)
         self.dpsi = zeros_f(X, Y, 3)
         # island variables, allocated by streamfunction_init (streamfct_init.f90:87-93)

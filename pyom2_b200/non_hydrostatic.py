@@ -7,6 +7,8 @@ make_coeff_non_hydro (non_hydrostatic.f90:70)  :class:`NonHydrostatic` (operator
 congrad_non_hydro (non_hydrostatic.f90:146)    :meth:`NonHydrostatic.congrad_non_hydro`,
                                                :func:`congrad_non_hydro`
 apply_op_3D (non_hydrostatic.f90:247)          :meth:`NonHydrostatic.apply_op_3d`
+solve_non_hydrostatic (non_hydrostatic.f90:5)  :meth:`NonHydrostatic.solve_non_hydrostatic`,
+                                               :func:`solve_non_hydrostatic`
 =============================================  ====================================================
 
 Arrays are Fortran-ordered float64 (nx+4, ny+4, nz) buffers: numpy (host,
@@ -23,7 +25,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import PyOMGPUError
-from .external import _f64, _host, _is_torch, _ptr, _stream, _torch_like
+from .external import _f64, _from_device_f, _host, _is_torch, _ptr, _stream, _to_device_f, _torch_like
 
 
 class NonHydrostatic:
@@ -105,6 +107,37 @@ class NonHydrostatic:
         return info.iterations, info.as_dict()
 
 
+    def solve_non_hydrostatic(self, M=None):
+        """non_hydrostatic.f90:5-63 on the model arrays u, v, w, dw, dw_mix,
+        p_non_hydro (numpy host arrays are copied to the GPU and back; torch
+        CUDA tensors are updated in place).  Sets M.congr_itts_non_hydro and
+        returns the solve's info dict."""
+        import torch
+        M = M or self.M
+        dev = torch.device("cuda")
+        D = {n: _to_device_f(getattr(M, n), dev) for n in ("u", "v", "w", "dw", "dw_mix", "p_non_hydro")}
+        s = _abi.State3D()
+        s.taum1, s.tau, s.taup1, s.itt = int(M.taum1), int(M.tau), int(M.taup1), int(M.itt)
+        s.congr_max_itts_non_hydro = int(M.congr_max_itts_non_hydro)
+        s.dt_mom, s.AB_eps = float(M.dt_mom), float(M.AB_eps)
+        s.congr_epsilon_non_hydro = float(M.congr_epsilon_non_hydro)
+        for n, t in D.items():
+            setattr(s, n, C.c_void_p(t.data_ptr()))
+        info = _abi.SolveInfo()
+        rc = self._L.pyomgpu_solve_non_hydrostatic(self._h, C.byref(s), C.byref(info), _stream())
+        _abi.check(rc, allow=(_abi.OK, _abi.MAXITER, _abi.DIVERGED))
+        if rc == _abi.MAXITER:
+            warnings.warn("solve_non_hydrostatic: max iterations exceeded", RuntimeWarning, stacklevel=2)
+        elif rc == _abi.DIVERGED:
+            warnings.warn("solve_non_hydrostatic: non hydrostatic solver diverging", RuntimeWarning, stacklevel=2)
+        for n in ("u", "v", "w", "p_non_hydro"):
+            a = getattr(M, n)
+            if not _is_torch(a):
+                a[...] = _from_device_f(D[n])
+        M.congr_itts_non_hydro = int(s.congr_itts_non_hydro)
+        return info.as_dict()
+
+
 _CACHE = {}
 
 
@@ -128,3 +161,9 @@ def congrad_non_hydro(M, forc):
     it, _ = _nh_for(M).congrad_non_hydro(forc, p)
     M.congr_itts_non_hydro = it
     return it
+
+
+def solve_non_hydrostatic(M):
+    """Module-level form of the reference call ``solve_non_hydrostatic``
+    (momentum.f90:167): updates M's u, v, w and p_non_hydro in place."""
+    return _nh_for(M).solve_non_hydrostatic(M)

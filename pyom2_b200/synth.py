@@ -550,4 +550,33 @@ def nonhydro_tank(nx, ny, nz, seed, cyclic_x=False, dx=0.01, slope=True, vel_rms
     return Workload3D(f"tank_{nx}x{ny}x{nz}", M, forc, p0, seed)
 
 
+def nonhydro_state(W: Workload3D, seed: int, vel_rms=1e-3):
+    """Fill the model arrays that solve_non_hydrostatic reads (u, v, w at
+    the three time levels, dw at tau and taum1, dw_mix, p_non_hydro at tau and
+    taum1) with seeded smooth masked fields; w is zero at the rigid lid (k =
+    nz), so the forcing the step builds is consistent."""
+    M = W.M
+    rng = np.random.default_rng(np.random.PCG64(seed))
+    shape3 = M.shape2d + (M.nz,)
+    cyc = (M.enable_cyclic_x, M.enable_cyclic_y, False)
+    sig = (max(1.0, M.nx / 16.0), max(1.0, M.ny / 16.0), max(1.0, M.nz / 8.0))
+
+    def field(mask, rms):
+        f = smooth_field(rng, shape3, sig, cyc)
+        f *= rms / (np.sqrt(np.mean(f ** 2)) + 1e-300)
+        f = np.asfortranarray(f * mask)
+        setcyclic_xy(M, f)
+        return f
+
+    for lev in range(3):
+        M.u[..., lev] = field(M.maskU, vel_rms)
+        M.v[..., lev] = field(M.maskV, vel_rms)
+        M.w[..., lev] = field(M.maskW, vel_rms)
+        M.dw[..., lev] = field(M.maskW, vel_rms * 1e-3)
+        M.p_non_hydro[..., lev] = field(M.maskT, 1e-4)
+    M.w[:, :, M.nz - 1, :] = 0.0
+    M.dw_mix[...] = field(M.maskW, vel_rms * 1e-4)
+    return W
+
+
 WORKLOADS = {"c0": config0, "c1": config1, "c3": config3}

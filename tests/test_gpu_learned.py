@@ -146,10 +146,13 @@ def test_fcg_reaches_1e10_and_matches_oracle(oracle_lib, name):
 
 
 def test_training_reduces_loss():
-    """A few hundred Adam steps on solver-generated pairs of a grid of the
-    training family (1440x720 recipe) lower the relative energy-norm loss
-    (the training loop runs end to end on the GPU: pair generation, forward,
-    loss, backward, update)."""
+    """Adam steps on solver-generated pairs of a grid of the training family
+    (1440x720 recipe) lower the relative energy-norm loss on a fixed set of
+    held-out pairs (the training loop runs end to end on the GPU: pair
+    generation, forward, loss, backward, update).  Per-pair losses are noisy
+    (random perturbation scales) and the gradient sums are not bit-for-bit
+    reproducible, so the check is on the mean over 32 fixed pairs, with the
+    learning rate annealed."""
     W = synth._global_like(1440, 720, -80.0, 80.0, 2002, n_land_masses=20, name="train_2002")
     E = ExternalMode(W.M)
     import warnings
@@ -157,10 +160,14 @@ def test_training_reduces_loss():
         warnings.simplefilter("ignore", RuntimeWarning)
         E.streamfunction_init(**LIMITS)
     basis = learned.rhs_basis(W, 2, seed=11)
+    held = learned.pair_stream(W, E, basis, seed=99)
+    held = [next(held) for _ in range(32)]
     pc = learned.LearnedPreconditioner(E, training=True, seed=0)
-    losses = learned.generate_and_train(pc, W, E, basis, steps=400, lr=1e-3, seed=4)
+    before = np.mean([pc.train_step(r, e, 0.0) for r, e in held])
+    losses = learned.generate_and_train(pc, W, E, basis, steps=800, lr=1e-3, lr_final=1e-4, seed=4)
+    after = np.mean([pc.train_step(r, e, 0.0) for r, e in held])
     assert np.all(np.isfinite(losses))
-    assert np.mean(losses[-100:]) < 0.8 * np.mean(losses[:50])
+    assert after < 0.85 * before, (before, after)
     pc.close()
 
 

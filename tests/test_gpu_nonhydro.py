@@ -143,3 +143,27 @@ def test_grid_size_changes_only_rounding(oracle_lib, blocks):
     io = O.congrad(cf, W.forc, po, eps=1e-9, max_it=5000)
     assert info["status"] == 0 and abs(it - io["iterations"]) <= 1
     nh.close()
+
+
+@pytest.mark.parametrize("cyclic_x,itt", [(False, 1), (True, 0)])
+def test_solve_non_hydrostatic_step_matches_oracle(oracle_lib, cyclic_x, itt):
+    """The whole step (non_hydrostatic.f90:5-63) on the GPU against the
+    oracle's: same iteration count within one, u, v, w and p_non_hydro at all
+    three levels within 1e-7 of their size (the CG iterate's rounding)."""
+    from pyom2_b200.non_hydrostatic import solve_non_hydrostatic
+    W = synth.nonhydro_state(synth.nonhydro_tank(48, 20, 12, 6, cyclic_x=cyclic_x), 9)
+    M = W.M
+    M.itt = itt
+    M.congr_epsilon_non_hydro = 1e-10
+    Mo = M.copy()
+    O = oracle_lib.Oracle3D(Mo)
+    rc = O.solve_non_hydrostatic()
+    assert rc == 0
+    info = solve_non_hydrostatic(M)
+    assert info["status"] == 0
+    assert abs(M.congr_itts_non_hydro - Mo.congr_itts_non_hydro) <= 1
+    for n in ("u", "v", "w", "p_non_hydro"):
+        a, b = getattr(M, n), getattr(Mo, n)
+        assert np.abs(a - b).max() <= 1e-7 * np.abs(b).max(), n
+    # fields the step does not touch are untouched
+    assert np.array_equal(M.u[..., M.tau - 1], Mo.u[..., Mo.tau - 1])
