@@ -204,6 +204,83 @@ def c2_batch(steps, warmup, count=64):
             "note": "one launch for all 64 grids vs one launch per grid; FP64 Jacobi-PCG, same stop"}
 
 
+def c3_learned(steps, warmup):
+    """Config 3: the learned FCG on the 2048x1024 grid (config-1 recipe, seed
+    1003; the network is trained on the 1440x720 family and applied to this
+    larger grid unchanged) against FP64 Jacobi-PCG, both from zero to the FP64
+    true relative residual 1e-10.  Device time by CUDA events."""
+    import warnings
+
+    import torch
+    from pyom2_b200 import _abi, learned, synth
+    from pyom2_b200.external import ExternalMode
+
+    W = synth.config3()
+    E = ExternalMode(W.M)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        E.streamfunction_init(maxipp=10**6, maxq=10**6)
+    pc = learned.LearnedPreconditioner(E, params=learned.load_params())
+    f = torch.from_numpy(np.ascontiguousarray(W.forc.T)).cuda().T
+    x = torch.zeros_like(f.T).T
+    stream = torch.cuda.current_stream()
+    out = {"workload": f"c3_{W.M.nx}x{W.M.ny}", "nisle": int(W.M.nisle), "rtol": RTOL}
+    for name, fn in (("pcg64", lambda: E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64)),
+                     ("fcg", lambda: learned.solve_fcg(E, pc, f, x, rtol=RTOL))):
+        ms, info = [], None
+        for k in range(warmup + steps):
+            x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            info = fn()
+            e1.record(stream)
+            e1.synchronize()
+            if k >= warmup:
+                ms.append(e0.elapsed_time(e1))
+        out[name] = {"ms": statistics.median(ms), "iterations": info["iterations"],
+                     "outer_iterations": info["outer_iterations"], "rel_residual": info["rel_residual"]}
+    out["fcg_speedup_vs_pcg64"] = out["pcg64"]["ms"] / out["fcg"]["ms"]
+    pc.close()
+    return out
+
+
+def c4_sequence(steps, spinup=10, members=8, methods=("ref", "batch", "pcg64", "mixed32", "fcg")):
+    """Config 4: consecutive solve_streamfunction steps of ``members``
+    re-entrant channel runs (256x256x20, 60S-30S, one 2000 m ridge) driven by
+    the seeded synthetic tendency sequence of pyom2_b200/sequence.py, each
+    solve warm-started from the reference's first guess.  Per method: a fresh
+    ensemble, ``spinup`` untimed steps, then ``steps`` steps timed with CUDA
+    events (the whole step: tendencies, begin, solve, end, for all members)."""
+    import torch
+    from pyom2_b200 import synth
+    from pyom2_b200.sequence import ChannelEnsemble
+
+    W = synth.config4()
+    out = {"workload": f"c4_{W.M.nx}x{W.M.ny}x{W.M.nz}", "members": members, "steps_timed": steps,
+           "spinup_steps": spinup, "rtol": RTOL, "congr_epsilon_ref": W.M.congr_epsilon}
+    stream = torch.cuda.current_stream()
+    for method in methods:
+        ens = ChannelEnsemble(W, members=members, seed=1004)
+        for _ in range(spinup):
+            ens.step(method, rtol=RTOL)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its, rel = [], []
+        e0.record(stream)
+        for _ in range(steps):
+            infos = ens.step(method, rtol=RTOL)
+            its += [i["iterations"] for i in infos]
+            rel += [i.get("rel_residual", -1.0) for i in infos]
+        e1.record(stream)
+        e1.synchronize()
+        out[method] = {"ms_per_step": e0.elapsed_time(e1) / steps, "mean_iterations": float(np.mean(its)),
+                       "max_rel_residual": float(max(rel))}
+        ens.close()
+    out["note"] = ("ref = congrad_streamfunction per member (reference stop congr_epsilon, absolute); the others "
+                   "stop at the FP64 true relative residual rtol; batch = all members in one launch")
+    return out
+
+
 NH_BYTES_PER_CELL_ITER = 66  # res, s read twice (32), p read + write (16), res, s written (16), flags twice (2)
 
 
@@ -306,6 +383,11 @@ def main():
     ap.add_argument("--with-c2", action="store_true",
                     help="also time config 2 (64 basins in one work-queue launch vs 64 sequential solves)")
     ap.add_argument("--c2-count", type=int, default=64, help="basins of config 2 (fewer for profiling)")
+    ap.add_argument("--with-c3", action="store_true",
+                    help="also time config 3 (learned FCG vs Jacobi-PCG on the 2048x1024 grid)")
+    ap.add_argument("--with-c4", action="store_true",
+                    help="also time config 4 (8-member channel ensemble, consecutive warm-started solves)")
+    ap.add_argument("--c4-steps", type=int, default=20, help="timed steps per method of config 4")
     ap.add_argument("--no-nh", action="store_true",
                     help="skip the non-hydrostatic 3-D pressure solve (congrad_non_hydro) leg")
     ap.add_argument("--nh-only", action="store_true",
@@ -459,6 +541,10 @@ def main():
                                      "fcg_iterations": results["fcg"]["iterations"],
                                      "pcg64_iterations": results["pcg64"]["iterations"],
                                      "speedup": results["pcg64"]["value"] / results["fcg"]["value"]}
+    if args.with_c3 and rank == 0:
+        out["c3_learned"] = c3_learned(max(1, args.steps // 5), 1)
+    if args.with_c4 and rank == 0:
+        out["c4_sequence"] = c4_sequence(args.c4_steps)
     if not args.no_nh and rank == 0:
         out["non_hydrostatic"] = nh_bench(max(2, args.steps // 3), 3, peak, nh_grid, max_it=args.nh_max_it,
                                           cpu=world == 1 and not args.no_cpu_baseline)

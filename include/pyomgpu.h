@@ -275,6 +275,19 @@ int32_t pyomgpu_line_integral(pyomgpu_ctx* ctx, int32_t isle, const double* uloc
  * supported. */
 int32_t pyomgpu_solve_streamfunction(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_solve_info* info,
                                      pyomgpu_stream stream);
+/* solve_streamfunction split around its solve, so that any solver (the batch
+ * kernel over ensemble members, pyomgpu_solve_rtol, pyomgpu_solve_fcg) can
+ * take the place of congrad_streamfunction (solve_streamfct.f90:57):
+ *   _begin: hydrostatic pressure and its gradient, the forcing (written to
+ *           forc, a DEVICE (nx+4, ny+4) array; fpx/fpy stay in the context)
+ *           and the first guess 2 dpsi(tau) - dpsi(taum1) in dpsi(:,:,taup1)
+ *           (solve_streamfct.f90:24-56);
+ *   _end:   dpsi(:,:,taup1) made cyclic, the island correction, psi and the
+ *           3-D velocity update (:58-118).
+ * begin + pyomgpu_congrad_streamfunction + end computes what
+ * pyomgpu_solve_streamfunction does.  Stream-ordered; no synchronisation. */
+int32_t pyomgpu_solve_streamfunction_begin(pyomgpu_ctx* ctx, pyomgpu_state* st, double* forc, pyomgpu_stream stream);
+int32_t pyomgpu_solve_streamfunction_end(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_stream stream);
 /* solve_pressure (solve_pressure.f90:10-82) on device-resident model arrays. */
 int32_t pyomgpu_solve_pressure(pyomgpu_ctx* ctx, pyomgpu_state* st, pyomgpu_solve_info* info,
                                pyomgpu_stream stream);

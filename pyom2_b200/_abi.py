@@ -33,6 +33,7 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_congrad_surf_press", "pyomgpu_solve_rtol",
            "pyomgpu_apply_op", "pyomgpu_get_inv_diag", "pyomgpu_line_integral",
            "pyomgpu_solve_streamfunction", "pyomgpu_solve_pressure",
+           "pyomgpu_solve_streamfunction_begin", "pyomgpu_solve_streamfunction_end",
            "pyomgpu_conv3x3_bf16", "pyomgpu_precond_num_params", "pyomgpu_precond_create",
            "pyomgpu_precond_destroy", "pyomgpu_precond_rebind", "pyomgpu_precond_set_params", "pyomgpu_precond_get_params",
            "pyomgpu_precond_get_grads", "pyomgpu_precond_apply", "pyomgpu_precond_train_step",
@@ -137,6 +138,8 @@ def load(path: str = LIB_PATH):
         "pyomgpu_line_integral": (i32, [vp, i32, vp, vp, P(d), vp]),
         "pyomgpu_solve_streamfunction": (i32, [vp, P(State), P(SolveInfo), vp]),
         "pyomgpu_solve_pressure": (i32, [vp, P(State), P(SolveInfo), vp]),
+        "pyomgpu_solve_streamfunction_begin": (i32, [vp, P(State), vp, vp]),
+        "pyomgpu_solve_streamfunction_end": (i32, [vp, P(State), vp]),
         "pyomgpu_conv3x3_bf16": (i32, [i32, i32, i32, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, i32, vp]),
         "pyomgpu_precond_num_params": (C.c_int64, []),
         "pyomgpu_precond_create": (i32, [vp, i32, P(vp)]),

@@ -1217,6 +1217,46 @@ int32_t pyomgpu_solve_streamfunction(pyomgpu_ctx* c, pyomgpu_state* s, pyomgpu_s
   return rc;
 }
 
+int32_t pyomgpu_solve_streamfunction_begin(pyomgpu_ctx* c, pyomgpu_state* s, double* forc, pyomgpu_stream stream) {
+  if (!c || !s || !forc) return fail(PYOMGPU_EINVAL, "null argument");
+  if (!state_ok(s)) return fail(PYOMGPU_EINVAL, "state arrays must be device pointers with valid time levels");
+  if (!is_device_ptr(forc)) return fail(PYOMGPU_EINVAL, "forc must be a device pointer");
+  if (!c->have_islands) return fail(PYOMGPU_ESTATE, "islands not set up (streamfunction_init)");
+  cudaStream_t st = (cudaStream_t)stream;
+  StepDev d = step_dev(c, s);
+  const size_t n2 = c->n2;
+  launch_hydrostatic(d, st);                   // solve_streamfct.f90:24-37
+  launch_sf_forcing(d, c->fpx, c->fpy, forc, st);  // :39-53 (fpx, fpy stay in the context)
+  double* dp1 = s->dpsi + (size_t)(s->taup1 - 1) * n2;
+  launch_first_guess(c->g, dp1, s->dpsi + (size_t)(s->tau - 1) * n2, s->dpsi + (size_t)(s->taum1 - 1) * n2, st);
+  CK(cudaGetLastError());
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_solve_streamfunction_end(pyomgpu_ctx* c, pyomgpu_state* s, pyomgpu_stream stream) {
+  if (!c || !s) return fail(PYOMGPU_EINVAL, "null argument");
+  if (!state_ok(s)) return fail(PYOMGPU_EINVAL, "state arrays must be device pointers with valid time levels");
+  const int nisle = c->isl.nisle;
+  if (nisle > 1 && (!c->have_psin || !c->have_line_psin)) return fail(PYOMGPU_ESTATE, "psin / line_psin missing");
+  if (nisle > 1 && !is_device_ptr(s->dpsin)) return fail(PYOMGPU_EINVAL, "dpsin must be a device pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  StepDev d = step_dev(c, s);
+  const size_t n2 = c->n2;
+  double* dp1 = s->dpsi + (size_t)(s->taup1 - 1) * n2;
+  launch_setcyclic_user(c->g, dp1, st);  // border_exchg/setcyclic (:58-59)
+  if (nisle > 1) {
+    if (c->lu_singular) return fail(PYOMGPU_SINGULAR, "in solve_streamfunction, lapack info not zero");
+    LineGeo lg = line_geo(c);
+    launch_line_integral_uv(c->nx, c->idev, lg, c->fpx, c->fpy, 1, nisle - 1, c->line_forc, st);
+    launch_line_integral_psi(c->nx, c->ny, c->idev, lg, dp1, n2, 1, 1, nisle - 1, c->line_psi0, st);
+    launch_island_solve(nisle, c->lu, c->ipiv, c->line_forc, c->line_psi0, s->dpsin, s->tau, st);
+  }
+  launch_sf_psi_update(d, c->psin, nisle, s->dpsin, st);
+  launch_sf_velocity_update(d, st);
+  CK(cudaGetLastError());
+  return PYOMGPU_OK;
+}
+
 int32_t pyomgpu_solve_pressure(pyomgpu_ctx* c, pyomgpu_state* s, pyomgpu_solve_info* info, pyomgpu_stream stream) {
   if (!c || !s) return fail(PYOMGPU_EINVAL, "null argument");
   if (!c->have_sp) return fail(PYOMGPU_ESTATE, "context has no surface-pressure operator");

@@ -21,7 +21,8 @@ rescaled to the stated rms.  The workloads:
 * ``config2``   64 closed basins, nx in [128,1024], ny in [128,768],
                 10-40 % land, 0-12 interior islands each.
 * ``config4``   256x256x20 re-entrant channel, 60S-30S, one 2000 m
-                meridional ridge; a seeded sequence of momentum tendencies.
+                meridional ridge; a seeded sequence of momentum tendencies
+                (pyom2_b200/sequence.py).
 
 The right-hand side follows solve_streamfct.f90:39-53: a vertically
 integrated forcing (fpx, fpy) is scaled by ``hur/hvr`` and its curl is the
@@ -425,6 +426,31 @@ def config3(seed: int = 1003, nx=2048, ny=1024) -> Workload:
     """2048x1024 with the config1 recipe."""
     return _global_like(nx, ny, -80.0, 80.0, seed, n_land_masses=20,
                         name=f"c3_{nx}x{ny}")
+
+
+def config4(seed: int = 1004, nx=256, ny=256, nz=20) -> Workload:
+    """Re-entrant channel: cyclic in x, 0.25 degree in x, 60S-30S, closed to
+    the north and south (calc_topo's land rows, so the walls are the two land
+    masses and the channel transport is the one island unknown), 4000 m deep
+    with one meridional ridge 2000 m high (Gaussian, 8-cell half width) at a
+    seeded longitude.  The time-dependent inputs come from
+    :class:`pyom2_b200.sequence.TendencySequence`."""
+    rng = np.random.default_rng(np.random.PCG64(seed))
+    M = ModelState(nx, ny, nz, enable_cyclic_x=True, coord_degree=True)
+    M.dxt[2:nx + 2] = 0.25
+    M.dyt[2:ny + 2] = 30.0 / ny
+    M.x_origin, M.y_origin = 0.0, -60.0
+    M.dzt[:] = 4000.0 / nz
+    M.dt_mom = 1800.0
+    M.congr_max_iterations = 20000  # the reference's channel set-ups raise it too (py_config/acc2.py:30)
+    calc_grid(M)
+    i = np.arange(1, nx + 1, dtype=np.float64)
+    ic = nx * rng.uniform(0.3, 0.7)
+    H = 4000.0 - 2000.0 * np.exp(-((i - ic) / 8.0) ** 2)
+    M.kbot[2:nx + 2, 2:ny + 2] = _kbot_from_depth(H, M.dzt[0], nz)[:, None]
+    calc_topo(M)
+    forc = np.zeros(M.shape2d, order="F")
+    return Workload(f"c4_{nx}x{ny}x{nz}", M, None, None, forc, seed, meta={"ridge_i": float(ic)})
 
 
 def basin(nx, ny, seed, land_frac, n_islands, nz=20, lat0=-60.0) -> Workload:

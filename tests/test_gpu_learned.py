@@ -201,3 +201,25 @@ def test_ablation_trained_network_gains():
     assert trained["outer_iterations"] == 1  # converged without the Jacobi-PCG fallback
     assert trained["iterations"] < 0.8 * untrained["iterations"]
     assert trained["iterations"] < 0.8 * pcg["iterations"]
+
+
+def test_fcg_on_config3_grid(oracle_lib):
+    """Config 3: the network trained on the 1440x720 family drives flexible CG
+    on the 2048x1024 grid to the FP64 true residual 1e-10; the answer agrees
+    with Jacobi-PCG's to 1e-8 relative."""
+    W = synth.config3()
+    E = ExternalMode(W.M)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        E.streamfunction_init(**LIMITS)
+    pc = learned.LearnedPreconditioner(E, params=learned.load_params())
+    s = np.zeros(W.M.shape2d, order="F")
+    info = learned.solve_fcg(E, pc, W.forc, s, rtol=1e-10, max_it=20000)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
+    sp = np.zeros(W.M.shape2d, order="F")
+    ip = E.solve_rtol(W.forc, sp, rtol=1e-10, precision=_abi.PREC_F64)
+    m = E.make_inv_sfc() != 0
+    assert np.linalg.norm((s - sp)[m]) <= 1e-8 * np.linalg.norm(sp[m])
+    print("config 3 iterations: fcg", info["iterations"], "pcg", ip["iterations"])
+    pc.close()
