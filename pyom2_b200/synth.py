@@ -428,8 +428,9 @@ def config3(seed: int = 1003, nx=2048, ny=1024) -> Workload:
                         name=f"c3_{nx}x{ny}")
 
 
-def config4(seed: int = 1004, nx=256, ny=256, nz=20) -> Workload:
-    """Re-entrant channel: cyclic in x, 0.25 degree in x, 60S-30S, closed to
+def config4(seed: int = 1004, nx=256, ny=256, nz=20, lon_extent=64.0) -> Workload:
+    """Re-entrant channel: cyclic in x, 64 degrees long (0.25 degree cells at
+    nx = 256), 60S-30S, closed to
     the north and south (calc_topo's land rows, so the walls are the two land
     masses and the channel transport is the one island unknown), 4000 m deep
     with one meridional ridge 2000 m high (Gaussian, 8-cell half width) at a
@@ -437,7 +438,7 @@ def config4(seed: int = 1004, nx=256, ny=256, nz=20) -> Workload:
     :class:`pyom2_b200.sequence.TendencySequence`."""
     rng = np.random.default_rng(np.random.PCG64(seed))
     M = ModelState(nx, ny, nz, enable_cyclic_x=True, coord_degree=True)
-    M.dxt[2:nx + 2] = 0.25
+    M.dxt[2:nx + 2] = lon_extent / nx  # 0.25 degree at the default size
     M.dyt[2:ny + 2] = 30.0 / ny
     M.x_origin, M.y_origin = 0.0, -60.0
     M.dzt[:] = 4000.0 / nz

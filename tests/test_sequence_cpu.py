@@ -8,7 +8,7 @@ from pyom2_b200.sequence import TAUX, TendencySequence
 
 
 def test_channel_grid_and_islands(oracle_lib):
-    W = synth.config4(1004, nx=64, ny=48, nz=8)
+    W = synth.config4(1004, nx=64, ny=64, nz=8)
     M = W.M
     assert M.enable_cyclic_x and not M.enable_cyclic_y
     rc, allmap, nisle, maxb = oracle_lib.Oracle(M).island_map(maxipp=10**6, maxq=10**6)
