@@ -177,9 +177,20 @@ int32_t pyomgpu_island_boundaries(int32_t nx, int32_t ny, int32_t cyclic_x, cons
                                   int32_t maxipp, int32_t maxq, int32_t* nisle, int32_t* max_boundary,
                                   int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary);
 
+/* The same result computed on the GPU (current device): connected-component
+ * labelling by union-find with labels in the reference's scan order, and one
+ * thread walking each island's coast.  kbot host or device.  Bit-identical to
+ * pyomgpu_island_boundaries; the flood-fill queue limit maxq does not apply
+ * (there is no queue).  Not in the reference. */
+int32_t pyomgpu_island_boundaries_gpu(int32_t nx, int32_t ny, int32_t cyclic_x, const int32_t* kbot, int32_t mnisle,
+                                      int32_t maxipp, int32_t maxq, int32_t* nisle, int32_t* max_boundary,
+                                      int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary,
+                                      pyomgpu_stream stream);
+
 /* Whole of streamfunction_init: land map from kbot (host), island labels,
  * perimeter tracing, one psin solve per island (batched on the GPU) and the
- * line_psin matrix.  Results stay in the context; read them with
+ * line_psin matrix (labelling and tracing as pyomgpu_island_boundaries_gpu).
+ * Results stay in the context; read them with
  * pyomgpu_island_sizes / pyomgpu_get_islands. */
 int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* ctx, const int32_t* kbot, int32_t mnisle, int32_t maxipp,
                                     int32_t maxq, double congr_epsilon, int32_t congr_max_iterations,

@@ -26,7 +26,7 @@ STATUS_NAMES = {OK: "ok", MAXITER: "max iterations exceeded", DIVERGED: "solver 
 # every symbol include/pyomgpu.h declares
 EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomgpu_ctx_destroy",
            "pyomgpu_set_sync_timeout", "pyomgpu_inject_barrier_stall", "pyomgpu_autotune", "pyomgpu_isleperim",
-           "pyomgpu_island_boundaries", "pyomgpu_streamfunction_init",
+           "pyomgpu_island_boundaries", "pyomgpu_island_boundaries_gpu", "pyomgpu_streamfunction_init",
            "pyomgpu_island_sizes", "pyomgpu_get_islands", "pyomgpu_set_islands",
            "pyomgpu_congrad_streamfunction", "pyomgpu_congrad_streamfunction_noalloc",
            "pyomgpu_congrad_streamfunction_batch",
@@ -124,6 +124,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_autotune": (i32, [vp, i32, P(i32), P(i32), P(i32), P(d), vp]),
         "pyomgpu_isleperim": (i32, [vp, i32, i32, i32, i32, i32, i32, vp, P(i32), vp]),
         "pyomgpu_island_boundaries": (i32, [i32, i32, i32, vp, i32, i32, i32, P(i32), P(i32), vp, vp, vp]),
+        "pyomgpu_island_boundaries_gpu": (i32, [i32, i32, i32, vp, i32, i32, i32, P(i32), P(i32), vp, vp, vp, vp]),
         "pyomgpu_streamfunction_init": (i32, [vp, vp, i32, i32, i32, d, i32, vp]),
         "pyomgpu_island_sizes": (i32, [vp, P(i32), P(i32)]),
         "pyomgpu_get_islands": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),

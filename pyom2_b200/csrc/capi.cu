@@ -659,6 +659,27 @@ bool state_ok(const pyomgpu_state* s) {
          s->taum1 <= 3;
 }
 
+// island_boundaries_gpu on a host or device kbot
+int gpu_islands(int nx, int ny, bool cyclic_x, const int32_t* kbot, const IslandLimits& L, IslandSet& S,
+                cudaStream_t st) {
+  const int32_t* kd = kbot;
+  int32_t* tmp = nullptr;
+  const size_t n2 = (size_t)(nx + 4) * (ny + 4);
+  if (!is_device_ptr(kbot)) {
+    if (int rc = dalloc(&tmp, n2)) return rc;
+    if (cudaMemcpyAsync(tmp, kbot, n2 * sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      cudaFree(tmp);
+      return fail(PYOMGPU_ECUDA, "island kbot upload");
+    }
+    kd = tmp;
+  }
+  const int rc = island_boundaries_gpu(nx, ny, cyclic_x, kd, L, S, nullptr, (void*)st);
+  if (tmp) cudaFree(tmp);
+  if (rc <= -100) return fail(PYOMGPU_ECUDA, "GPU island labelling failed (%d)", rc);
+  if (rc) return island_error(rc);
+  return PYOMGPU_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -845,6 +866,28 @@ int32_t pyomgpu_island_boundaries(int32_t nx, int32_t ny, int32_t cyclic_x, cons
   return PYOMGPU_OK;
 }
 
+int32_t pyomgpu_island_boundaries_gpu(int32_t nx, int32_t ny, int32_t cyclic_x, const int32_t* kbot, int32_t mnisle,
+                                      int32_t maxipp, int32_t maxq, int32_t* nisle, int32_t* max_boundary,
+                                      int32_t* boundary, int32_t* line_dir, int32_t* nr_boundary,
+                                      pyomgpu_stream stream) {
+  if (!kbot || !nisle || !max_boundary || nx < 4 || ny < 4) return fail(PYOMGPU_EINVAL, "bad arguments");
+  IslandLimits L = limits(mnisle, maxipp, maxq);
+  IslandSet S;
+  if (int rc = gpu_islands(nx, ny, cyclic_x != 0, kbot, L, S, (cudaStream_t)stream)) return rc;
+  if (!boundary) {
+    *nisle = S.nisle;
+    *max_boundary = S.max_boundary;
+    return PYOMGPU_OK;
+  }
+  if (*nisle != S.nisle || *max_boundary != S.max_boundary || !line_dir || !nr_boundary)
+    return fail(PYOMGPU_EINVAL, "island arrays sized for (%d,%d), need (%d,%d)", *nisle, *max_boundary, S.nisle,
+                S.max_boundary);
+  std::copy(S.boundary.begin(), S.boundary.end(), boundary);
+  std::copy(S.line_dir.begin(), S.line_dir.end(), line_dir);
+  std::copy(S.nr_boundary.begin(), S.nr_boundary.end(), nr_boundary);
+  return PYOMGPU_OK;
+}
+
 int32_t pyomgpu_isleperim(const int32_t* kmt, int32_t imt, int32_t jmt, int32_t cyclic, int32_t mnisle,
                           int32_t maxipp, int32_t maxq, int32_t* map, int32_t* nisle, int32_t* nippts) {
   if (!kmt || !map || !nisle || imt < 3 || jmt < 3) return fail(PYOMGPU_EINVAL, "bad isleperim arguments");
@@ -863,13 +906,9 @@ int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* c, const int32_t* kbot, int32_t
     return fail(PYOMGPU_EINVAL, "cyclic meridional boundary conditions not implemented for the streamfunction");
   cudaStream_t st = (cudaStream_t)stream;
   IslandLimits L = limits(mnisle, maxipp, maxq);
-  std::vector<int> allmap;
-  int nisle = 0, maxb = 0;
-  int rc = island_map(c->nx, c->ny, c->g.cyclic_x != 0, kbot, L, allmap, &nisle, &maxb);
-  if (rc) return island_error(rc);
   IslandSet S;
-  rc = island_trace(c->nx, c->ny, c->g.cyclic_x != 0, allmap, nisle, maxb, L, S);
-  if (rc) return island_error(rc);
+  int rc = gpu_islands(c->nx, c->ny, c->g.cyclic_x != 0, kbot, L, S, st);  // labelling + tracing on the GPU
+  if (rc) return rc;
   c->isl = std::move(S);
   if ((rc = rebuild_islands(c))) return rc;
   return psin_and_line_psin(c, eps, max_it, st);

@@ -39,4 +39,10 @@ int island_trace(int nx, int ny, bool cyclic_x, const std::vector<int>& allmap, 
                  const IslandLimits& lim, IslandSet& out);
 int lu_factor(int n, std::vector<double>& a, std::vector<int>& ipiv);
 
+// The same labelling and tracing on the GPU (islands_gpu.cu), kbot (nx+4,
+// ny+4) a device array; bit-identical results, no flood-fill queue (maxq
+// unused).  Codes below -99 are CUDA failures.  stream is a cudaStream_t.
+int island_boundaries_gpu(int nx, int ny, bool cyclic_x, const int* kbot_dev, const IslandLimits& lim,
+                          IslandSet& out, std::vector<int>* allmap_out, void* stream);
+
 }  // namespace pyomgpu

@@ -394,20 +394,23 @@ def congrad_streamfunction_batch(contexts, forcs, sols, eps=1e-12, max_it=100000
     return [i.as_dict() for i in infos]
 
 
-def island_boundaries(M, mnisle=0, maxipp=0, maxq=0):
-    """Island labels and traced perimeters (streamfct_init.f90:35-267) on the
-    host: returns (boundary, line_dir, nr_boundary) in the reference layout."""
+def island_boundaries(M, mnisle=0, maxipp=0, maxq=0, gpu=False):
+    """Island labels and traced perimeters (streamfct_init.f90:35-267):
+    returns (boundary, line_dir, nr_boundary) in the reference layout.  On
+    the host (the flood-fill restatement) or, with ``gpu``, on the GPU."""
     L = _abi.load()
     kbot = np.asfortranarray(_host(M.kbot), dtype=np.int32)
     n, mb = C.c_int32(), C.c_int32()
     args = (int(M.nx), int(M.ny), int(bool(M.enable_cyclic_x)), C.c_void_p(kbot.ctypes.data), int(mnisle),
             int(maxipp), int(maxq))
-    _abi.check(L.pyomgpu_island_boundaries(*args, C.byref(n), C.byref(mb), None, None, None))
+    fn = L.pyomgpu_island_boundaries_gpu if gpu else L.pyomgpu_island_boundaries
+    tail = (_stream(),) if gpu else ()
+    _abi.check(fn(*args, C.byref(n), C.byref(mb), None, None, None, *tail))
     b = np.zeros((n.value, mb.value, 2), dtype=np.int32, order="F")
     d = np.zeros_like(b)
     nr = np.zeros(n.value, dtype=np.int32)
-    _abi.check(L.pyomgpu_island_boundaries(*args, C.byref(n), C.byref(mb), C.c_void_p(b.ctypes.data),
-                                           C.c_void_p(d.ctypes.data), C.c_void_p(nr.ctypes.data)))
+    _abi.check(fn(*args, C.byref(n), C.byref(mb), C.c_void_p(b.ctypes.data), C.c_void_p(d.ctypes.data),
+                  C.c_void_p(nr.ctypes.data), *tail))
     return b, d, nr
 
 
