@@ -10,9 +10,11 @@
 // marked it.  So the masses are the 8-connected components of the land,
 // numbered by the scan position of their first cell, and a perimeter cell
 // carries minus the smallest label among its land neighbours.  Here:
-//   1. union-find over the scanned cells (lock-free atomicMin unions with
-//      the four forward neighbours), every root the smallest scan key of its
-//      component;
+//   1. union-find over the scanned cells (each cell starts under its
+//      smallest-key land neighbour; lock-free compare-and-swap hooking of the
+//      larger root under the smaller with the four forward neighbours;
+//      pointer jumping in every find), every root the smallest scan key of
+//      its component;
 //   2. the roots, ranked in key order by a block scan, are the labels;
 //   3. land cells take their root's label, ocean cells minus the smallest
 //      label among their land neighbours (and are counted per label).
@@ -21,8 +23,9 @@
 // need no flood fill either: a second union-find joins neighbouring cells of
 // equal island number, an island's first mass is the component of its
 // smallest scan key, and the map value at a cell (1 own first mass, -1 next
-// to it, else 0 or another mass) is evaluated where the walk reads it.  One
-// thread walks each island.
+// to it, else 0 or another mass) is evaluated where it is read.  The start
+// points of all islands are searched at once (the first hit in the
+// reference's search order per island), then one thread walks each island.
 //
 // Differences from the reference, both only in failure cases: there is no
 // flood-fill queue, so its capacity limit maxq never applies; the perimeter
@@ -68,31 +71,40 @@ struct IGrid {
 
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
-__device__ __forceinline__ int find_root(const int* parent, int x) {
-  int p = vload(parent + x);
-  while (p != x) {
-    x = p;
-    p = vload(parent + x);
+// Root of x with intermediate pointer jumping: every visited node is pointed
+// past its parent.  Parents only ever move to smaller keys of the same
+// component, so concurrent jumps keep the forest valid.
+__device__ __forceinline__ int find_root(int* parent, int x) {
+  int curr = vload(parent + x);
+  if (curr != x) {
+    int prev = x, next;
+    while (curr > (next = vload(parent + curr))) {
+      parent[prev] = next;
+      prev = curr;
+      curr = next;
+    }
   }
-  return x;
+  return curr;
 }
 
-// Join the components of a and b; the root with the smaller key survives.
-// Every atomicMin either links or lowers a link, so retries are finite; the
-// cap turns a pathological case into an error instead of a long spin.
+// Join the components of a and b: the larger root is hooked under the
+// smaller one by compare-and-swap, retried from the value found when another
+// thread got there first.  Each failed swap moves to a smaller key, so the
+// retries are finite; the cap turns a pathological case into an error.
 __device__ __forceinline__ bool unite(int* parent, int a, int b) {
+  a = find_root(parent, a);
+  b = find_root(parent, b);
   for (int it = 0; it < kUnionCap; ++it) {
-    a = find_root(parent, a);
-    b = find_root(parent, b);
     if (a == b) return true;
-    if (a > b) {
-      const int t = a;
-      a = b;
-      b = t;
+    if (a < b) {
+      const int old = atomicCAS(parent + b, b, a);
+      if (old == b) return true;
+      b = old;
+    } else {
+      const int old = atomicCAS(parent + a, a, b);
+      if (old == a) return true;
+      a = old;
     }
-    const int old = atomicMin(parent + b, a);
-    if (old == b) return true;
-    b = old;
   }
   return false;
 }
@@ -111,12 +123,25 @@ __device__ __forceinline__ bool is_land(const IGrid& G, const int* kbot, int i, 
   return kbot[(size_t)(fi + 1) + (size_t)(fj + 1) * (G.nx + 4)] <= 0;
 }
 
+// parent = the smallest key among the cell and its 8-adjacent land cells
+// (shallow initial trees), -1 for ocean
 __global__ void k_init_land(IGrid G, const int* kbot, int* parent) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= G.K()) return;
   int i, j;
   G.cell(k, i, j);
-  parent[k] = is_land(G, kbot, i, j) ? k : -1;
+  if (!is_land(G, kbot, i, j)) {
+    parent[k] = -1;
+    return;
+  }
+  const int e = G.east(i), w = G.west(i), n = G.north(j), s = G.south(j);
+  const int ni[8] = {i, e, e, e, i, w, w, w}, nj[8] = {n, n, j, s, s, s, j, n};
+  int m = k;
+  for (int q = 0; q < 8; ++q) {
+    if (ni[q] == 0 || nj[q] == 0) continue;
+    if (is_land(G, kbot, ni[q], nj[q])) m = min(m, G.key(ni[q], nj[q]));
+  }
+  parent[k] = m;
 }
 
 // union with the four forward neighbours (east, north-east, north, north-west):
@@ -143,8 +168,19 @@ __global__ void k_init_isle(IGrid G, const int* allmap, int* parent, int* first_
   int i, j;
   G.cell(k, i, j);
   const int v = allmap[G.at(i, j)];
-  parent[k] = v > 0 ? k : -1;
-  if (v > 0) atomicMin(first_key + v, k);
+  if (v <= 0) {
+    parent[k] = -1;
+    return;
+  }
+  atomicMin(first_key + v, k);
+  const int e = G.east(i), w = G.west(i), n = G.north(j), s = G.south(j);
+  const int ni[8] = {i, e, e, e, i, w, w, w}, nj[8] = {n, n, j, s, s, s, j, n};
+  int m = k;
+  for (int q = 0; q < 8; ++q) {
+    if (ni[q] == 0 || nj[q] == 0) continue;
+    if (allmap[G.at(ni[q], nj[q])] == v) m = min(m, G.key(ni[q], nj[q]));
+  }
+  parent[k] = m;
 }
 
 __global__ void k_union_isle(IGrid G, const int* allmap, int* parent, int* err) {
@@ -285,9 +321,39 @@ __device__ int isle_map(const IGrid& G, const int* allmap, const int* parent, in
   return 0;
 }
 
-// streamfct_init.f90:116-257, one thread per island
-__global__ void k_trace(IGrid G, const int* allmap, const int* parent, const int* first_key, int nisle, int max_boundary,
-                        int* boundary, int* line_dir, int* nr_boundary, int* status) {
+// Position of Fortran (i, j) in the start-point search order of
+// streamfct_init.f90:116-165: columns nx/2+1 .. nx, then nx/2 .. 1; j = 0 .. ny.
+__device__ __forceinline__ long long start_order(int nx, int ny, int i, int j) {
+  const int h = nx / 2;
+  const long long col = i >= h + 1 ? (long long)(i - (h + 1)) : (long long)(nx - h) + (h - i);
+  return col * (ny + 1) + j;
+}
+
+// Start-point search of every island at once: (i, j) is a start of island v
+// when v's map reads (1, -1) or (-1, 1) at (i, j), (i, j+1); each island keeps
+// the first such point in the search order.
+__global__ void k_start(IGrid G, const int* allmap, const int* parent, const int* first_key,
+                        unsigned long long* start) {
+  const int nx = G.nx, ny = G.ny;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)nx * (ny + 1)) return;
+  const int i = 1 + (int)(e % nx), j = (int)(e / nx);
+  const int c0 = allmap[G.at(i + 2, j + 2)], c1 = allmap[G.at(i + 2, j + 3)];
+  for (int t = 0; t < 2; ++t) {
+    const int v = t == 0 ? c0 : c1;
+    if (v <= 0 || (t == 1 && v == c0)) continue;
+    const int a = isle_map(G, allmap, parent, first_key[v], v, i + 2, j + 2);
+    const int b = isle_map(G, allmap, parent, first_key[v], v, i + 2, j + 3);
+    if ((a == 1 && b == -1) || (a == -1 && b == 1))
+      atomicMin(start + v, (unsigned long long)start_order(nx, ny, i, j));
+  }
+}
+
+// streamfct_init.f90:116-257: the coast walk, one thread per island, from the
+// start point k_start found
+__global__ void k_trace(IGrid G, const int* allmap, const int* parent, const int* first_key,
+                        const unsigned long long* start, int nisle, int max_boundary, int* boundary, int* line_dir,
+                        int* nr_boundary, int* status) {
   const int isle = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (isle > nisle) return;
   const int nx = G.nx, ny = G.ny;
@@ -296,35 +362,30 @@ __global__ void k_trace(IGrid G, const int* allmap, const int* parent, const int
   auto B = [&](int* a, int n, int c) -> int& {
     return a[(size_t)(isle - 1) + (size_t)(n - 1) * nisle + (size_t)(c - 1) * nisle * max_boundary];
   };
-  int ij0 = 0, ij1 = 0, d0 = 0, d1 = 0;
-  bool found = false;
-  auto probe = [&](int i) {
-    for (int j = 0; j <= ny && !found; ++j) {
-      const int a = M(i, j), b = M(i, j + 1);
-      if (a == 1 && b == -1) {
-        ij0 = i;
-        ij1 = j;
-        d0 = 1;
-        d1 = 0;
-        B(boundary, 1, 1) = i - 1;
-        B(boundary, 1, 2) = j;
-        found = true;
-      } else if (a == -1 && b == 1) {
-        ij0 = i - 1;
-        ij1 = j;
-        d0 = -1;
-        d1 = 0;
-        B(boundary, 1, 1) = i;
-        B(boundary, 1, 2) = j;
-        found = true;
-      }
-    }
-  };
-  for (int i = nx / 2 + 1; i <= nx && !found; ++i) probe(i);
-  for (int i = nx / 2; i >= 1 && !found; --i) probe(i);
-  if (!found) {
+  if (start[isle] == ~0ull) {
     status[isle - 1] = kIslNoStart;
     return;
+  }
+  int ij0 = 0, ij1 = 0, d0 = 0, d1 = 0;
+  {
+    const long long o = (long long)start[isle];
+    const int h = nx / 2;
+    const long long col = o / (ny + 1);
+    const int j = (int)(o % (ny + 1));
+    const int i = col < nx - h ? (int)(h + 1 + col) : (int)(h - (col - (nx - h)));
+    if (M(i, j) == 1) {  // (1, -1): walk east
+      ij0 = i;
+      ij1 = j;
+      d0 = 1;
+      B(boundary, 1, 1) = i - 1;
+      B(boundary, 1, 2) = j;
+    } else {  // (-1, 1): walk west
+      ij0 = i - 1;
+      ij1 = j;
+      d0 = -1;
+      B(boundary, 1, 1) = i;
+      B(boundary, 1, 2) = j;
+    }
   }
   B(line_dir, 1, 1) = d0;
   B(line_dir, 1, 2) = d1;
@@ -481,9 +542,14 @@ int island_boundaries_gpu(int nx, int ny, bool cyclic_x, const int* kbot_dev, co
   k_init_isle<<<nb, kIGThreads, 0, st>>>(G, allmap, parent, first_key);
   k_union_isle<<<nb, kIGThreads, 0, st>>>(G, allmap, parent, scal + 1);
   k_flatten<<<nb, kIGThreads, 0, st>>>(G, parent);
-  if (nisle > 0)
-    k_trace<<<nblk(nisle), kIGThreads, 0, st>>>(G, allmap, parent, first_key, nisle, max_boundary, boundary, line_dir,
-                                                nr, status);
+  unsigned long long* start = D.get<unsigned long long>((size_t)nisle + 1);
+  if (!start) return -100;
+  cudaMemsetAsync(start, 0xff, ((size_t)nisle + 1) * sizeof(unsigned long long), st);
+  if (nisle > 0) {
+    k_start<<<nblk((size_t)nx * (ny + 1)), kIGThreads, 0, st>>>(G, allmap, parent, first_key, start);
+    k_trace<<<nblk(nisle), kIGThreads, 0, st>>>(G, allmap, parent, first_key, start, nisle, max_boundary, boundary,
+                                                line_dir, nr, status);
+  }
   out.nisle = nisle;
   out.max_boundary = max_boundary;
   out.boundary.assign((size_t)nisle * max_boundary * 2, 0);
