@@ -244,7 +244,7 @@ def c3_learned(steps, warmup):
     return out
 
 
-def c4_sequence(steps, spinup=10, members=8, methods=("ref", "batch", "pcg64", "mixed32", "fcg")):
+def c4_sequence(steps, spinup=10, members=8, methods=("ref", "batch_ref", "batch", "pcg64", "mixed32", "fcg")):
     """Config 4: consecutive solve_streamfunction steps of ``members``
     re-entrant channel runs (256x256x20, 60S-30S, one 2000 m ridge) driven by
     the seeded synthetic tendency sequence of pyom2_b200/sequence.py, each
@@ -276,8 +276,9 @@ def c4_sequence(steps, spinup=10, members=8, methods=("ref", "batch", "pcg64", "
         out[method] = {"ms_per_step": e0.elapsed_time(e1) / steps, "mean_iterations": float(np.mean(its)),
                        "max_rel_residual": float(max(rel))}
         ens.close()
-    out["note"] = ("ref = congrad_streamfunction per member (reference stop congr_epsilon, absolute); the others "
-                   "stop at the FP64 true relative residual rtol; batch = all members in one launch")
+    out["note"] = ("ref = congrad_streamfunction per member, batch_ref = all members in one launch, both with the "
+                   "reference stop (congr_epsilon, absolute); the others stop at the FP64 true relative residual "
+                   "rtol; batch = all members in one launch")
     return out
 
 

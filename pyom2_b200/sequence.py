@@ -26,13 +26,14 @@ Each step runs ``pyomgpu_solve_streamfunction_begin`` for every member, one
 of the solvers below on the members' forcings, and
 ``pyomgpu_solve_streamfunction_end`` for every member:
 
-=========  ============================================================
-"ref"      congrad_streamfunction per member (the reference algorithm and stop)
-"batch"    all members in one launch of the work-queue kernel (FP64 PCG, rtol stop)
-"pcg64"    pyomgpu_solve_rtol FP64 per member (rtol stop)
-"mixed32"  pyomgpu_solve_rtol FP32 with FP64 refinement per member (rtol stop)
-"fcg"      the learned flexible CG per member (rtol stop, Jacobi-PCG fallback)
-=========  ============================================================
+===========  ==========================================================================
+"ref"        congrad_streamfunction per member (the reference algorithm and stop)
+"batch_ref"  all members in one launch of the work-queue kernel, the reference's stop
+"batch"      all members in one launch of the work-queue kernel (FP64 PCG, rtol stop)
+"pcg64"      pyomgpu_solve_rtol FP64 per member (rtol stop)
+"mixed32"    pyomgpu_solve_rtol FP32 with FP64 refinement per member (rtol stop)
+"fcg"        the learned flexible CG per member (rtol stop, Jacobi-PCG fallback)
+===========  ==========================================================================
 """
 from __future__ import annotations
 
@@ -193,6 +194,11 @@ class ChannelEnsemble:
         sols = [self.dpsi_taup1(m) for m in range(self.members)]
         if method == "batch":
             return congrad_streamfunction_batch(self.ems, forcs, sols, eps=0.0, max_it=10**6, rtol=rtol)
+        if method == "batch_ref":
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore", RuntimeWarning)
+                return congrad_streamfunction_batch(self.ems, forcs, sols, eps=float(self.M.congr_epsilon),
+                                                    max_it=int(self.M.congr_max_iterations), rtol=0.0)
         out = []
         for m, E in enumerate(self.ems):
             if method == "ref":

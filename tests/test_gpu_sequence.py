@@ -73,3 +73,24 @@ def test_solvers_agree_on_the_sequence():
         for m in range(3):
             a, b = res[method][m], res["batch"][m]
             assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max(), (method, m)
+
+
+def test_batched_reference_stop_matches_sequential():
+    """All members in one work-queue launch with the reference's own stop
+    (congr_epsilon): the same states as the per-member congrad path."""
+    W = small_channel(1006)
+    out = {}
+    for method in ("ref", "batch_ref"):
+        ens = ChannelEnsemble(W, members=3, seed=1006)
+        its = []
+        for step in range(3):
+            infos = ens.step(method)
+            its.append([i["iterations"] for i in infos])
+        out[method] = ([ens.host_state(m) for m in range(3)], its)
+        ens.close()
+    for step_its_a, step_its_b in zip(out["ref"][1], out["batch_ref"][1]):
+        assert all(abs(a - b) <= 1 for a, b in zip(step_its_a, step_its_b))
+    for m in range(3):
+        for n in ("psi", "dpsi", "u"):
+            a, b = out["batch_ref"][0][m][n], out["ref"][0][m][n]
+            assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max(), (m, n)
