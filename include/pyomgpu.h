@@ -338,6 +338,12 @@ int32_t pyomgpu_nh_set_grid(pyomgpu_nh* nh, int32_t blocks);
 int32_t pyomgpu_nh_set_brick(pyomgpu_nh* nh, int32_t ty, int32_t kc);
 /* TMA pipeline depth of the CG sweeps: 2..4 stages (0 = automatic, 2). */
 int32_t pyomgpu_nh_set_stages(pyomgpu_nh* nh, int32_t stages);
+/* CG kernel: 1 = the grid-wide brick kernel, 2 = one thread-block cluster
+ * (up to 16 blocks) with the fields resident in distributed shared memory
+ * (grids of at most 110704 cells; cluster barriers instead of grid barriers,
+ * so the barrier-stall hook does not apply), 0 = automatic (2 up to 32768
+ * cells).  Reduction order differs, results change at rounding level. */
+int32_t pyomgpu_nh_set_variant(pyomgpu_nh* nh, int32_t variant);
 /* res = A p1 over the interior, zero halo (apply_op_3D).  (nx+4, ny+4, nz)
  * Fortran-layout arrays, host or device. */
 int32_t pyomgpu_apply_op_3d(pyomgpu_nh* nh, const double* p1, double* res, pyomgpu_stream stream);

@@ -39,7 +39,8 @@ EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomg
            "pyomgpu_precond_get_grads", "pyomgpu_precond_apply", "pyomgpu_precond_train_step",
            "pyomgpu_unet_forward_backward", "pyomgpu_solve_fcg",
            "pyomgpu_nh_create", "pyomgpu_nh_destroy", "pyomgpu_nh_set_sync_timeout",
-           "pyomgpu_nh_inject_barrier_stall", "pyomgpu_nh_set_grid", "pyomgpu_nh_set_brick", "pyomgpu_nh_set_stages", "pyomgpu_apply_op_3d",
+           "pyomgpu_nh_inject_barrier_stall", "pyomgpu_nh_set_grid", "pyomgpu_nh_set_brick", "pyomgpu_nh_set_stages", "pyomgpu_nh_set_variant",
+           "pyomgpu_apply_op_3d",
            "pyomgpu_congrad_non_hydro", "pyomgpu_solve_non_hydrostatic")
 
 
@@ -160,6 +161,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_nh_set_grid": (i32, [vp, i32]),
         "pyomgpu_nh_set_brick": (i32, [vp, i32, i32]),
         "pyomgpu_nh_set_stages": (i32, [vp, i32]),
+        "pyomgpu_nh_set_variant": (i32, [vp, i32]),
         "pyomgpu_apply_op_3d": (i32, [vp, vp, vp, vp]),
         "pyomgpu_congrad_non_hydro": (i32, [vp, vp, vp, d, i32, P(SolveInfo), vp]),
         "pyomgpu_solve_non_hydrostatic": (i32, [vp, P(State3D), P(SolveInfo), vp]),

@@ -35,10 +35,14 @@
 #include <cstring>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "../../include/pyomgpu.h"
 #include "cg_ref.cuh"
 #include "nonhydro.cuh"
 #include "tma.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace pyomgpu {
 
@@ -223,6 +227,111 @@ __device__ __forceinline__ bool nh_sweep(const NHParams& P, int cur, double bq, 
   return __syncthreads_and(ok && prod_ok) != 0;  // also: every stage is read to the end before the next sweep
 }
 
+// Scalar state of congrad_non_hydro's loop (non_hydrostatic.f90:177-242),
+// the same in every thread of every block.  The convergence test of
+// iteration n needs max|p| of the direction formed after it, so it runs after
+// the next iteration's first sweep (after_a).
+struct NHCtl {
+  enum { kGo = 0, kOk = 1, kErr = 2 };
+  double beta = 0, bb = 0, rtol2bb = 0, eps = 0, rtol = 0;
+  double betamin = 0, step1 = 0, est = 0, bq = 0, alpha_prev = 0, rr_prev = 0;
+  int max_it = 0, n = 0, status = PYOMGPU_OK;
+
+  __device__ int start(double rsold, double bb_, const NHParams& P) {
+    beta = rsold;
+    bb = bb_;
+    rtol = P.rtol;
+    rtol2bb = P.rtol * P.rtol * bb;
+    eps = P.eps;
+    max_it = P.max_it;
+    rr_prev = beta;
+    if (beta == 0.0) {  // :177
+      n = 0;
+      return kOk;
+    }
+    if (max_it < 1) {
+      n = 1;
+      status = PYOMGPU_MAXITER;
+      return kErr;
+    }
+    n = 1;
+    return kGo;
+  }
+  // after sweep A of iteration n: (s_n, A s_n) and max|s_n| over maskT
+  __device__ int after_a(double sAs, double smax, double& alpha) {
+    if (n > 1) {  // convergence test of iteration n-1 (:215-226)
+      const int m = n - 1;
+      const double step = fabs(alpha_prev) * smax;
+      if (m == 1) {
+        step1 = step;
+        est = step;
+        if (step < eps) {
+          n = m;
+          return kOk;
+        }
+      } else if (step < eps) {
+        const double rate = exp(log(step / step1) / (double)(m - 1));
+        est = step * rate / (1.0 - rate);
+        if (est < eps) {
+          n = m;
+          return kOk;
+        }
+      }
+      if (est != est) {
+        n = m;
+        status = PYOMGPU_NAN;
+        return kErr;
+      }
+      if (rtol > 0.0 && (bb > 0.0 ? rr_prev <= rtol2bb : rr_prev == 0.0)) {
+        est = sqrt(rr_prev);
+        n = m;
+        return kOk;
+      }
+      if (m >= max_it) {  // :228
+        n = max_it + 1;
+        status = PYOMGPU_MAXITER;
+        return kErr;
+      }
+    }
+    if (sAs == 0.0) return kOk;  // :185
+    alpha = beta / sAs;
+    return kGo;
+  }
+  // after sweep B of iteration n: rsnew = (res, res) over maskT
+  __device__ int after_b(double rsnew, double alpha) {
+    bq = rsnew / beta;  // p = res + rsnew/rsold*p (:189)
+    beta = rsnew;
+    if (n == 1) {  // divergence test (:197-205)
+      betamin = fabs(rsnew);
+    } else if (n > 2) {
+      betamin = fmin(betamin, fabs(rsnew));
+      if (fabs(rsnew) > 100.0 * betamin) {
+        status = PYOMGPU_DIVERGED;
+        return kErr;
+      }
+    }
+    alpha_prev = alpha;
+    rr_prev = rsnew;
+    ++n;
+    return kGo;
+  }
+  __device__ void finish(int how, CGResult* out) {
+    int converged = 0;
+    if (how == kOk) {
+      converged = 1;
+      status = PYOMGPU_OK;
+    } else if (est != est) {
+      status = PYOMGPU_NAN;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      out->iterations = n;
+      out->converged = converged;
+      out->status = status;
+      out->est = est;
+    }
+  }
+};
+
 template <bool CX, bool CY>
 __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_constant__ NHParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -285,33 +394,17 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
   if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns, P.stall_extra)) return;
   double red0[2];
   grid_collect<2, -1, kNHThreads>(P.slots, 4, nb, red0);
-  double beta = red0[0];
-  const double bb = red0[1];
-  const double rtol2bb = P.rtol * P.rtol * bb;
+  NHCtl ctl;
+  int how = ctl.start(red0[0], red0[1], P);
 
-  const double eps = P.eps;
-  const int max_it = P.max_it;
-  double betamin = 0.0, step1 = 0.0, est = 0.0, bq = 0.0, alpha_prev = 0.0, rr_prev = beta;
-  int n = 0, status = PYOMGPU_OK, converged = 0;
-
-  if (beta == 0.0) {  // :177
-    n = 0;
-    goto done_ok;
-  }
-  if (max_it < 1) {
-    n = 1;
-    status = PYOMGPU_MAXITER;
-    goto done_err;
-  }
-
-  for (n = 1;; n++) {
-    const int cur = n & 1;
+  while (how == NHCtl::kGo) {
+    const int cur = ctl.n & 1;
     // -------------------------------------------------------------- sweep A
     {
       double* __restrict__ Sn = P.s[cur ^ 1];
       double acc_dot = 0.0, acc_max = 0.0;
       const bool ok = nh_sweep<false>(
-          P, cur, bq, smem, pp,
+          P, cur, ctl.bq, smem, pp,
           [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double, double) {
             ptrdiff_t ox, oy;
             nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
@@ -332,103 +425,260 @@ __global__ void __launch_bounds__(kNHThreads, 2) nh_cg_kernel(const __grid_const
     }
     const unsigned long long ep_a = epoch;
     if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
-    double sAs, smax;
-    {
-      double r2[2];
-      grid_collect<2, 1, kNHThreads>(P.slots + (size_t)((ep_a & 1) * nb) * 4, 4, nb, r2);
-      sAs = r2[0];
-      smax = r2[1];
-    }
-    if (n > 1) {  // convergence test of iteration n-1 (:215-226) with max|p| of its new p
-      const int m = n - 1;
-      const double step = fabs(alpha_prev) * smax;
-      if (m == 1) {
-        step1 = step;
-        est = step;
-        if (step < eps) {
-          n = m;
-          goto done_ok;
-        }
-      } else if (step < eps) {
-        const double rate = exp(log(step / step1) / (double)(m - 1));
-        est = step * rate / (1.0 - rate);
-        if (est < eps) {
-          n = m;
-          goto done_ok;
-        }
-      }
-      if (est != est) {
-        n = m;
-        status = PYOMGPU_NAN;
-        goto done_err;
-      }
-      if (P.rtol > 0.0 && (bb > 0.0 ? rr_prev <= rtol2bb : rr_prev == 0.0)) {
-        est = sqrt(rr_prev);
-        n = m;
-        goto done_ok;
-      }
-      if (m >= max_it) {  // :228
-        n = max_it + 1;
-        status = PYOMGPU_MAXITER;
-        goto done_err;
-      }
-    }
-    if (sAs == 0.0) goto done_ok;  // :185
-    {
-      const double alpha = beta / sAs;
-      // ------------------------------------------------------------ sweep B
-      double acc_r = 0.0;
-      const bool ok = nh_sweep<true>(
-          P, cur, bq, smem, pp,
-          [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double rc, double pc) {
-            const double r = __dsub_rn(rc, __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
-            const double d = __dmul_rn(alpha, sc);                // p_non_hydro + alpha*p (:187)
-            ptrdiff_t ox, oy;
-            nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
-            pnh[q] = __dadd_rn(pc, d);
-            nh_add_halo<CX, CY>(pnh, q, ox, oy, d);
-            nh_put<CX, CY>(res, q, ox, oy, r);
-            if (f & kNHMaskT) acc_r += r * r;
-          });
-      if (!ok) return;
-      double v[1] = {acc_r}, out[1];
-      block_reduce<1, -1, kNHThreads>(v, out);
-      if (threadIdx.x == 0) P.slots[(size_t)((epoch & 1) * nb + blockIdx.x) * 4] = out[0];
-      const unsigned long long ep_b = epoch;
-      if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
-      double r1[1];
-      grid_collect<1, -1, kNHThreads>(P.slots + (size_t)((ep_b & 1) * nb) * 4, 4, nb, r1);
-      const double rsnew = r1[0];
-      bq = rsnew / beta;  // p = res + rsnew/rsold*p (:189)
-      beta = rsnew;
-      if (n == 1) {  // divergence test (:197-205)
-        betamin = fabs(rsnew);
-      } else if (n > 2) {
-        betamin = fmin(betamin, fabs(rsnew));
-        if (fabs(rsnew) > 100.0 * betamin) {
-          status = PYOMGPU_DIVERGED;
-          goto done_err;
-        }
-      }
-      alpha_prev = alpha;
-      rr_prev = rsnew;
-    }
+    double r2[2];
+    grid_collect<2, 1, kNHThreads>(P.slots + (size_t)((ep_a & 1) * nb) * 4, 4, nb, r2);
+    double alpha = 0.0;
+    how = ctl.after_a(r2[0], r2[1], alpha);
+    if (how != NHCtl::kGo) break;
+    // -------------------------------------------------------------- sweep B
+    double acc_r = 0.0;
+    const bool ok = nh_sweep<true>(
+        P, cur, ctl.bq, smem, pp,
+        [&](int i, int j, int, uint32_t f, size_t q, double a, double sc, double rc, double pc) {
+          const double r = __dsub_rn(rc, __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
+          const double d = __dmul_rn(alpha, sc);                // p_non_hydro + alpha*p (:187)
+          ptrdiff_t ox, oy;
+          nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
+          pnh[q] = __dadd_rn(pc, d);
+          nh_add_halo<CX, CY>(pnh, q, ox, oy, d);
+          nh_put<CX, CY>(res, q, ox, oy, r);
+          if (f & kNHMaskT) acc_r += r * r;
+        });
+    if (!ok) return;
+    double v[1] = {acc_r}, out[1];
+    block_reduce<1, -1, kNHThreads>(v, out);
+    if (threadIdx.x == 0) P.slots[(size_t)((epoch & 1) * nb + blockIdx.x) * 4] = out[0];
+    const unsigned long long ep_b = epoch;
+    if (!grid_sync(P.ctl, nb, epoch, P.timeout_ns)) return;
+    double r1[1];
+    grid_collect<1, -1, kNHThreads>(P.slots + (size_t)((ep_b & 1) * nb) * 4, 4, nb, r1);
+    how = ctl.after_b(r1[0], alpha);
   }
+  ctl.finish(how, P.out);
+}
 
-done_ok:
-  converged = 1;
-  status = PYOMGPU_OK;
-  goto done;
-done_err:
-  converged = 0;
-  if (est != est) status = PYOMGPU_NAN;
-done:
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    P.out->iterations = n;
-    P.out->converged = converged;
-    P.out->status = status;
-    P.out->est = est;
+// Block-wide reduction whose result every thread receives.
+template <int NV, int kMaxSlot, int kThreads>
+__device__ __forceinline__ void block_allreduce(const double (&v)[NV], double (&out)[NV]) {
+  __shared__ double sh[NV];
+  double r[NV];
+  block_reduce<NV, kMaxSlot, kThreads>(v, r);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NV; k++) sh[k] = r[k];
+  __syncthreads();
+  for (int k = 0; k < NV; k++) out[k] = sh[k];
+  __syncthreads();
+}
+
+// Block reduction for kThreads <= 1024: warp shuffles, then warp 0 over the
+// warp results; thread 0 gets the result.  Fixed order.
+template <int NV, int kMaxSlot, int kThreads>
+__device__ __forceinline__ void block_reduce_fast(const double (&v)[NV], double (&out)[NV]) {
+  __shared__ double sh[kThreads / 32][NV];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    const double r = (k == kMaxSlot) ? warp_max(v[k]) : warp_sum(v[k]);
+    if (lane == 0) sh[w][k] = r;
   }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double r = lane < kThreads / 32 ? sh[lane][k] : 0.0;
+      r = (k == kMaxSlot) ? warp_max(r) : warp_sum(r);
+      out[k] = r;
+    }
+  }
+  __syncthreads();
+}
+
+// Small grids: the whole solve in one thread-block cluster of C <= 16 blocks
+// (one per SM).  The interior cells, in compact (i, j, k) order, are split
+// into C contiguous chunks; each block keeps res, the direction (two buffers:
+// the previous and the one being formed), p_non_hydro and the flags of its
+// chunk in shared memory (33 bytes per cell; p is written back at the end,
+// the cyclic halo copies of p are summed in global memory as the reference
+// sums them) and reads a neighbour in another chunk from the
+// owner's shared memory (distributed shared memory).  Sweep A forms the new
+// direction res + bq s_old itself wherever it reads it, local or remote, so
+// no barrier is needed before its stencil.  A neighbour across a cyclic
+// boundary wraps; one across a closed boundary reads 0, as the reference's
+// zero halo of p does.  Two cluster
+// barriers per iteration carry the reductions; each block's warp 0 combines
+// the C block partials in the same order.  Same control flow and per-cell
+// arithmetic as nh_cg_kernel.
+template <bool CX, bool CY>
+__global__ void __launch_bounds__(kNHSmallThreads, 1) nh_cg_small_kernel(const __grid_constant__ NHParams P) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double part[4], total[4];
+  __shared__ const double* rankR[kNHMaxCluster];
+  __shared__ double* rankS[2][kNHMaxCluster];
+  cg::cluster_group cluster = cg::this_cluster();
+  const NHGeo G = P.G;
+  const NHOp op = P.op;
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.nz;
+  const int nxy = nx * ny, N = nxy * nz;
+  const int C = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+  const int chunk = P.small_chunk;
+  const int c0 = rank * chunk, c1 = min(N, c0 + chunk);
+  double* R = reinterpret_cast<double*>(smem);
+  double* S0 = R + chunk;
+  double* S1 = S0 + chunk;
+  double* Pl = S1 + chunk;  // p_non_hydro of the chunk
+  uint8_t* F = reinterpret_cast<uint8_t*>(Pl + chunk);
+  double* __restrict__ pnh = P.p;
+  if (threadIdx.x < C) {
+    rankR[threadIdx.x] = cluster.map_shared_rank(R, (int)threadIdx.x);
+    rankS[0][threadIdx.x] = cluster.map_shared_rank(S0, (int)threadIdx.x);
+    rankS[1][threadIdx.x] = cluster.map_shared_rank(S1, (int)threadIdx.x);
+  }
+  auto decode = [&](int c, int& i, int& j, int& k) {
+    i = c % nx + 1;
+    const int r = c / nx;
+    j = r % ny + 1;
+    k = r / ny + 1;
+  };
+  // compact neighbour of cell c (i, j) in direction (di, dj, dk); -1 across a closed boundary
+  auto nbi = [&](int c, int i, int j, int di, int dj, int dk) -> int {
+    if (di == 1) return i < nx ? c + 1 : (CX ? c - (nx - 1) : -1);
+    if (di == -1) return i > 1 ? c - 1 : (CX ? c + (nx - 1) : -1);
+    if (dj == 1) return j < ny ? c + nx : (CY ? c - nx * (ny - 1) : -1);
+    if (dj == -1) return j > 1 ? c - nx : (CY ? c + nx * (ny - 1) : -1);
+    return c + dk * nxy;  // only read where the vertical face is open, so inside
+  };
+  // Block partials (thread 0 wrote part[0..nv)) summed over the cluster, max
+  // for slot max_slot; warp 0 of every block combines them in rank order.
+  auto cluster_total = [&](int nv, int max_slot, double* out) {
+    cluster.sync();
+    if (threadIdx.x < 32) {
+      for (int q = 0; q < nv; q++) {
+        double v = 0.0;
+        if ((int)threadIdx.x < C) v = cluster.map_shared_rank(part, (int)threadIdx.x)[q];
+        v = (q == max_slot) ? warp_max(v) : warp_sum(v);
+        if (threadIdx.x == 0) total[q] = v;
+      }
+    }
+    __syncthreads();
+    for (int q = 0; q < nv; q++) out[q] = total[q];
+  };
+  // ------------------------------------------------------------------ init
+  double red[2];
+  {
+    double v[2] = {0.0, 0.0};
+    for (int c = c0 + (int)threadIdx.x; c < c1; c += kNHSmallThreads) {
+      int i, j, k;
+      decode(c, i, j, k);
+      const size_t q = G.at(i, j, k);
+      const uint32_t f = __ldg(op.flags + op.fidx(ny, i, j, k));
+      const double a = nh_apply(op, G, i, j, k, f,
+                                [&](int di, int dj, int dk) { return pnh[q + nh_off(G, di, dj, dk)]; });
+      const double fo = P.forc[fidx3(nx, ny, i, j, k)];
+      const double r = __dsub_rn(fo, a);
+      R[c - c0] = r;
+      S0[c - c0] = 0.0;
+      S1[c - c0] = 0.0;
+      Pl[c - c0] = pnh[q];
+      F[c - c0] = (uint8_t)f;
+      if (f & kNHMaskT) {
+        v[0] += r * r;
+        v[1] += fo * fo;
+      }
+    }
+    double out[2];
+    block_reduce_fast<2, -1, kNHSmallThreads>(v, out);
+    if (threadIdx.x == 0) {
+      part[0] = out[0];
+      part[1] = out[1];
+    }
+    cluster_total(2, -1, red);
+  }
+  NHCtl ctl;
+  int how = ctl.start(red[0], red[1], P);
+  while (how == NHCtl::kGo) {
+    const int nw = ctl.n & 1;  // buffer the new direction goes to
+    double* const* Sold = rankS[nw ^ 1];
+    double* Snew = nw ? S1 : S0;
+    const double bq = ctl.bq;
+    const double* Sold_local = nw ? S0 : S1;
+    // s_n at compact cell n: res + rsnew/rsold * p (:189), separately rounded, from its owner's res and
+    // s_old (plain shared-memory loads inside the chunk)
+    auto sform = [&](int n) -> double {
+      if (n >= c0 && n < c1) return __dadd_rn(R[n - c0], __dmul_rn(bq, Sold_local[n - c0]));
+      const int o = n / chunk, l = n - o * chunk;
+      return __dadd_rn(rankR[o][l], __dmul_rn(bq, Sold[o][l]));
+    };
+    // ------------------------------------------------------------ sweep A
+    double acc[2] = {0.0, 0.0};
+    for (int c = c0 + (int)threadIdx.x; c < c1; c += kNHSmallThreads) {
+      const uint32_t f = F[c - c0];
+      const double sc = __dadd_rn(R[c - c0], __dmul_rn(bq, (nw ? S0 : S1)[c - c0]));
+      Snew[c - c0] = sc;
+      if (!(f & kNHMaskT)) continue;
+      int i, j, k;
+      decode(c, i, j, k);
+      const double a = nh_apply(op, G, i, j, k, f, [&](int di, int dj, int dk) {
+        if (di == 0 && dj == 0 && dk == 0) return sc;
+        const int n = nbi(c, i, j, di, dj, dk);
+        return n < 0 ? 0.0 : sform(n);
+      });
+      acc[0] += sc * a;
+      acc[1] = fmax(acc[1], fabs(sc));
+    }
+    double out2[2], rA[2];
+    block_reduce_fast<2, 1, kNHSmallThreads>(acc, out2);
+    if (threadIdx.x == 0) {
+      part[0] = out2[0];
+      part[1] = out2[1];
+    }
+    cluster_total(2, 1, rA);  // also: every block's new direction is complete
+    double alpha = 0.0;
+    how = ctl.after_a(rA[0], rA[1], alpha);
+    if (how != NHCtl::kGo) break;
+    // ------------------------------------------------------------ sweep B
+    double* const* Sn = rankS[nw];
+    double accr[1] = {0.0};
+    for (int c = c0 + (int)threadIdx.x; c < c1; c += kNHSmallThreads) {
+      const uint32_t f = F[c - c0];
+      int i, j, k;
+      decode(c, i, j, k);
+      const double a = nh_apply(op, G, i, j, k, f, [&](int di, int dj, int dk) {
+        const int n = (di == 0 && dj == 0 && dk == 0) ? c : nbi(c, i, j, di, dj, dk);
+        if (n < 0) return 0.0;
+        if (n >= c0 && n < c1) return (double)Snew[n - c0];
+        const int o = n / chunk;
+        return Sn[o][n - o * chunk];
+      });
+      const double sc = Snew[c - c0];
+      const double r = __dsub_rn(R[c - c0], __dmul_rn(alpha, a));  // res = res - alpha*Ap (:188)
+      const double d = __dmul_rn(alpha, sc);                        // p_non_hydro + alpha*p (:187)
+      Pl[c - c0] = __dadd_rn(Pl[c - c0], d);
+      if (CX || CY) {  // the halo copies keep their own sums in global memory (few cells)
+        ptrdiff_t ox, oy;
+        nh_copy_offsets<CX, CY>(G.g, i, j, ox, oy);
+        if (ox || oy) nh_add_halo<CX, CY>(pnh, G.at(i, j, k), ox, oy, d);
+      }
+      R[c - c0] = r;
+      if (f & kNHMaskT) accr[0] += r * r;
+    }
+    double out1[1], rB[1];
+    block_reduce_fast<1, -1, kNHSmallThreads>(accr, out1);
+    if (threadIdx.x == 0) part[0] = out1[0];
+    cluster_total(1, -1, rB);  // also: no block changes res while a neighbour still forms directions from it
+    how = ctl.after_b(rB[0], alpha);
+  }
+  ctl.finish(how, P.out);
+  for (int c = c0 + (int)threadIdx.x; c < c1; c += kNHSmallThreads) {
+    int i, j, k;
+    decode(c, i, j, k);
+    pnh[G.at(i, j, k)] = Pl[c - c0];
+  }
+  cluster.sync();  // no block leaves while another may still read its shared memory
+}
+
+const void* nh_cg_small_kernel_ptr(bool cx, bool cy) {
+  if (cx) return cy ? (const void*)nh_cg_small_kernel<true, true> : (const void*)nh_cg_small_kernel<true, false>;
+  return cy ? (const void*)nh_cg_small_kernel<false, true> : (const void*)nh_cg_small_kernel<false, false>;
 }
 
 const void* nh_cg_kernel_ptr(bool cx, bool cy) {
@@ -619,6 +869,7 @@ struct pyomgpu_nh {
   int grid = 0;        // 0: automatic
   int ty = 0, kc = 0;  // brick shape (0: automatic)
   int ns = 0;          // pipeline stages (0: automatic)
+  int variant = 0;     // 0 automatic, 1 brick kernel, 2 single-block kernel
   double timeout_s = 2.0;
   unsigned stall_next = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -812,6 +1063,12 @@ int32_t pyomgpu_nh_create(const pyomgpu_grid3d* gr, pyomgpu_nh** out) {
     attr_ok = attr_ok && cudaFuncSetAttribute(nh_cg_kernel_ptr(v & 1, v >> 1),
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kNHSmemMax) == cudaSuccess;
+  for (int v = 0; v < 4; v++)
+    attr_ok = attr_ok &&
+              cudaFuncSetAttribute(nh_cg_small_kernel_ptr(v & 1, v >> 1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kNHSmallSmemMax) == cudaSuccess &&
+              cudaFuncSetAttribute(nh_cg_small_kernel_ptr(v & 1, v >> 1),
+                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
   if (!attr_ok) {
     cudaGetLastError();
     delete h;
@@ -872,6 +1129,14 @@ int32_t pyomgpu_nh_set_stages(pyomgpu_nh* h, int32_t stages) {
   return PYOMGPU_OK;
 }
 
+int32_t pyomgpu_nh_set_variant(pyomgpu_nh* h, int32_t variant) {
+  if (!h || variant < 0 || variant > 2) return nfail(PYOMGPU_EINVAL, "nh_set_variant: 0, 1 or 2");
+  if (variant == 2 && (size_t)h->G.g.nx * h->G.g.ny * h->G.nz > (size_t)kNHSmallMaxCells)
+    return nfail(PYOMGPU_EINVAL, "nh_set_variant: the cluster kernel holds at most %d cells", kNHSmallMaxCells);
+  h->variant = variant;
+  return PYOMGPU_OK;
+}
+
 int32_t pyomgpu_apply_op_3d(pyomgpu_nh* h, const double* p1, double* res, pyomgpu_stream stream) {
   if (!h || !p1 || !res) return nfail(PYOMGPU_EINVAL, "apply_op_3d: null argument");
   cudaStream_t st = (cudaStream_t)stream;
@@ -893,6 +1158,8 @@ int32_t pyomgpu_apply_op_3d(pyomgpu_nh* h, const double* p1, double* res, pyomgp
 }  // extern "C"
 
 namespace {
+
+int nh_finish_cg(pyomgpu_nh* h, double* pdev, pyomgpu_solve_info* info, cudaStream_t st);
 
 // congrad_non_hydro on device arrays: fdev (forcing) and pdev (p_non_hydro(:,:,:,taup1), in/out), both
 // Fortran layout.  pdev may be a staging buffer whose result the caller copies out.
@@ -919,6 +1186,43 @@ int nh_run_cg(pyomgpu_nh* h, const double* fdev, double* pdev, double eps, int m
   P.stall_extra = h->stall_next;
   h->stall_next = 0;
   P.out = h->d_result;
+  const size_t ncell = (size_t)h->G.g.nx * h->G.g.ny * h->G.nz;
+  const bool small = h->variant == 2 || (h->variant == 0 && ncell <= (size_t)kNHClusterAuto);
+  if (small) {
+    // cluster of C = 1, 2, 4, 8 or 16 blocks with about one cell per thread, each chunk within shared memory
+    int C = 1;
+    while (C < kNHMaxCluster && ((size_t)C * kNHSmallThreads < ncell || (ncell + C - 1) / C > (size_t)kNHSmallMaxChunk))
+      C *= 2;
+    const int chunk = (int)((ncell + C - 1) / C);
+    P.small_chunk = chunk;
+    const void* kfs = nh_cg_small_kernel_ptr(h->cyclic_x != 0, h->cyclic_y != 0);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(kNHSmallThreads);
+    cfg.dynamicSmemBytes = nh_small_smem_bytes(chunk);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kfs, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      nclusters = 0;
+    }
+    if (nclusters >= 1) {
+      void* sargs[] = {&P};
+      NCK(cudaEventRecord(h->e0, st));
+      NCK(cudaLaunchKernelExC(&cfg, kfs, sargs));
+      NCK(cudaEventRecord(h->e1, st));
+      return nh_finish_cg(h, pdev, info, st);
+    }
+    if (h->variant == 2) return nfail(PYOMGPU_ECUDA, "congrad_non_hydro: a cluster of %d blocks cannot be placed", C);
+    // automatic choice: the brick kernel below
+  }
   // brick shape: 32 x ty x kc, ty the largest power of two <= min(8, ny), kc = (8/ty) kw with kw the
   // largest level count per warp whose pipeline stages leave room for two blocks per SM
   int ty = h->ty, kc = h->kc, ns = h->ns > 0 ? h->ns : 2;
@@ -968,6 +1272,11 @@ int nh_run_cg(pyomgpu_nh* h, const double* fdev, double* pdev, double eps, int m
   NCK(cudaEventRecord(h->e0, st));
   NCK(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kNHThreads), args, smem, st));
   NCK(cudaEventRecord(h->e1, st));
+  return nh_finish_cg(h, pdev, info, st);
+}
+
+// Result of a CG launch: status, iterations, device time; p unpacked to pdev.
+int nh_finish_cg(pyomgpu_nh* h, double* pdev, pyomgpu_solve_info* info, cudaStream_t st) {
   NCK(cudaMemcpyAsync(h->h_result, h->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
   NCK(cudaMemcpyAsync(h->h_err, &h->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
   launch_nh_unpack(h->G, h->p, pdev, st);

@@ -149,6 +149,7 @@ struct alignas(64) NHParams {
   NHOp op;
   int ty, kw, kc;                    // brick shape
   int ns;                            // pipeline stages
+  int small_chunk;                   // cluster variant: cells per block
   int nbx, nby, nbz;                 // bricks per dimension
   const double* forc;  // Fortran layout (nx+4, ny+4, nz), device
   double* p;           // padded p_non_hydro(:,:,:,taup1), in/out
@@ -183,6 +184,17 @@ void launch_nh_step_pre(const NHStep& S, cudaStream_t st);
 void launch_nh_step_post(const NHStep& S, cudaStream_t st);
 
 const void* nh_cg_kernel_ptr(bool cyclic_x, bool cyclic_y);
+
+// cluster variant for small grids: res, direction and flags distributed over
+// the shared memory of up to kNHMaxCluster blocks
+constexpr int kNHSmallThreads = 1024;
+constexpr int kNHMaxCluster = 16;
+constexpr size_t nh_small_smem_bytes(size_t chunk) { return (chunk * 33 + 15) / 16 * 16; }
+constexpr size_t kNHSmallSmemMax = 223 * 1024;  // 227 KB per block less room for the static buffers
+constexpr int kNHSmallMaxChunk = (int)(kNHSmallSmemMax / 33);
+constexpr int kNHSmallMaxCells = kNHMaxCluster * kNHSmallMaxChunk;
+constexpr int kNHClusterAuto = 32768;  // automatic choice: the cluster kernel up to this many cells
+const void* nh_cg_small_kernel_ptr(bool cyclic_x, bool cyclic_y);
 void launch_nh_apply(const NHGeo& G, const NHOp& op, const double* p, double* res, cudaStream_t st);
 void launch_nh_pack(const NHGeo& G, const double* user, double* padded, cudaStream_t st);
 void launch_nh_unpack(const NHGeo& G, const double* padded, double* user, cudaStream_t st);

@@ -85,6 +85,11 @@ class NonHydrostatic:
         """TMA pipeline depth of the CG sweeps (2..4; 0 = automatic)."""
         _abi.check(self._L.pyomgpu_nh_set_stages(self._h, int(stages)))
 
+    def set_variant(self, variant: int):
+        """CG kernel: 1 grid-wide bricks, 2 one block resident in shared memory
+        (small grids), 0 automatic."""
+        _abi.check(self._L.pyomgpu_nh_set_variant(self._h, int(variant)))
+
     def apply_op_3d(self, p):
         """non_hydrostatic.f90:247-276: ``res = A p`` over the interior, zero halo."""
         res = np.zeros(self.shape, order="F") if not _is_torch(p) else _torch_like(p)

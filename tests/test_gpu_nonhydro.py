@@ -167,3 +167,31 @@ def test_solve_non_hydrostatic_step_matches_oracle(oracle_lib, cyclic_x, itt):
         assert np.abs(a - b).max() <= 1e-7 * np.abs(b).max(), n
     # fields the step does not touch are untouched
     assert np.array_equal(M.u[..., M.tau - 1], Mo.u[..., Mo.tau - 1])
+
+
+@pytest.mark.parametrize("name,kw", [CASES[1], CASES[3]])
+def test_single_block_kernel_matches_oracle_and_bricks(oracle_lib, name, kw):
+    """Small grids run in one block with the fields in shared memory; the
+    result follows the oracle as the brick kernel's does."""
+    W = world(kw)
+    O = oracle_lib.Oracle3D(W.M)
+    cf = O.make_coeff()
+    nh = NonHydrostatic(W.M)
+    out = {}
+    for variant in (1, 2):
+        nh.set_variant(variant)
+        p = W.p0.copy(order="F")
+        it, info = nh.congrad_non_hydro(W.forc, p, eps=1e-9, max_it=5000)
+        io = O.congrad(cf, W.forc, W.p0.copy(order="F"), eps=1e-9, max_it=5000)
+        assert info["status"] == 0 and abs(it - io["iterations"]) <= 1, (variant, it, io)
+        ps = W.p0.copy(order="F")
+        O.congrad(cf, W.forc, ps, eps=0.0, max_it=it)
+        assert rel_max(p, ps, np.ones(p.shape, bool)) < 1e-7, variant
+        out[variant] = (it, p)
+    # max-iteration semantics on the single-block kernel too
+    p = W.p0.copy(order="F")
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        it, info = nh.congrad_non_hydro(W.forc, p, eps=1e-30, max_it=9)
+    assert info["status"] == _abi.MAXITER and it == 10
+    nh.close()
