@@ -384,6 +384,7 @@ def main():
     ap.add_argument("--with-c2", action="store_true",
                     help="also time config 2 (64 basins in one work-queue launch vs 64 sequential solves)")
     ap.add_argument("--c2-count", type=int, default=64, help="basins of config 2 (fewer for profiling)")
+    ap.add_argument("--c2-only", action="store_true", help="time only config 2 and print its object (profiling runs)")
     ap.add_argument("--with-c3", action="store_true",
                     help="also time config 3 (learned FCG vs Jacobi-PCG on the 2048x1024 grid)")
     ap.add_argument("--with-c4", action="store_true",
@@ -414,6 +415,11 @@ def main():
     from pyom2_b200.external import ExternalMode, _ptr
 
     nh_grid = tuple(int(v) for v in args.nh_grid.split("x"))
+    if args.c2_only:
+        r = c2_batch(max(1, args.steps), 1, args.c2_count)
+        if rank == 0:
+            print(json.dumps({"c2_batch": r}), flush=True)
+        return
     if args.nh_only:
         r = nh_bench(args.steps, args.warmup, peaks()[0], nh_grid, max_it=args.nh_max_it,
                      cpu=not args.no_cpu_baseline)
