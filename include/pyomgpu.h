@@ -150,6 +150,21 @@ int32_t pyomgpu_set_sync_timeout(pyomgpu_ctx* ctx, double seconds);
  * context stays usable).  Cleared after that launch. */
 int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* ctx, int32_t enable);
 
+/* CG kernel of the streamfunction solves (congrad_streamfunction,
+ * solve_streamfunction, solve_rtol F64, the learned solver's fallback):
+ * 1 = the tiled kernel (any grid; the one pyomgpu_autotune tunes),
+ * 2 = the on-chip-resident kernel (one piece of the grid per SM, with the
+ *     direction and face couplings in shared memory and the residual,
+ *     solution and preconditioner in tensor memory for the whole solve;
+ *     grids whose largest piece fits, about 1.04 M points on 148 SMs),
+ * 0 = automatic (2 wherever the grid fits).  PYOMGPU_EINVAL for 2 on a grid
+ * that does not fit.  The surface-pressure solve always uses 1.  Reduction
+ * order differs between the kernels: results change at rounding level. */
+int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* ctx, int32_t kernel);
+/* Piece layout the resident kernel uses on this grid: pieces in x and y and
+ * points per thread; PYOMGPU_EINVAL when the grid does not fit. */
+int32_t pyomgpu_resident_layout(pyomgpu_ctx* ctx, int32_t* npx, int32_t* npy, int32_t* points_per_thread);
+
 /* Autotuner of the solve kernel: times `iterations` iterations of the
  * Jacobi-PCG kernel on this grid (a fixed pseudo-random right-hand side) for
  * every tile shape tx x ty in {32,64,96,128} x {8,16,24,32} and every

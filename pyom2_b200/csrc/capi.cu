@@ -92,10 +92,143 @@ int stage_in(pyomgpu_ctx* c, const double* user, double* stage, const double** o
   return 0;
 }
 
+// Waits for a CG launch bracketed by c->e0/e1 and fills info from its result.
+int finish_cg(pyomgpu_ctx* c, pyomgpu_solve_info* info, cudaStream_t st) {
+  CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
+  int err = 0;
+  CK(cudaMemcpyAsync(c->h_scal, &c->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::memcpy(&err, c->h_scal, sizeof(int));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->e0, c->e1));
+  if (info) {
+    info->iterations = c->h_result->iterations;
+    info->converged = c->h_result->converged;
+    info->status = c->h_result->status;
+    info->outer_iterations = 1;
+    info->estimated_error = c->h_result->est;
+    info->rel_residual = -1.0;
+    info->device_ms = ms;
+    info->kernel_launches = 1;
+    if (err) {
+      info->status = PYOMGPU_TIMEOUT;
+      info->converged = 0;
+    }
+  }
+  if (err) return fail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded %.3f s", c->timeout_s);
+  return c->h_result->status;
+}
+
+// Piece layout of the resident kernel for this grid, planned once: among the
+// npx x npy cuts (at most one piece per SM, pieces at least 2 x 2) whose
+// largest piece fits in shared memory and in the worker threads, the one with
+// the smallest estimated iteration time (shared-memory traffic of the largest
+// piece, ~0.27 ns per point, plus ~5 ns of reduction per block).  Allocates
+// the exchange buffers.  Returns PYOMGPU_OK with c->resd.ok telling whether
+// the grid fits, or an error code.
+int res_plan(pyomgpu_ctx* c) {
+  auto& R = c->resd;
+  if (R.planned) return PYOMGPU_OK;
+  R.planned = true;
+  R.ok = false;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess)
+    return fail(PYOMGPU_ECUDA, "device attribute query failed");
+  size_t stat = 0;
+  for (int k = 0; k < kResNP; k++) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, cg_res_kernel_ptr(kResP[k])) != cudaSuccess)
+      return fail(PYOMGPU_ECUDA, "resident kernel attributes");
+    stat = std::max(stat, fa.sharedSizeBytes);
+  }
+  if ((size_t)optin <= stat) return PYOMGPU_OK;
+  const size_t cap = (size_t)optin - stat;
+  const int maxb = std::min(c->nsm, kResMaxSlots - 1);
+  double best = 1e300;
+  for (int npx = 1; npx <= std::min(c->nx / 2, maxb); npx++)
+    for (int npy = 1; npy <= c->ny / 2 && npx * npy <= maxb; npy++) {
+      const int w = (c->nx + npx - 1) / npx, h = (c->ny + npy - 1) / npy;
+      if (res_smem_bytes(w, h) > cap || w + h > kResWorkers) continue;
+      int pp = 0;
+      for (int k = 0; k < kResNP && !pp; k++)
+        if (res_threads(w, h, kResP[k]) <= kResWorkers) pp = kResP[k];
+      if (!pp) continue;
+      const double cost = 0.27 * w * h + 5.0 * npx * npy;
+      if (cost < best) {
+        best = cost;
+        R.npx = npx;
+        R.npy = npy;
+        R.wmax = w;
+        R.hmax = h;
+        R.p = pp;
+        R.smem = res_smem_bytes(w, h);
+      }
+    }
+  if (best == 1e300) return PYOMGPU_OK;
+  for (int k = 0; k < kResNP; k++)
+    if (cudaFuncSetAttribute(cg_res_kernel_ptr(kResP[k]), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) !=
+        cudaSuccess)
+      return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the resident kernel");
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_res_kernel_ptr(R.p), kResThreads, R.smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return PYOMGPU_OK;
+  const int nb = R.npx * R.npy;
+  if (int rc = dalloc(&R.hx, 2 * c->g.size())) return rc;
+  if (int rc = dalloc(&R.slots, (size_t)3 * (nb + 1) * 4)) return rc;
+  R.ok = true;
+  return PYOMGPU_OK;
+}
+
+bool use_resident(pyomgpu_ctx* c) {
+  if (c->cg_kernel == 1) return false;
+  return res_plan(c) == PYOMGPU_OK && c->resd.ok;
+}
+
+// The streamfunction solve in the on-chip-resident kernel (cg_res.cu).
+int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, double rtol, pyomgpu_solve_info* info,
+               cudaStream_t st) {
+  auto& R = c->resd;
+  const size_t bytes = c->g.size() * sizeof(double);
+  const int nb = R.npx * R.npy;
+  CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
+  CK(cudaMemsetAsync(c->res, 0, bytes, st));
+  CK(cudaMemsetAsync(R.slots, 0xFF, (size_t)3 * (nb + 1) * 4 * sizeof(double), st));
+  CGResParams P{};
+  P.g = c->g;
+  P.op = c->sf.dev();
+  P.forc = forc_dev;
+  P.sol = c->sol;
+  P.res = c->res;
+  P.hx = R.hx;
+  P.hsize = (long long)c->g.size();
+  P.slots = R.slots;
+  P.nslot = nb + 1;
+  P.npx = R.npx;
+  P.npy = R.npy;
+  P.wmax = R.wmax;
+  P.hmax = R.hmax;
+  P.eps = eps;
+  P.rtol = rtol;
+  P.max_it = max_it;
+  P.ctl = c->ctl;
+  P.timeout_ns = (unsigned long long)(c->timeout_s * 1e9);
+  P.stall_extra = c->stall_next;
+  c->stall_next = 0;
+  P.out = c->d_result;
+  void* args[] = {&P};
+  CK(cudaEventRecord(c->e0, st));
+  CK(cudaLaunchCooperativeKernel(cg_res_kernel_ptr(R.p), dim3(nb), dim3(kResThreads), args, R.smem, st));
+  CK(cudaEventRecord(c->e1, st));
+  return finish_cg(c, info, st);
+}
+
 // Runs the persistent CG kernel on c->sol (padded, already packed) with the
 // Fortran-layout device forcing.  Fills info (iterations, status, timing).
 int run_cg_ref(pyomgpu_ctx* c, bool surf_press, const double* forc_dev, double eps, int max_it, double rtol,
                pyomgpu_solve_info* info, cudaStream_t st) {
+  if (!surf_press && use_resident(c)) return run_cg_res(c, forc_dev, eps, max_it, rtol, info, st);
   const OpBuf& op = surf_press ? c->sp : c->sf;
   const size_t bytes = c->g.size() * sizeof(double);
   CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
@@ -136,29 +269,7 @@ int run_cg_ref(pyomgpu_ctx* c, bool surf_press, const double* forc_dev, double e
   CK(cudaLaunchCooperativeKernel(cg_ref_kernel_ptr(surf_press), dim3(grid), dim3(kCGThreads), args,
                                  cg_smem_bytes(tx, ty), st));
   CK(cudaEventRecord(c->e1, st));
-  CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
-  int err = 0;
-  CK(cudaMemcpyAsync(c->h_scal, &c->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  std::memcpy(&err, c->h_scal, sizeof(int));
-  float ms = 0.f;
-  CK(cudaEventElapsedTime(&ms, c->e0, c->e1));
-  if (info) {
-    info->iterations = c->h_result->iterations;
-    info->converged = c->h_result->converged;
-    info->status = c->h_result->status;
-    info->outer_iterations = 1;
-    info->estimated_error = c->h_result->est;
-    info->rel_residual = -1.0;
-    info->device_ms = ms;
-    info->kernel_launches = 1;
-    if (err) {
-      info->status = PYOMGPU_TIMEOUT;
-      info->converged = 0;
-    }
-  }
-  if (err) return fail(PYOMGPU_TIMEOUT, "grid barrier wait exceeded %.3f s", c->timeout_s);
-  return c->h_result->status;
+  return finish_cg(c, info, st);
 }
 
 }  // namespace
@@ -791,6 +902,26 @@ int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* c, int32_t enable) {
   return PYOMGPU_OK;
 }
 
+int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* c, int32_t kernel) {
+  if (!c || kernel < 0 || kernel > 2) return fail(PYOMGPU_EINVAL, "set_cg_kernel: bad arguments");
+  if (kernel == 2) {
+    if (int rc = res_plan(c)) return rc;
+    if (!c->resd.ok) return fail(PYOMGPU_EINVAL, "the grid does not fit the resident kernel");
+  }
+  c->cg_kernel = kernel;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_resident_layout(pyomgpu_ctx* c, int32_t* npx, int32_t* npy, int32_t* points_per_thread) {
+  if (!c) return fail(PYOMGPU_EINVAL, "null context");
+  if (int rc = res_plan(c)) return rc;
+  if (!c->resd.ok) return fail(PYOMGPU_EINVAL, "the grid does not fit the resident kernel");
+  if (npx) *npx = c->resd.npx;
+  if (npy) *npy = c->resd.npy;
+  if (points_per_thread) *points_per_thread = c->resd.p;
+  return PYOMGPU_OK;
+}
+
 int32_t pyomgpu_autotune(pyomgpu_ctx* c, int32_t iterations, int32_t* tile_x, int32_t* tile_y, int32_t* grid,
                          double* us_per_iteration, pyomgpu_stream stream) {
   if (!c || iterations < 10) return fail(PYOMGPU_EINVAL, "autotune: bad arguments");
@@ -819,6 +950,8 @@ int32_t pyomgpu_autotune(pyomgpu_ctx* c, int32_t iterations, int32_t* tile_x, in
     }
   pyomgpu_ctx::Tune best{};
   best.us_per_it = 1e300;
+  const int kernel_choice = c->cg_kernel;
+  c->cg_kernel = 1;  // the tiled kernel is the one tuned
   for (int pass = 0; pass < 2; ++pass)  // every candidate twice, the faster run counts
     for (const Cand& k : cands) {
       c->tune = pyomgpu_ctx::Tune{true, k.tx, k.ty, k.grid, 0.0};
@@ -827,6 +960,7 @@ int32_t pyomgpu_autotune(pyomgpu_ctx* c, int32_t iterations, int32_t* tile_x, in
       int rc = run_cg_ref(c, false, c->stage_a, 0.0, iterations, 0.0, &info, st);
       if (rc < 0 || rc == PYOMGPU_TIMEOUT) {
         c->tune = pyomgpu_ctx::Tune{};
+        c->cg_kernel = kernel_choice;
         return rc;
       }
       if (info.iterations < 1) continue;
@@ -834,6 +968,7 @@ int32_t pyomgpu_autotune(pyomgpu_ctx* c, int32_t iterations, int32_t* tile_x, in
       if (us < best.us_per_it) best = pyomgpu_ctx::Tune{true, k.tx, k.ty, k.grid, us};
     }
   c->tune = best.done ? best : pyomgpu_ctx::Tune{};
+  c->cg_kernel = kernel_choice;
   if (tile_x) *tile_x = c->tune.done ? c->tune.tx : kTileX;
   if (tile_y) *tile_y = c->tune.done ? c->tune.ty : kTileY;
   if (grid) *grid = c->tune.grid;

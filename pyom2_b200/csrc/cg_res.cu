@@ -1,0 +1,688 @@
+// On-chip-resident Jacobi-PCG kernel for congrad_streamfunction
+// (solve_streamfct.f90:153-327): the control flow of cg_ref_kernel<false>,
+// laid out so that an iteration moves no field through HBM and only the
+// piece boundaries through L2.
+//
+// The grid is cut into npx x npy rectangular pieces, one per block and one
+// block per SM (512 threads, cooperative launch).  For the whole solve a block
+// keeps
+//   shared memory: the search direction with a one-cell halo and the x- and
+//                  y-face couplings FX, FY of its piece (~182 KB for a 39 x 180
+//                  piece, i.e. 1440 x 720 over 148 SMs);
+//   TMEM:          the residual, the solution and the preconditioner Z of the
+//                  points a thread owns (tcgen05.ld/st of whole 32-bit columns
+//                  of the thread's lane; no MMA), 96 of the 128 columns each
+//                  thread of a 512-thread block can reach;
+//   registers:     the direction and one more value per point: Z*res between
+//                  the residual update and the next direction, As between the
+//                  stencil and the residual update.
+// Warps 1-15 own the points: a thread owns a column segment of P points, so
+// the north and south neighbours of its stencil come from its own registers.
+// Warp 0 runs the reductions across blocks and the control flow, so the
+// registers of its exp/log arithmetic do not add to the workers' arrays.
+//
+// Reductions and halo exchange use no arrival counter:
+//   * each block writes its partial sums into its own slot (the last word with
+//     st.release); warp 0 of every block polls all slots (lane l: slots l,
+//     l+32, ...) until no word is empty any more, and the sums are formed in a
+//     fixed order, so all blocks obtain bit-identical scalars and take the
+//     same decisions.  Slots rotate over three buffers; a block empties its
+//     slot of epoch e+2 as soon as it completes epoch e, when every reader of
+//     the slot's previous contents has finished.
+//   * after the residual update a block writes (Z*res, s) of its boundary
+//     points into two padded exchange arrays (with the setcyclic_xy copies)
+//     before its slot is released, so once a block has acquired every slot
+//     of that reduction the values of its halo are visible: it loads them
+//     once (bypassing L1) and recomputes the neighbours' next direction on
+//     the halo with the operation their owner uses.  A value is overwritten
+//     only in the next sweep B, after the reader has published the next
+//     reduction, which it does after its loads have returned.  Nothing polls
+//     the exchange arrays (polling them from every thread swamped L2).
+// Every wait is bounded by %globaltimer; on time-out the kernel records
+// PYOMGPU_TIMEOUT in the control block, frees its TMEM and returns.
+#include <math.h>
+
+#include "cg_res.cuh"
+#include "tc.cuh"
+
+namespace pyomgpu {
+namespace {
+
+__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ double ld_acquire_f64(const double* p) {
+  double v;
+  asm volatile("ld.acquire.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+// Plain store, cached in L2 only (ordered before a later st.release of the
+// same thread, or of thread 0 after a block barrier).
+__device__ __forceinline__ void st_weak_f64(double* p, double v) { __stcg(p, v); }
+__device__ __forceinline__ void st_release_f64(double* p, double v) {
+  asm volatile("st.release.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ bool is_empty(double v) {
+  return (unsigned long long)__double_as_longlong(v) == kResEmpty;
+}
+__device__ __forceinline__ double empty_word() { return __longlong_as_double((long long)kResEmpty); }
+// A NaN that carries the empty pattern is sent as the canonical NaN.
+__device__ __forceinline__ double sendable(double v) {
+  return is_empty(v) ? __longlong_as_double(0x7fffffffffffffffll) : v;
+}
+
+// Writes v at interior (i,j) of an exchange array and at the halo positions
+// setcyclic_xy fills from it.
+__device__ __forceinline__ void publish_cyclic(double* a, const Geo& g, int i, int j, double v) {
+  st_weak_f64(a + g.at(i, j), v);
+  int xc, yc;
+  cyclic_copies(g, i, j, xc, yc);
+  if (xc != 0x7fffffff) st_weak_f64(a + g.at(xc, j), v);
+  if (yc != 0x7fffffff) {
+    st_weak_f64(a + g.at(i, yc), v);
+    if (xc != 0x7fffffff) st_weak_f64(a + g.at(xc, yc), v);
+  }
+}
+
+// An integer the compiler has to treat as produced here: index arithmetic
+// derived from it is redone in each sweep instead of being hoisted out of the
+// iteration loop and held in registers for the whole solve.
+__device__ __forceinline__ int opaque(int v) {
+  asm volatile("" : "+r"(v));
+  return v;
+}
+
+// --------------------------------------------------------------------- TMEM
+// 32x32b shape: thread t of warp w moves whole 32-bit columns of TMEM lane
+// 32*(w%4) + t; a double occupies two adjacent columns (low word first).
+__device__ __forceinline__ void tm_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void tm_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
+               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void tm_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void tm_st16(uint32_t taddr, const uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+// N = 8 or 16 columns
+template <int N>
+__device__ __forceinline__ void tm_ld(uint32_t taddr, uint32_t (&v)[N]) {
+  if constexpr (N == 8)
+    tm_ld8(taddr, v);
+  else
+    tm_ld16(taddr, v);
+}
+template <int N>
+__device__ __forceinline__ void tm_st(uint32_t taddr, const uint32_t (&v)[N]) {
+  if constexpr (N == 8)
+    tm_st8(taddr, v);
+  else
+    tm_st16(taddr, v);
+}
+__device__ __forceinline__ void tm_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ double col_get(const uint32_t* v, int k) {
+  return __hiloint2double((int)v[2 * k + 1], (int)v[2 * k]);
+}
+__device__ __forceinline__ void col_put(uint32_t* v, int k, double d) {
+  v[2 * k] = (uint32_t)__double2loint(d);
+  v[2 * k + 1] = (uint32_t)__double2hiint(d);
+}
+
+// ------------------------------------------------------------ control flow
+// Scalars of the solve in shared memory, advanced by thread 0 only (the
+// reference's congrad_streamfunction variables).
+struct ResCtl {
+  double beta, bb, rtol2bb, betam1, betamin, step1, est, bq, alpha;
+  int n, status, act, stop_after;
+};
+constexpr int kRun = 0, kDoneOk = 1, kDoneErr = 2;
+constexpr int kStepInit = 0, kStepA = 1, kStepB = 2;
+
+__device__ __forceinline__ void ctl_stop(ResCtl& C, int act, int status) {
+  C.act = act;
+  C.status = status;
+}
+
+// Start of iteration C.n: max_it, NaN and divergence tests, beta/betam1.
+__device__ void ctl_begin(ResCtl& C, const CGResParams& P) {
+  if (C.n > P.max_it) return ctl_stop(C, kDoneErr, PYOMGPU_MAXITER);  // solve_streamfct.f90:303-304
+  if (C.beta != C.beta) {  // early NaN stop (the reference runs on and halts at the end)
+    C.est = C.beta;
+    return ctl_stop(C, kDoneErr, PYOMGPU_NAN);
+  }
+  if (C.n == 1) {  // :232-240
+    C.betamin = fabs(C.beta);
+  } else if (C.n > 2) {
+    C.betamin = fmin(C.betamin, fabs(C.beta));
+    if (fabs(C.beta) > 100.0 * C.betamin) return ctl_stop(C, kDoneErr, PYOMGPU_DIVERGED);
+  }
+  C.bq = C.beta / C.betam1;  // :244
+}
+
+// v = (Z res, res), sum f^2 and sum res^2 over the unknowns, max|Z res|
+__device__ void ctl_init(ResCtl& C, const CGResParams& P, const double* v) {
+  C.beta = v[0];
+  C.bb = v[1];
+  C.rtol2bb = P.rtol * P.rtol * C.bb;
+  C.betam1 = 1.0;
+  C.betamin = C.step1 = C.est = C.bq = C.alpha = 0.0;
+  C.n = 0;
+  C.status = PYOMGPU_OK;
+  C.act = kRun;
+  C.stop_after = 0;
+  if (100.0 * v[3] < P.eps) {  // solve_streamfct.f90:210-213
+    C.est = 100.0 * v[3];
+    return ctl_stop(C, kDoneOk, PYOMGPU_OK);
+  }
+  C.n = 1;
+  ctl_begin(C, P);
+}
+
+// v = (s, As), max|s|
+__device__ void ctl_after_a(ResCtl& C, const CGResParams& P, const double* v) {
+  const double F_1EM10 = (double)1.e-10f;  // solve_streamfct.f90:262, a default-real literal
+  const double sAs = v[0], smax = v[1];
+  C.stop_after = 0;
+  if (fabs(sAs) < fabs(C.beta) * F_1EM10) {  // :262-266
+    C.est = 100.0 * smax;
+    return ctl_stop(C, kDoneOk, PYOMGPU_OK);
+  }
+  C.alpha = C.beta / sAs;
+  const double step = fabs(C.alpha) * smax;  // :283-297, decided now, applied after the update
+  if (C.n == 1) {
+    C.step1 = step;
+    C.est = step;
+    C.stop_after = step < P.eps;
+  } else if (step < P.eps) {
+    const double rate = exp(log(step / C.step1) / (double)(C.n - 1));
+    C.est = step * rate / (1.0 - rate);
+    C.stop_after = C.est < P.eps;
+  }
+}
+
+// v = (Z res, res) and sum res^2 over the unknowns of the updated residual
+__device__ void ctl_after_b(ResCtl& C, const CGResParams& P, const double* v) {
+  const double beta_next = v[0], rr_next = v[1];
+  if (P.rtol > 0.0 && (C.bb > 0.0 ? rr_next <= C.rtol2bb : rr_next == 0.0)) {
+    C.est = sqrt(rr_next);
+    return ctl_stop(C, kDoneOk, PYOMGPU_OK);
+  }
+  C.betam1 = C.beta;
+  C.beta = beta_next;
+  C.n += 1;
+  ctl_begin(C, P);
+}
+
+// ------------------------------------------------- reduction and exchange
+struct Halo {
+  int sidx;       // shared-memory index (-1: none)
+  long long gidx; // offset of the Z*res word in the exchange buffer; the direction is hsize further
+  double q, s;    // received Z*res and direction
+};
+
+// Loads this thread's halo values (after a completed reduction).
+__device__ __forceinline__ void worker_halo_load(const CGResParams& P, Halo (&hl)[2]) {
+#pragma unroll
+  for (int e = 0; e < 2; e++)
+    if (hl[e].sidx >= 0) {
+      hl[e].q = __ldcg(P.hx + hl[e].gidx);
+      hl[e].s = __ldcg(P.hx + hl[e].gidx + P.hsize);
+    }
+}
+
+__device__ __forceinline__ double* res_slot(const CGResParams& P, unsigned ep, int b) {
+  return P.slots + ((size_t)(ep % 3u) * P.nslot + b) * 4;
+}
+
+// Worker side of a reduction: per-warp partials of the worker warps into wred.
+template <int NV, int kMaxSlot>
+__device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*wred)[4]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    const double r = (k == kMaxSlot) ? warp_max(v[k]) : warp_sum(v[k]);
+    if (lane == 0) wred[w][k] = r;
+  }
+}
+
+// Controller side of epoch ep (warp 0, after the workers' partials are in
+// wred): lane 0 sums them in warp order and publishes the block's slot (last
+// word with st.release); lane l polls the slots l, l+32, ... of all npoll
+// blocks until no word is empty; the totals are formed in a fixed order, so
+// every block obtains the same bits, and lane 0 advances the control state.
+// False on time-out.
+template <int NV, int kMaxSlot, int kStep>
+__device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int npoll, ResCtl& C,
+                                                 const double (*wred)[4]) {
+  const int lane = threadIdx.x;
+  {
+    double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const double x = (lane >= 1 && lane < kResThreads / 32) ? wred[lane][k] : 0.0;
+      t[k] = (k == kMaxSlot) ? warp_max(x) : warp_sum(x);
+    }
+    if (lane == 0) {
+      double* mine = res_slot(P, ep, blockIdx.x);
+#pragma unroll
+      for (int k = 0; k < NV - 1; k++) st_weak_f64(mine + k, sendable(t[k]));
+      st_release_f64(mine + NV - 1, sendable(t[NV - 1]));
+    }
+  }
+  constexpr int kPer = kResMaxSlots / 32;
+  double got[kPer][NV];
+  unsigned want = 0, have = 0;
+#pragma unroll
+  for (int m = 0; m < kPer; m++) {
+    if (lane + 32 * m < npoll) want |= 1u << m;
+#pragma unroll
+    for (int k = 0; k < NV; k++) got[m][k] = 0.0;
+  }
+  bool ok = true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned spin = 1; have != want; spin++) {
+#pragma unroll
+    for (int m = 0; m < kPer; m++) {
+      if (!((want & ~have) >> m & 1u)) continue;
+      const double* sl = res_slot(P, ep, lane + 32 * m);
+      bool all = true;
+#pragma unroll
+      for (int k = 0; k < NV - 1; k++) {
+        got[m][k] = ld_relaxed_f64(sl + k);
+        all = all && !is_empty(got[m][k]);
+      }
+      got[m][NV - 1] = ld_acquire_f64(sl + NV - 1);
+      if (all && !is_empty(got[m][NV - 1])) have |= 1u << m;
+    }
+    if (have != want && (spin & 31u) == 0u &&
+        (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
+      atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+      ok = false;
+      break;
+    }
+  }
+  double out[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+#pragma unroll
+    for (int m = 0; m < kPer; m++)
+      if (have >> m & 1u) a = (k == kMaxSlot) ? fmax(a, got[m][k]) : a + got[m][k];
+    out[k] = (k == kMaxSlot) ? warp_max(a) : warp_sum(a);
+  }
+  if (lane == 0) {
+    if (kStep == kStepInit)
+      ctl_init(C, P, out);
+    else if (kStep == kStepA)
+      ctl_after_a(C, P, out);
+    else
+      ctl_after_b(C, P, out);
+    // every block has finished reading epoch ep-1 (it published epoch ep),
+    // so this block's slot of that buffer (= the one of epoch ep+2) is free
+    double* mine = res_slot(P, ep + 2, blockIdx.x);
+#pragma unroll
+    for (int k = 0; k < 4; k++) st_weak_f64(mine + k, empty_word());
+  }
+  return ok;
+}
+
+__device__ __forceinline__ void workers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kResWorkers) : "memory");
+}
+
+}  // namespace
+
+// Block layout: warp 0 is the controller (reductions across blocks, control
+// flow), warps 1-15 are the workers that own the points.  Both sides pass the
+// same sequence of block barriers: S1 (the workers' partials are in shared
+// memory) and S2 (the controller's decision is in shared memory, or a wait
+// timed out).  Work that overlaps the wait of the other blocks (the solution
+// update) runs between S1 and S2.
+template <int P>
+__global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_constant__ CGResParams Pm) {
+  constexpr int CH = P == 8 ? 8 : 4;  // points per TMEM chunk (tcgen05 .x16 / .x8; .x16 at P = 16 spills)
+  constexpr int NC = P / CH;  // chunks per field
+  constexpr int CW = 2 * CH;  // TMEM columns per chunk
+  static_assert(P % CH == 0 && NC * CW <= 32, "a field takes at most 32 TMEM columns per thread");
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint32_t s_tmem;
+  __shared__ ResCtl C;
+  __shared__ double wred[kResThreads / 32][4];
+  const Geo g = Pm.g;
+  const OpDev<double> op = Pm.op;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    tc::tmem_alloc(&s_tmem, 512);
+    tc::tmem_relinquish();
+  }
+
+  const int nb = gridDim.x;
+  const int px = blockIdx.x % Pm.npx, py = blockIdx.x / Pm.npx;
+  const int ilo = 1 + (int)(((long long)px * g.nx) / Pm.npx);
+  const int ihi = (int)(((long long)(px + 1) * g.nx) / Pm.npx);
+  const int jlo = 1 + (int)(((long long)py * g.ny) / Pm.npy);
+  const int jhi = (int)(((long long)(py + 1) * g.ny) / Pm.npy);
+  const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, sp = pw + 2;
+  const int pw_ = pw, ph_ = ph, jlo_ = jlo;
+  double* ss = sm;                    // (pw+2) x (ph+2): direction, halo included
+  double* sfx = ss + sp * (ph + 2);   // (pw+1) x ph: FX(ilo+lx, j), lx = 0..pw
+  double* sfy = sfx + (pw + 1) * ph;  // pw x (ph+1): FY(i, jlo+ly), ly = 0..ph
+  double* sbx = sfy + pw * (ph + 1);  // ph: bx(jlo+ly), then ph: by(jlo+ly)
+
+  for (int e = threadIdx.x; e < sp * (ph + 2); e += kResThreads) ss[e] = 0.0;
+  for (int e = threadIdx.x; e < (pw + 1) * ph; e += kResThreads)
+    sfx[e] = op.FX[g.at(ilo + e % (pw + 1), jlo + e / (pw + 1))];
+  for (int e = threadIdx.x; e < pw * (ph + 1); e += kResThreads) sfy[e] = op.FY[g.at(ilo + e % pw, jlo + e / pw)];
+  for (int e = threadIdx.x; e < ph; e += kResThreads) {
+    sbx[e] = op.bx[jlo + e + 1];
+    sbx[ph + e] = op.by[jlo + e + 1];
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+
+  if (warp == 0) {
+    // ============================================================ controller
+    unsigned ep = 0;
+    bool stopped_after_update = false;  // the stop decided before sweep B (C stays as the workers read it)
+    __syncthreads();  // S1
+    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred);
+    if (!__syncthreads_and(ok)) goto out;  // S2
+    if (C.act == kRun) {
+      for (;;) {
+        __syncthreads();  // S1: partials of sweep A
+        ok = controller_epoch<2, 1, kStepA>(Pm, ++ep, nb, C, wred);
+        if (!__syncthreads_and(ok)) goto out;  // S2
+        if (C.act != kRun) break;
+        if (C.stop_after) {  // the workers finish sweep B and stop
+          stopped_after_update = true;
+          break;
+        }
+        __syncthreads();  // S1: partials of sweep B
+        ok = controller_epoch<2, -1, kStepB>(Pm, ++ep, nb, C, wred);
+        if (!__syncthreads_and(ok)) goto out;  // S2
+        if (C.act != kRun) break;
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const int converged = stopped_after_update || C.act == kDoneOk;
+      Pm.out->iterations = C.n;
+      Pm.out->converged = converged;
+      Pm.out->status = converged ? PYOMGPU_OK : (C.est != C.est ? PYOMGPU_NAN : C.status);
+      Pm.out->est = C.est;
+    }
+  } else {
+    // =============================================================== workers
+    // this thread's column segment: column lx, rows ly0 .. ly0+nrow-1
+    const int wt = (int)threadIdx.x - 32;
+    const int lx_ = wt % Pm.wmax;
+    const int ly0_ = (wt / Pm.wmax) * P;
+    const int nrow_ = (lx_ < pw && ly0_ < ph) ? min(P, ph - ly0_) : 0;
+    const int i_ = ilo + lx_;
+    int lx = lx_, ly0 = ly0_, nrow = nrow_, i = i_;
+    const double axi = nrow_ > 0 ? op.ax[i_ + 1] : 0.0;
+    // TMEM of this thread: lane 32*(warp%4)+lane, 32 columns per field from 128*(warp/4)
+    const uint32_t tm = s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * (warp >> 2));
+    const uint32_t t_res = tm, t_sol = tm + 32, t_z = tm + 64;
+
+    // halo positions received (west, east, south, north edges that have a
+    // neighbour; a non-cyclic domain edge keeps the zero direction)
+    Halo hl[2];
+    {
+      const int nW = (ilo > 1 || g.cyclic_x) ? ph : 0, nE = (ihi < g.nx || g.cyclic_x) ? ph : 0;
+      const int nS = (jlo > 1 || g.cyclic_y) ? pw : 0, nN = (jhi < g.ny || g.cyclic_y) ? pw : 0;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int h = wt + e * kResWorkers;
+        hl[e].sidx = -1;
+        hl[e].gidx = 0;
+        hl[e].q = hl[e].s = 0.0;
+        if (h >= nW + nE + nS + nN) continue;
+        int hx, hy;
+        if (h < nW) {
+          hx = -1;
+          hy = h;
+        } else if (h < nW + nE) {
+          hx = pw;
+          hy = h - nW;
+        } else if (h < nW + nE + nS) {
+          hx = h - nW - nE;
+          hy = -1;
+        } else {
+          hx = h - nW - nE - nS;
+          hy = ph;
+        }
+        hl[e].sidx = (hy + 1) * sp + hx + 1;
+        hl[e].gidx = (long long)g.at(ilo + hx, jlo + hy);
+      }
+    }
+
+    double s[P], q[P];  // direction; q: Z*res before sweep A, As after it
+
+    // ---------------------------------------------------------------- init
+    // res = forc - A sol, solve_streamfct.f90:196-201
+    {
+      double v[4] = {0.0, 0.0, 0.0, 0.0};  // beta, bb, rr, zresmax
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        uint32_t br[CW], bz[CW], bx[CW];
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+          const int u = c * CH + k;
+          double rv = 0.0, w = 0.0, x = 0.0;
+          s[u] = 0.0;
+          q[u] = 0.0;
+          if (u < nrow) {
+            const int ly = ly0 + u, j = jlo + ly;
+            const double f = Pm.forc[fidx(g.nx, i, j)];
+            rv = f - apply_point(op, g, Pm.sol, i, j);
+            w = op.W[g.at(i, j)];
+            x = Pm.sol[g.at(i, j)];
+            const double zr = w * rv;
+            v[0] += zr * rv;
+            if (w != 0.0) {
+              v[1] += f * f;
+              v[2] += rv * rv;
+            }
+            v[3] = fmax(v[3], fabs(zr));
+            q[u] = zr;
+            if (lx == 0 || lx == pw - 1 || ly == 0 || ly == ph - 1) {
+              publish_cyclic(Pm.hx, g, i, j, zr);
+              publish_cyclic(Pm.hx + Pm.hsize, g, i, j, 0.0);
+            }
+          }
+          col_put(br, k, rv);
+          col_put(bz, k, w);
+          col_put(bx, k, x);
+        }
+        tm_st<CW>(t_res + c * CW, br);
+        tm_st<CW>(t_z + c * CW, bz);
+        tm_st<CW>(t_sol + c * CW, bx);
+      }
+      tm_wait_st();
+      worker_partials<4, 3>(v, wred);
+    }
+    __syncthreads();                       // S1
+    if (!__syncthreads_and(1)) goto out;  // S2
+    if (C.act != kRun) goto done;
+    worker_halo_load(Pm, hl);
+
+    for (;;) {
+      // ---------------------------------------------- sweep A: direction, As
+      lx = opaque(lx_);
+      ly0 = opaque(ly0_);
+      nrow = opaque(nrow_);
+      {
+        const int sp = opaque(pw + 2);
+        const double bq = C.bq;
+#pragma unroll
+        for (int u = 0; u < P; u++)
+          if (u < nrow) {
+            s[u] = q[u] + bq * s[u];
+            ss[(ly0 + u + 1) * sp + lx + 1] = s[u];
+          }
+#pragma unroll
+        for (int e = 0; e < 2; e++)
+          if (hl[e].sidx >= 0) ss[hl[e].sidx] = hl[e].q + bq * hl[e].s;
+      }
+      workers_sync();
+      lx = opaque(lx_);
+      ly0 = opaque(ly0_);
+      nrow = opaque(nrow_);
+      {
+        const int pw = opaque(pw_), sp = pw + 2, ph = opaque(ph_);
+        double v[2] = {0.0, 0.0};  // (s, As), max|s|
+        if (nrow > 0) {
+          double fys = sfy[ly0 * pw + lx];
+#pragma unroll
+          for (int u = 0; u < P; u++)
+            if (u < nrow) {
+              const int ly = ly0 + u;
+              const int k = (ly + 1) * sp + lx + 1;
+              const double sc = s[u];
+              const double se = ss[k + 1], sw = ss[k - 1];
+              const double sn = (u + 1 < P && u + 1 < nrow) ? s[u + 1 < P ? u + 1 : u] : ss[k + sp];
+              const double so = (u > 0) ? s[u > 0 ? u - 1 : 0] : ss[k - sp];
+              const double fxw = sfx[ly * (pw + 1) + lx], fxe = sfx[ly * (pw + 1) + lx + 1];
+              const double fyn = sfy[(ly + 1) * pw + lx];
+              const double a = axi * sbx[ly] * (fxe * (se - sc) + fxw * (sw - sc)) +
+                               sbx[ph + ly] * (fyn * (sn - sc) + fys * (so - sc));
+              v[0] += sc * a;
+              v[1] = fmax(v[1], fabs(sc));
+              q[u] = a;
+              fys = fyn;
+            }
+        }
+        worker_partials<2, 1>(v, wred);
+      }
+      __syncthreads();                           // S1
+      if (!__syncthreads_and(1)) goto out;      // S2
+      if (C.act != kRun) goto done;
+      // ---------------------------------------------- sweep B: residual update
+      lx = opaque(lx_);
+      ly0 = opaque(ly0_);
+      nrow = opaque(nrow_);
+      i = opaque(i_);
+      {
+        const int pw = opaque(pw_), ph = opaque(ph_), jlo = opaque(jlo_);
+        const double alpha = C.alpha;
+        const bool stop_after = C.stop_after != 0;
+        double v[2] = {0.0, 0.0};  // (Z res, res), sum res^2 over the unknowns
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          uint32_t br[CW], bz[CW];
+          tm_ld<CW>(t_res + c * CW, br);
+          tm_ld<CW>(t_z + c * CW, bz);
+          tm_wait_ld();
+#pragma unroll
+          for (int k = 0; k < CH; k++) {
+            const int u = c * CH + k;
+            if (u < nrow) {
+              const double w = col_get(bz, k);
+              const double rv = col_get(br, k) - alpha * q[u];
+              const double zr = w * rv;
+              v[0] += zr * rv;
+              if (w != 0.0) v[1] += rv * rv;
+              q[u] = zr;
+              col_put(br, k, rv);
+            }
+          }
+          tm_st<CW>(t_res + c * CW, br);
+        }
+        // boundary points to the neighbours: (Z res, s) for their next direction
+        if (nrow > 0) {
+          const bool edge_col = lx == 0 || lx == pw - 1;
+#pragma unroll
+          for (int u = 0; u < P; u++) {
+            const int ly = ly0 + u;
+            if (u < nrow && (edge_col || ly == 0 || ly == ph - 1)) {
+              publish_cyclic(Pm.hx, g, i, jlo + ly, q[u]);
+              publish_cyclic(Pm.hx + Pm.hsize, g, i, jlo + ly, s[u]);
+            }
+          }
+        }
+        if (!stop_after) {
+          worker_partials<2, -1>(v, wred);
+          __syncthreads();  // S1
+        }
+        // sol += alpha*s (solve_streamfct.f90:278), while the other blocks finish
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          uint32_t bx[CW];
+          tm_ld<CW>(t_sol + c * CW, bx);
+          tm_wait_ld();
+#pragma unroll
+          for (int k = 0; k < CH; k++) {
+            const int u = c * CH + k;
+            if (u < nrow) col_put(bx, k, col_get(bx, k) + alpha * s[u]);
+          }
+          tm_st<CW>(t_sol + c * CW, bx);
+        }
+        tm_wait_st();
+        if (stop_after) goto done;
+      }
+      if (!__syncthreads_and(1)) goto out;  // S2
+      if (C.act != kRun) goto done;
+      worker_halo_load(Pm, hl);
+    }
+
+  done:
+    // the residual and solution of the last iterate back to global memory
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      uint32_t br[CW], bx[CW];
+      tm_ld<CW>(t_res + c * CW, br);
+      tm_ld<CW>(t_sol + c * CW, bx);
+      tm_wait_ld();
+#pragma unroll
+      for (int k = 0; k < CH; k++) {
+        const int u = c * CH + k;
+        if (u < nrow) {
+          const int j = jlo + ly0 + u;
+          store_cyclic(Pm.res, g, i, j, col_get(br, k));
+          Pm.sol[g.at(i, j)] = col_get(bx, k);
+        }
+      }
+    }
+  }
+out:
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(s_tmem, 512);
+}
+
+template __global__ void cg_res_kernel<4>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<8>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<16>(const __grid_constant__ CGResParams);
+
+const void* cg_res_kernel_ptr(int p) {
+  switch (p) {
+    case 4: return (const void*)cg_res_kernel<4>;
+    case 8: return (const void*)cg_res_kernel<8>;
+    case 16: return (const void*)cg_res_kernel<16>;
+    default: return nullptr;
+  }
+}
+
+}  // namespace pyomgpu

@@ -11,6 +11,7 @@
 #include "cg_batch.cuh"
 #include "cg_pipe.cuh"
 #include "cg_ref.cuh"
+#include "cg_res.cuh"
 #include "common.cuh"
 #include "islands.h"
 #include "kernels.cuh"
@@ -88,6 +89,16 @@ struct pyomgpu_ctx {
     double us_per_it = 0;
   } tune;
 
+  // on-chip-resident kernel of the streamfunction solves (cg_res.cu): piece
+  // layout planned on first use, exchange buffers allocated with it
+  int cg_kernel = 0;  // 0 automatic, 1 tiled cg_ref_kernel, 2 resident cg_res_kernel
+  struct Resident {
+    bool planned = false, ok = false;
+    int npx = 0, npy = 0, wmax = 0, hmax = 0, p = 0;
+    size_t smem = 0;
+    double *hx = nullptr, *slots = nullptr;
+  } resd;
+
   // work-queue batch (pyomgpu_congrad_streamfunction_batch and the psin
   // solves); grows to the largest batch run through this context
   struct Batch {
@@ -116,6 +127,8 @@ struct pyomgpu_ctx {
     if (batch.h_probs) cudaFreeHost(batch.h_probs);
     if (batch.h_state) cudaFreeHost(batch.h_state);
     if (batch.h_rr) cudaFreeHost(batch.h_rr);
+    for (void* p : {(void*)resd.hx, (void*)resd.slots})
+      if (p) cudaFree(p);
     void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
                     sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,
                     res, s0, s1, As, sol, stage_a, stage_b, fpx, fpy, forc, zeros, part, scal, ctl, slots, d_result,

@@ -148,6 +148,23 @@ class ExternalMode:
         can never complete, so it ends with PYOMGPU_TIMEOUT."""
         _abi.check(self._L.pyomgpu_inject_barrier_stall(self._ctx, int(bool(enable))))
 
+    def set_cg_kernel(self, kernel: str = "auto"):
+        """CG kernel of the streamfunction solves: ``"tiled"`` (any grid),
+        ``"resident"`` (one piece of the grid per SM, held on chip for the
+        whole solve; raises on a grid that does not fit) or ``"auto"``."""
+        code = {"auto": 0, "tiled": 1, "resident": 2}[kernel]
+        _abi.check(self._L.pyomgpu_set_cg_kernel(self._ctx, code))
+
+    def resident_layout(self):
+        """(pieces in x, pieces in y, points per thread) of the resident
+        kernel on this grid, or None when the grid does not fit."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        rc = self._L.pyomgpu_resident_layout(self._ctx, C.byref(a), C.byref(b), C.byref(c))
+        if rc == _abi.EINVAL:
+            return None
+        _abi.check(rc)
+        return a.value, b.value, c.value
+
     # ---- islands -----------------------------------------------------------------
     def streamfunction_init(self, M=None, mnisle=0, maxipp=0, maxq=0, eps=None, max_it=None):
         """streamfct_init.f90:7-304; fills ``nisle, boundary, line_dir,

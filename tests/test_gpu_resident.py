@@ -1,0 +1,139 @@
+"""The on-chip-resident streamfunction CG kernel (csrc/cg_res.cu) against the
+CPU oracle and against the tiled kernel (csrc/cg_ref.cu) on the same inputs.
+
+Tolerances: both kernels run congrad_streamfunction's algorithm in FP64 with
+tree-ordered dot products (different orders), so converged solutions agree
+with the oracle and with each other to 1e-10 relative and iteration counts
+within one; the reference's status paths (max_it, NaN, time-out) are exact.
+"""
+import numpy as np
+import pytest
+
+from pyom2_b200 import _abi, synth
+from pyom2_b200.external import ExternalMode
+
+pytestmark = pytest.mark.gpu
+
+RTOL_SOL = 1e-10
+
+
+def rel(a, b, mask=None):
+    a, b = np.asarray(a), np.asarray(b)
+    if mask is not None:
+        a, b = a[mask], b[mask]
+    n = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / n if n > 0 else np.linalg.norm(a - b)
+
+
+WORLDS = {
+    "c0": lambda: synth.config0(),
+    "cyclic96": lambda: synth._global_like(96, 48, -80.0, 80.0, 13, n_land_masses=6, mask_sigma=4.0,
+                                           depth_sigma=4.0, name="small"),
+    "cyclic200": lambda: synth._global_like(200, 100, -80.0, 80.0, 9, n_land_masses=10, mask_sigma=4.0,
+                                            depth_sigma=4.0, name="small"),
+    "basin130": lambda: synth.basin(130, 70, 302, 0.25, 6),
+    "channel96": lambda: synth.config4(1004, nx=96, ny=96, nz=4),
+}
+
+
+def setup(name, oracle_lib, kernel):
+    W = WORLDS[name]()
+    O = oracle_lib.Oracle(W.M.copy())
+    O.streamfunction_init(maxipp=10**6, maxq=10**6)
+    E = ExternalMode(W.M)
+    E.streamfunction_init(maxipp=10**6, maxq=10**6)
+    E.set_cg_kernel(kernel)
+    return W, O, E
+
+
+@pytest.mark.parametrize("kernel", ["resident", "tiled"])
+@pytest.mark.parametrize("name", list(WORLDS))
+def test_congrad_streamfunction_matches_oracle(oracle_lib, name, kernel):
+    W, O, E = setup(name, oracle_lib, kernel)
+    cf = O.make_coeff_streamfunction()
+    rng = np.random.default_rng(11)
+    sol0 = np.asfortranarray(rng.standard_normal(W.M.shape2d) * 1e3)
+    so = sol0.copy(order="F")
+    ro = O.congrad_streamfunction(cf, W.forc, so)
+    sg = sol0.copy(order="F")
+    it, conv, info = E.congrad_streamfunction(W.forc, sg)
+    assert conv == ro["converged"] and abs(it - ro["iterations"]) <= 1, (it, ro["iterations"])
+    assert rel(sg, so) < RTOL_SOL
+    # halo as the reference leaves it (set once at entry)
+    assert rel(sg[:2], so[:2]) < RTOL_SOL or np.array_equal(sg[:2], so[:2])
+
+
+@pytest.mark.parametrize("name", ["c0", "cyclic200"])
+def test_solve_rtol_resident(oracle_lib, name):
+    W, O, E = setup(name, oracle_lib, "resident")
+    sol = np.zeros(W.M.shape2d, order="F")
+    info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=_abi.PREC_F64)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
+    cf = O.make_coeff_streamfunction()
+    Z = O.make_inv_sfc(cf)
+    assert O.rel_residual(cf, Z, W.forc, sol) <= 1.5e-10
+
+
+def test_headline_grid_layout_and_kernels_agree():
+    """1440 x 720 (20 islands): 37 x 4 pieces of at most 39 x 180 points, 16
+    points per thread; the resident and tiled kernels reach the same solution
+    and the same iteration count within one."""
+    W = synth.config1()
+    E = ExternalMode(W.M)
+    E.streamfunction_init(maxipp=10**6, maxq=10**6)
+    assert E.resident_layout() == (37, 4, 16)
+    out = {}
+    for kernel in ("tiled", "resident"):
+        E.set_cg_kernel(kernel)
+        sol = np.zeros(W.M.shape2d, order="F")
+        info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=_abi.PREC_F64)
+        assert info["status"] == 0 and info["rel_residual"] <= 1e-10, (kernel, info)
+        out[kernel] = (sol, info)
+    (st, it_t), (sr, it_r) = [(out[k][0], out[k][1]) for k in ("tiled", "resident")]
+    assert abs(it_t["iterations"] - it_r["iterations"]) <= 1
+    assert rel(sr, st) < 1e-8
+    print("1440x720 device ms: tiled %.2f, resident %.2f" % (it_t["device_ms"], it_r["device_ms"]))
+
+
+def test_reruns_are_bit_identical():
+    W = WORLDS["cyclic200"]()
+    E = ExternalMode(W.M)
+    E.streamfunction_init(maxipp=10**6, maxq=10**6)
+    E.set_cg_kernel("resident")
+    a = np.zeros(W.M.shape2d, order="F")
+    b = np.zeros(W.M.shape2d, order="F")
+    ia = E.congrad_streamfunction(W.forc, a)[0]
+    ib = E.congrad_streamfunction(W.forc, b)[0]
+    assert ia == ib and np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("kernel", ["resident", "tiled"])
+def test_status_paths(oracle_lib, kernel):
+    W, O, E = setup("c0", oracle_lib, kernel)
+    bad = W.forc.copy(order="F")
+    bad[10, 10] = np.nan
+    with pytest.raises(_abi.PyOMGPUError) as e:
+        E.congrad_streamfunction(bad, np.zeros(W.M.shape2d, order="F"))
+    assert e.value.code == _abi.NAN
+    with pytest.warns(RuntimeWarning):
+        it, conv, info = E.congrad_streamfunction(W.forc, np.zeros(W.M.shape2d, order="F"), max_it=3)
+    assert it == 4 and not conv and info["status"] == _abi.MAXITER
+    E.set_sync_timeout(1e-3)
+    E.inject_barrier_stall(True)
+    with pytest.raises(_abi.PyOMGPUError) as e:
+        E.congrad_streamfunction(W.forc, np.zeros(W.M.shape2d, order="F"))
+    assert e.value.code == _abi.TIMEOUT
+    E.set_sync_timeout(2.0)
+    s = np.zeros(W.M.shape2d, order="F")
+    it, conv, _ = E.congrad_streamfunction(W.forc, s)  # the context is still usable
+    assert conv and it > 10
+
+
+def test_too_large_grid_is_refused():
+    W = synth.config3()  # 2048 x 1024: pieces do not fit on chip
+    E = ExternalMode(W.M)
+    assert E.resident_layout() is None
+    with pytest.raises(_abi.PyOMGPUError) as e:
+        E.set_cg_kernel("resident")
+    assert e.value.code == _abi.EINVAL
+    E.set_cg_kernel("auto")
