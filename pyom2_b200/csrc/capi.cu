@@ -175,7 +175,7 @@ int res_plan(pyomgpu_ctx* c) {
       per_sm < 1)
     return PYOMGPU_OK;
   const int nb = R.npx * R.npy;
-  if (int rc = dalloc(&R.hx, 2 * c->g.size())) return rc;
+  if (int rc = dalloc(&R.hx, 4 * c->g.size())) return rc;
   if (int rc = dalloc(&R.slots, (size_t)3 * (nb + 1) * 4)) return rc;
   R.ok = true;
   return PYOMGPU_OK;

@@ -29,9 +29,10 @@
 //     same decisions.  Slots rotate over three buffers; a block empties its
 //     slot of epoch e+2 as soon as it completes epoch e, when every reader of
 //     the slot's previous contents has finished.
-//   * after the residual update a block writes (Z*res, s) of its boundary
-//     points into two padded exchange arrays (with the setcyclic_xy copies)
-//     before its slot is released, so once a block has acquired every slot
+//   * after the residual update a block stages (Z*res, s) of its boundary
+//     points in shared memory and its workers copy them, one entry each, into
+//     exchange records (4 words per padded position, with the setcyclic_xy
+//     copies) before its slot is released, so once a block has acquired every slot
 //     of that reduction the values of its halo are visible: it loads them
 //     once (bypassing L1) and recomputes the neighbours' next direction on
 //     the halo with the operation their owner uses.  A value is overwritten
@@ -73,16 +74,17 @@ __device__ __forceinline__ double sendable(double v) {
   return is_empty(v) ? __longlong_as_double(0x7fffffffffffffffll) : v;
 }
 
-// Writes v at interior (i,j) of an exchange array and at the halo positions
+// Writes v into the exchange record (4 words per padded position; a word
+// offset is already added to a) of interior (i,j) and of the halo positions
 // setcyclic_xy fills from it.
 __device__ __forceinline__ void publish_cyclic(double* a, const Geo& g, int i, int j, double v) {
-  st_weak_f64(a + g.at(i, j), v);
+  st_weak_f64(a + 4 * g.at(i, j), v);
   int xc, yc;
   cyclic_copies(g, i, j, xc, yc);
-  if (xc != 0x7fffffff) st_weak_f64(a + g.at(xc, j), v);
+  if (xc != 0x7fffffff) st_weak_f64(a + 4 * g.at(xc, j), v);
   if (yc != 0x7fffffff) {
-    st_weak_f64(a + g.at(i, yc), v);
-    if (xc != 0x7fffffff) st_weak_f64(a + g.at(xc, yc), v);
+    st_weak_f64(a + 4 * g.at(i, yc), v);
+    if (xc != 0x7fffffff) st_weak_f64(a + 4 * g.at(xc, yc), v);
   }
 }
 
@@ -237,7 +239,7 @@ __device__ void ctl_after_b(ResCtl& C, const CGResParams& P, const double* v) {
 // ------------------------------------------------- reduction and exchange
 struct Halo {
   int sidx;       // shared-memory index (-1: none)
-  long long gidx; // offset of the Z*res word in the exchange buffer; the direction is hsize further
+  long long gidx; // padded position whose exchange record is received
   double q, s;    // received Z*res and direction
 };
 
@@ -246,9 +248,56 @@ __device__ __forceinline__ void worker_halo_load(const CGResParams& P, Halo (&hl
 #pragma unroll
   for (int e = 0; e < 2; e++)
     if (hl[e].sidx >= 0) {
-      hl[e].q = __ldcg(P.hx + hl[e].gidx);
-      hl[e].s = __ldcg(P.hx + hl[e].gidx + P.hsize);
+      hl[e].q = __ldcg(P.hx + 4 * hl[e].gidx);
+      hl[e].s = __ldcg(P.hx + 4 * hl[e].gidx + 1);
     }
+}
+
+// Boundary staging: the values of a piece's boundary points in shared memory,
+// entries [0,ph) west column, [ph,2ph) east column, [2ph,2ph+pw) south row,
+// [2ph+pw,2ph+2pw) north row (a corner point in two entries); quantity k of
+// entry e at k*nent+e.  One quantity of one point:
+__device__ __forceinline__ void stage_one(double* spub, int pw, int ph, int lx, int ly, double v) {
+  if (lx == 0) spub[ly] = v;
+  if (lx == pw - 1) spub[ph + ly] = v;
+  if (ly == 0) spub[2 * ph + lx] = v;
+  if (ly == ph - 1) spub[2 * ph + pw + lx] = v;
+}
+
+// The staged boundary values (NQ quantities) to the exchange records (word k
+// of a position's record, with the setcyclic_xy copies), one entry per worker
+// thread; only the edges some block reads.
+template <int NQ>
+__device__ __forceinline__ void copy_out(const CGResParams& P, const double* spub, int ilo, int ihi, int jlo, int jhi,
+                                         int wt) {
+  const Geo& g = P.g;
+  const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, nent = 2 * (pw + ph);
+#pragma unroll 1
+  for (int e = wt; e < nent; e += kResWorkers) {
+    int i, j;
+    bool need;
+    if (e < ph) {
+      i = ilo;
+      j = jlo + e;
+      need = ilo > 1 || g.cyclic_x;
+    } else if (e < 2 * ph) {
+      i = ihi;
+      j = jlo + e - ph;
+      need = ihi < g.nx || g.cyclic_x;
+    } else if (e < 2 * ph + pw) {
+      i = ilo + e - 2 * ph;
+      j = jlo;
+      need = jlo > 1 || g.cyclic_y;
+    } else {
+      i = ilo + e - 2 * ph - pw;
+      j = jhi;
+      need = jhi < g.ny || g.cyclic_y;
+    }
+    if (need) {
+#pragma unroll
+      for (int k = 0; k < NQ; k++) publish_cyclic(P.hx + k, g, i, j, spub[k * nent + e]);
+    }
+  }
 }
 
 __device__ __forceinline__ double* res_slot(const CGResParams& P, unsigned ep, int b) {
@@ -389,6 +438,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
   double* sfx = ss + sp * (ph + 2);   // (pw+1) x ph: FX(ilo+lx, j), lx = 0..pw
   double* sfy = sfx + (pw + 1) * ph;  // pw x (ph+1): FY(i, jlo+ly), ly = 0..ph
   double* sbx = sfy + pw * (ph + 1);  // ph: bx(jlo+ly), then ph: by(jlo+ly)
+  double* spub = sbx + 2 * ph;        // 2 x 2(pw+ph): staged boundary Z*res, direction
+  const int nent = 2 * (pw + ph);
 
   for (int e = threadIdx.x; e < sp * (ph + 2); e += kResThreads) ss[e] = 0.0;
   for (int e = threadIdx.x; e < (pw + 1) * ph; e += kResThreads)
@@ -507,10 +558,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
             }
             v[3] = fmax(v[3], fabs(zr));
             q[u] = zr;
-            if (lx == 0 || lx == pw - 1 || ly == 0 || ly == ph - 1) {
-              publish_cyclic(Pm.hx, g, i, j, zr);
-              publish_cyclic(Pm.hx + Pm.hsize, g, i, j, 0.0);
-            }
+            stage_one(spub, pw, ph, lx, ly, zr);
+            stage_one(spub + nent, pw, ph, lx, ly, 0.0);
           }
           col_put(br, k, rv);
           col_put(bz, k, w);
@@ -523,6 +572,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
       tm_wait_st();
       worker_partials<4, 3>(v, wred);
     }
+    workers_sync();
+    copy_out<2>(Pm, spub, ilo, ihi, jlo, jhi, wt);
     __syncthreads();                       // S1
     if (!__syncthreads_and(1)) goto out;  // S2
     if (C.act != kRun) goto done;
@@ -611,17 +662,14 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           tm_st<CW>(t_res + c * CW, br);
         }
         // boundary points to the neighbours: (Z res, s) for their next direction
-        if (nrow > 0) {
-          const bool edge_col = lx == 0 || lx == pw - 1;
 #pragma unroll
-          for (int u = 0; u < P; u++) {
-            const int ly = ly0 + u;
-            if (u < nrow && (edge_col || ly == 0 || ly == ph - 1)) {
-              publish_cyclic(Pm.hx, g, i, jlo + ly, q[u]);
-              publish_cyclic(Pm.hx + Pm.hsize, g, i, jlo + ly, s[u]);
-            }
+        for (int u = 0; u < P; u++)
+          if (u < nrow) {
+            stage_one(spub, pw, ph, lx, ly0 + u, q[u]);
+            stage_one(spub + 2 * (pw + ph), pw, ph, lx, ly0 + u, s[u]);
           }
-        }
+        workers_sync();
+        copy_out<2>(Pm, spub, ilo, ihi, jlo, jhi, wt);
         if (!stop_after) {
           worker_partials<2, -1>(v, wred);
           __syncthreads();  // S1

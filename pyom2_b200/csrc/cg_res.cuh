@@ -22,8 +22,8 @@ struct CGResParams {
   const double* forc;  // Fortran layout (ld nx+4), device
   double* sol;         // padded, halo valid on entry; interior updated
   double* res;         // padded; the residual of the last iterate on exit (with setcyclic copies)
-  double* hx;          // halo exchange: Z*res, then the direction (padded arrays of hsize words)
-  long long hsize;     // words per exchange array (padded field size)
+  double* hx;          // halo exchange: a 4-word record per padded position (Z*res, direction)
+  long long hsize;     // padded positions (records)
   double* slots;       // 3 buffers x nslot x 4 reduction words, all empty on entry
   int nslot;           // gridDim.x + 1
   int npx, npy;        // pieces in x and y (gridDim.x = npx * npy)
@@ -38,9 +38,11 @@ struct CGResParams {
 };
 
 // Dynamic shared memory of a w x h piece: the direction with its one-cell
-// halo, the x- and y-face couplings and the row factors bx, by.
+// halo, the x- and y-face couplings, the row factors bx, by and the staged
+// boundary values (2 per boundary entry).
 __host__ __device__ constexpr size_t res_smem_bytes(int w, int h) {
-  return 8 * ((size_t)(w + 2) * (h + 2) + (size_t)(w + 1) * h + (size_t)w * (h + 1) + 2 * (size_t)h);
+  return 8 * ((size_t)(w + 2) * (h + 2) + (size_t)(w + 1) * h + (size_t)w * (h + 1) + 2 * (size_t)h +
+              4 * (size_t)(w + h));
 }
 
 // Threads that a w x h piece needs with p points per thread.

@@ -155,6 +155,11 @@ class ExternalMode:
         code = {"auto": 0, "tiled": 1, "resident": 2}[kernel]
         _abi.check(self._L.pyomgpu_set_cg_kernel(self._ctx, code))
 
+    def resident_kernel_name(self):
+        """Name of the resident kernel instance the automatic choice launches."""
+        lay = self.resident_layout()
+        return None if lay is None else f"cg_res_kernel<{lay[2]}>"
+
     def resident_layout(self):
         """(pieces in x, pieces in y, points per thread) of the resident
         kernel on this grid, or None when the grid does not fit."""
