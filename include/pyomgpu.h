@@ -156,10 +156,17 @@ int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* ctx, int32_t enable);
  * 2 = the on-chip-resident kernel (one piece of the grid per SM, with the
  *     direction and face couplings in shared memory and the residual,
  *     solution and preconditioner in tensor memory for the whole solve;
- *     grids whose largest piece fits, about 1.04 M points on 148 SMs),
- * 0 = automatic (2 wherever the grid fits).  PYOMGPU_EINVAL for 2 on a grid
- * that does not fit.  The surface-pressure solve always uses 1.  Reduction
- * order differs between the kernels: results change at rounding level. */
+ *     grids whose largest piece fits, about 1.04 M points on 148 SMs), with
+ *     the reference's two reductions per iteration,
+ * 3 = the same resident layout with one reduction per iteration (A p by
+ *     recurrence and the reference's (p, Ap) by its exact bilinear expansion
+ *     in products of the sweep before; the reference's stopping tests are
+ *     evaluated one reduction later, on the same quantities),
+ * 0 = automatic (2 wherever the grid fits: at 1440 x 720 it is faster than 3,
+ *     whose seven-term reductions and register spills outweigh the saved one).  PYOMGPU_EINVAL for 2 or 3 on a
+ * grid that does not fit.  The surface-pressure solve always uses 1.
+ * Reduction order and recurrences differ between the kernels: results
+ * change at rounding level. */
 int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* ctx, int32_t kernel);
 /* Piece layout the resident kernel uses on this grid: pieces in x and y and
  * points per thread; PYOMGPU_EINVAL when the grid does not fit. */

@@ -136,10 +136,12 @@ int res_plan(pyomgpu_ctx* c) {
     return fail(PYOMGPU_ECUDA, "device attribute query failed");
   size_t stat = 0;
   for (int k = 0; k < kResNP; k++) {
-    cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, cg_res_kernel_ptr(kResP[k])) != cudaSuccess)
-      return fail(PYOMGPU_ECUDA, "resident kernel attributes");
-    stat = std::max(stat, fa.sharedSizeBytes);
+    for (bool single : {false, true}) {
+      cudaFuncAttributes fa{};
+      if (cudaFuncGetAttributes(&fa, cg_res_kernel_ptr(kResP[k], single)) != cudaSuccess)
+        return fail(PYOMGPU_ECUDA, "resident kernel attributes");
+      stat = std::max(stat, fa.sharedSizeBytes);
+    }
   }
   if ((size_t)optin <= stat) return PYOMGPU_OK;
   const size_t cap = (size_t)optin - stat;
@@ -166,17 +168,20 @@ int res_plan(pyomgpu_ctx* c) {
     }
   if (best == 1e300) return PYOMGPU_OK;
   for (int k = 0; k < kResNP; k++)
-    if (cudaFuncSetAttribute(cg_res_kernel_ptr(kResP[k]), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) !=
-        cudaSuccess)
-      return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the resident kernel");
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_res_kernel_ptr(R.p), kResThreads, R.smem) !=
-          cudaSuccess ||
-      per_sm < 1)
-    return PYOMGPU_OK;
+    for (bool single : {false, true})
+      if (cudaFuncSetAttribute(cg_res_kernel_ptr(kResP[k], single), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)cap) != cudaSuccess)
+        return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the resident kernel");
+  for (bool single : {false, true}) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_res_kernel_ptr(R.p, single), kResThreads,
+                                                      R.smem) != cudaSuccess ||
+        per_sm < 1)
+      return PYOMGPU_OK;
+  }
   const int nb = R.npx * R.npy;
-  if (int rc = dalloc(&R.hx, 4 * c->g.size())) return rc;
-  if (int rc = dalloc(&R.slots, (size_t)3 * (nb + 1) * 4)) return rc;
+  if (int rc = dalloc(&R.hx, 8 * c->g.size())) return rc;  // two record buffers
+  if (int rc = dalloc(&R.slots, (size_t)3 * (nb + 1) * kResSlotWords)) return rc;
   R.ok = true;
   return PYOMGPU_OK;
 }
@@ -194,7 +199,7 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   const int nb = R.npx * R.npy;
   CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
   CK(cudaMemsetAsync(c->res, 0, bytes, st));
-  CK(cudaMemsetAsync(R.slots, 0xFF, (size_t)3 * (nb + 1) * 4 * sizeof(double), st));
+  CK(cudaMemsetAsync(R.slots, 0xFF, (size_t)3 * (nb + 1) * kResSlotWords * sizeof(double), st));
   CGResParams P{};
   P.g = c->g;
   P.op = c->sf.dev();
@@ -219,7 +224,8 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   P.out = c->d_result;
   void* args[] = {&P};
   CK(cudaEventRecord(c->e0, st));
-  CK(cudaLaunchCooperativeKernel(cg_res_kernel_ptr(R.p), dim3(nb), dim3(kResThreads), args, R.smem, st));
+  const bool single = c->cg_kernel == 3;  // automatic: the two-reduction form (faster at 1440 x 720)
+  CK(cudaLaunchCooperativeKernel(cg_res_kernel_ptr(R.p, single), dim3(nb), dim3(kResThreads), args, R.smem, st));
   CK(cudaEventRecord(c->e1, st));
   return finish_cg(c, info, st);
 }
@@ -903,8 +909,8 @@ int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* c, int32_t enable) {
 }
 
 int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* c, int32_t kernel) {
-  if (!c || kernel < 0 || kernel > 2) return fail(PYOMGPU_EINVAL, "set_cg_kernel: bad arguments");
-  if (kernel == 2) {
+  if (!c || kernel < 0 || kernel > 3) return fail(PYOMGPU_EINVAL, "set_cg_kernel: bad arguments");
+  if (kernel >= 2) {
     if (int rc = res_plan(c)) return rc;
     if (!c->resd.ok) return fail(PYOMGPU_EINVAL, "the grid does not fit the resident kernel");
   }

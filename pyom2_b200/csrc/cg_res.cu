@@ -88,6 +88,16 @@ __device__ __forceinline__ void publish_cyclic(double* a, const Geo& g, int i, i
   }
 }
 
+// 16 bytes global -> shared, asynchronous and not cached in L1 (both
+// addresses 16-byte aligned); completed by cp_async_wait.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+}
+
 // An integer the compiler has to treat as produced here: index arithmetic
 // derived from it is redone in each sweep instead of being hoisted out of the
 // iteration loop and held in registers for the whole solve.
@@ -158,8 +168,8 @@ struct ResCtl {
   double beta, bb, rtol2bb, betam1, betamin, step1, est, bq, alpha;
   int n, status, act, stop_after;
 };
-constexpr int kRun = 0, kDoneOk = 1, kDoneErr = 2;
-constexpr int kStepInit = 0, kStepA = 1, kStepB = 2;
+constexpr int kRun = 0, kDoneOk = 1, kDoneErr = 2, kNeedMaxp = 3;
+constexpr int kStepInit = 0, kStepA = 1, kStepB = 2, kStepInitD = 3, kStepIter = 4, kStepMaxp = 5;
 
 __device__ __forceinline__ void ctl_stop(ResCtl& C, int act, int status) {
   C.act = act;
@@ -236,6 +246,53 @@ __device__ void ctl_after_b(ResCtl& C, const CGResParams& P, const double* v) {
   ctl_begin(C, P);
 }
 
+// Single-reduction form: with u = Z res, w = A u and the previous direction
+// p' and s' = A p', the new direction p = u + bq p' has
+//   (p, A p) = (u, w) + bq ((u, s') + (p', w)) + bq^2 (p', s'),
+// the bilinear expansion of the reference's (p, Ap) (exact for any operator;
+// this one is not symmetric, so the symmetric Chronopoulos-Gear shortcut
+// (u, w) - bq beta / alpha' does not apply).  All four products come from the
+// sweep before, so one reduction per iteration carries them with (Z res, res),
+// the residual norm and max|p|.  Sets alpha, or C.act = kNeedMaxp when
+// (p, Ap) is below the reference's breakdown threshold (its estimate then needs
+// max|p| of the new direction: one more reduction).
+__device__ void ctl1_direction(ResCtl& C, const CGResParams& P, const double* e) {
+  const double F_1EM10 = (double)1.e-10f;  // solve_streamfct.f90:262, a default-real literal
+  const double sAs = C.n == 1 ? e[0] : e[0] + C.bq * (e[1] + e[2]) + C.bq * C.bq * e[3];
+  if (fabs(sAs) < fabs(C.beta) * F_1EM10) {  // :262-266
+    C.act = kNeedMaxp;
+    return;
+  }
+  C.alpha = C.beta / sAs;
+}
+
+// v = (Z res, res), (u, w), (u, s'), (p', w), (p', s'), sum res^2 over the
+// unknowns of the updated residual and max|p| of iteration n, whose update is
+// done (p', s' its direction and A-product): the reference's
+// convergence test of iteration n (solve_streamfct.f90:283-297), the relative
+// residual stop, then the start of iteration n+1.
+__device__ void ctl1_iter(ResCtl& C, const CGResParams& P, const double* v) {
+  const double step = fabs(C.alpha) * v[6];
+  if (C.n == 1) {
+    C.step1 = step;
+    C.est = step;
+    if (step < P.eps) return ctl_stop(C, kDoneOk, PYOMGPU_OK);
+  } else if (step < P.eps) {
+    const double rate = exp(log(step / C.step1) / (double)(C.n - 1));
+    C.est = step * rate / (1.0 - rate);
+    if (C.est < P.eps) return ctl_stop(C, kDoneOk, PYOMGPU_OK);
+  }
+  if (P.rtol > 0.0 && (C.bb > 0.0 ? v[5] <= C.rtol2bb : v[5] == 0.0)) {
+    C.est = sqrt(v[5]);
+    return ctl_stop(C, kDoneOk, PYOMGPU_OK);
+  }
+  C.betam1 = C.beta;
+  C.beta = v[0];
+  C.n += 1;
+  ctl_begin(C, P);
+  if (C.act == kRun) ctl1_direction(C, P, v + 1);
+}
+
 // ------------------------------------------------- reduction and exchange
 struct Halo {
   int sidx;       // shared-memory index (-1: none)
@@ -268,8 +325,8 @@ __device__ __forceinline__ void stage_one(double* spub, int pw, int ph, int lx, 
 // of a position's record, with the setcyclic_xy copies), one entry per worker
 // thread; only the edges some block reads.
 template <int NQ>
-__device__ __forceinline__ void copy_out(const CGResParams& P, const double* spub, int ilo, int ihi, int jlo, int jhi,
-                                         int wt) {
+__device__ __forceinline__ void copy_out(const CGResParams& P, double* hx, const double* spub, int ilo, int ihi,
+                                         int jlo, int jhi, int wt) {
   const Geo& g = P.g;
   const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, nent = 2 * (pw + ph);
 #pragma unroll 1
@@ -295,18 +352,18 @@ __device__ __forceinline__ void copy_out(const CGResParams& P, const double* spu
     }
     if (need) {
 #pragma unroll
-      for (int k = 0; k < NQ; k++) publish_cyclic(P.hx + k, g, i, j, spub[k * nent + e]);
+      for (int k = 0; k < NQ; k++) publish_cyclic(hx + k, g, i, j, spub[k * nent + e]);
     }
   }
 }
 
 __device__ __forceinline__ double* res_slot(const CGResParams& P, unsigned ep, int b) {
-  return P.slots + ((size_t)(ep % 3u) * P.nslot + b) * 4;
+  return P.slots + ((size_t)(ep % 3u) * P.nslot + b) * kResSlotWords;
 }
 
 // Worker side of a reduction: per-warp partials of the worker warps into wred.
 template <int NV, int kMaxSlot>
-__device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*wred)[4]) {
+__device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*wred)[kResSlotWords]) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NV; k++) {
@@ -323,7 +380,7 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // False on time-out.
 template <int NV, int kMaxSlot, int kStep>
 __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int npoll, ResCtl& C,
-                                                 const double (*wred)[4]) {
+                                                 const double (*wred)[kResSlotWords]) {
   const int lane = threadIdx.x;
   {
     double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
@@ -385,13 +442,21 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       ctl_init(C, P, out);
     else if (kStep == kStepA)
       ctl_after_a(C, P, out);
-    else
+    else if (kStep == kStepB)
       ctl_after_b(C, P, out);
+    else if (kStep == kStepInitD)
+      ctl1_direction(C, P, out);
+    else if (kStep == kStepIter)
+      ctl1_iter(C, P, out);
+    else {  // kStepMaxp: the breakdown estimate, solve_streamfct.f90:262-266
+      C.est = 100.0 * out[0];
+      ctl_stop(C, kDoneOk, PYOMGPU_OK);
+    }
     // every block has finished reading epoch ep-1 (it published epoch ep),
     // so this block's slot of that buffer (= the one of epoch ep+2) is free
     double* mine = res_slot(P, ep + 2, blockIdx.x);
 #pragma unroll
-    for (int k = 0; k < 4; k++) st_weak_f64(mine + k, empty_word());
+    for (int k = 0; k < kResSlotWords; k++) st_weak_f64(mine + k, empty_word());
   }
   return ok;
 }
@@ -417,7 +482,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
   extern __shared__ __align__(16) double sm[];
   __shared__ uint32_t s_tmem;
   __shared__ ResCtl C;
-  __shared__ double wred[kResThreads / 32][4];
+  __shared__ double wred[kResThreads / 32][kResSlotWords];
   const Geo g = Pm.g;
   const OpDev<double> op = Pm.op;
   const int warp = threadIdx.x >> 5;
@@ -573,7 +638,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
       worker_partials<4, 3>(v, wred);
     }
     workers_sync();
-    copy_out<2>(Pm, spub, ilo, ihi, jlo, jhi, wt);
+    copy_out<2>(Pm, Pm.hx, spub, ilo, ihi, jlo, jhi, wt);
     __syncthreads();                       // S1
     if (!__syncthreads_and(1)) goto out;  // S2
     if (C.act != kRun) goto done;
@@ -669,7 +734,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
             stage_one(spub + 2 * (pw + ph), pw, ph, lx, ly0 + u, s[u]);
           }
         workers_sync();
-        copy_out<2>(Pm, spub, ilo, ihi, jlo, jhi, wt);
+        copy_out<2>(Pm, Pm.hx, spub, ilo, ihi, jlo, jhi, wt);
         if (!stop_after) {
           worker_partials<2, -1>(v, wred);
           __syncthreads();  // S1
@@ -724,11 +789,408 @@ template __global__ void cg_res_kernel<4>(const __grid_constant__ CGResParams);
 template __global__ void cg_res_kernel<8>(const __grid_constant__ CGResParams);
 template __global__ void cg_res_kernel<16>(const __grid_constant__ CGResParams);
 
-const void* cg_res_kernel_ptr(int p) {
+// Single-reduction variant (one cross-block reduction per iteration) of the
+// same Jacobi-PCG, in the style of Chronopoulos and Gear but with the exact
+// expansion of (p, Ap) (ctl1_direction).  With u = Z res and w = A u, the
+// sweep of iteration n does
+//   p = u + bq p,  s = w + bq s  (= A p),  res -= alpha s,  u = Z res,
+//   then w = A u (stencil),  sol += alpha p,
+// and one reduction returns (u, res), (u, w), (u, s), (p, w), (p, s),
+// |res|^2 over the unknowns and max|p|.  The reference's (p, Ap) and its
+// convergence test of iteration n (which needs max|p| of that iteration) are
+// evaluated at that reduction, so every stop leaves sol and res where the
+// reference's control flow leaves them; in exact arithmetic the iterates are
+// the reference's, in floating point they differ at rounding level (A p by
+// recurrence, (p, Ap) by expansion).  Per point the block keeps res, sol, Z and w in TMEM (all 128
+// columns of a thread) and p, s in registers; the exchange records carry
+// (res, w, s) of the boundary points, from which the neighbour's next u on
+// the halo is recomputed with its owner's operations (records double-buffered,
+// as each sweep has only one reduction between a write and the next).
+template <int P>
+__global__ void __launch_bounds__(kResThreads, 1) cg_res1_kernel(const __grid_constant__ CGResParams Pm) {
+  constexpr int CH = 4;       // points per TMEM chunk (tcgen05 .x8)
+  constexpr int NC = P / CH;  // chunks per field
+  constexpr int CW = 2 * CH;  // TMEM columns per chunk
+  static_assert(P % CH == 0 && NC * CW <= 32, "a field takes at most 32 TMEM columns per thread");
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint32_t s_tmem;
+  __shared__ ResCtl C;
+  __shared__ double wred[kResThreads / 32][kResSlotWords];
+  const Geo g = Pm.g;
+  const OpDev<double> op = Pm.op;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    tc::tmem_alloc(&s_tmem, 512);
+    tc::tmem_relinquish();
+  }
+
+  const int nb = gridDim.x;
+  const int px = blockIdx.x % Pm.npx, py = blockIdx.x / Pm.npx;
+  const int ilo = 1 + (int)(((long long)px * g.nx) / Pm.npx);
+  const int ihi = (int)(((long long)(px + 1) * g.nx) / Pm.npx);
+  const int jlo = 1 + (int)(((long long)py * g.ny) / Pm.npy);
+  const int jhi = (int)(((long long)(py + 1) * g.ny) / Pm.npy);
+  const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, sp = pw + 2;
+  const int pw_ = pw, ph_ = ph;
+  double* ss = sm;                    // (pw+2) x (ph+2): u = Z res, halo included
+  double* sfx = ss + sp * (ph + 2);   // (pw+1) x ph: FX(ilo+lx, j), lx = 0..pw
+  double* sfy = sfx + (pw + 1) * ph;  // pw x (ph+1): FY(i, jlo+ly), ly = 0..ph
+  double* sbx = sfy + pw * (ph + 1);  // ph: bx(jlo+ly), then ph: by(jlo+ly)
+  double* spub = sbx + 2 * ph;        // 3 x 2(pw+ph): staged boundary res, w, s
+  const int nent = 2 * (pw + ph);
+  double* shalo = reinterpret_cast<double*>(  // 2(pw+ph) x 4: received exchange records, 16-byte aligned
+      (reinterpret_cast<uintptr_t>(spub + 3 * nent) + 15) & ~(uintptr_t)15);
+
+  for (int e = threadIdx.x; e < sp * (ph + 2); e += kResThreads) ss[e] = 0.0;
+  for (int e = threadIdx.x; e < (pw + 1) * ph; e += kResThreads)
+    sfx[e] = op.FX[g.at(ilo + e % (pw + 1), jlo + e / (pw + 1))];
+  for (int e = threadIdx.x; e < pw * (ph + 1); e += kResThreads) sfy[e] = op.FY[g.at(ilo + e % pw, jlo + e / pw)];
+  for (int e = threadIdx.x; e < ph; e += kResThreads) {
+    sbx[e] = op.bx[jlo + e + 1];
+    sbx[ph + e] = op.by[jlo + e + 1];
+  }
+  for (int e = threadIdx.x; e < 3 * nent; e += kResThreads) spub[e] = 0.0;
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+
+  if (warp == 0) {
+    // ============================================================ controller
+    unsigned ep = 0;
+    __syncthreads();  // S1: init partials
+    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred);
+    if (!__syncthreads_and(ok)) goto out;  // S2
+    if (C.act == kRun) {
+      __syncthreads();  // S1: delta of the first direction
+      ok = controller_epoch<2, -1, kStepInitD>(Pm, ++ep, nb, C, wred);
+      if (!__syncthreads_and(ok)) goto out;  // S2
+      while (C.act == kRun) {
+        __syncthreads();  // S1: partials of one sweep
+        ok = controller_epoch<7, 6, kStepIter>(Pm, ++ep, nb, C, wred);
+        if (!__syncthreads_and(ok)) goto out;  // S2
+      }
+      if (C.act == kNeedMaxp) {
+        __syncthreads();  // S1: max|p| of the new direction
+        ok = controller_epoch<2, 0, kStepMaxp>(Pm, ++ep, nb, C, wred);
+        if (!__syncthreads_and(ok)) goto out;  // S2
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const int converged = C.act == kDoneOk;
+      Pm.out->iterations = C.n;
+      Pm.out->converged = converged;
+      Pm.out->status = converged ? PYOMGPU_OK : (C.est != C.est ? PYOMGPU_NAN : C.status);
+      Pm.out->est = C.est;
+    }
+  } else {
+    // =============================================================== workers
+    const int wt = (int)threadIdx.x - 32;
+    const int lx_ = wt % Pm.wmax;
+    const int ly0_ = (wt / Pm.wmax) * P;
+    const int nrow_ = (lx_ < pw && ly0_ < ph) ? min(P, ph - ly0_) : 0;
+    const int i_ = ilo + lx_;
+    int lx = lx_, ly0 = ly0_, nrow = nrow_;
+    const int i = i_;
+    const double axi = nrow_ > 0 ? op.ax[i_ + 1] : 0.0;
+    const uint32_t tm = s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * (warp >> 2));
+    const uint32_t t_res = tm, t_sol = tm + 32, t_z = tm + 64, t_w = tm + 96;
+
+    // halo positions received (record wt + e*kResWorkers of shalo), with Z of the source point
+    struct {
+      int sidx, gidx;
+      double z;
+    } hl[2];
+    {
+      const int nW = (ilo > 1 || g.cyclic_x) ? ph : 0, nE = (ihi < g.nx || g.cyclic_x) ? ph : 0;
+      const int nS = (jlo > 1 || g.cyclic_y) ? pw : 0, nN = (jhi < g.ny || g.cyclic_y) ? pw : 0;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int h = wt + e * kResWorkers;
+        hl[e].sidx = -1;
+        hl[e].gidx = 0;
+        hl[e].z = 0.0;
+        if (h >= nW + nE + nS + nN) continue;
+        int hx, hy;
+        if (h < nW) {
+          hx = -1;
+          hy = h;
+        } else if (h < nW + nE) {
+          hx = pw;
+          hy = h - nW;
+        } else if (h < nW + nE + nS) {
+          hx = h - nW - nE;
+          hy = -1;
+        } else {
+          hx = h - nW - nE - nS;
+          hy = ph;
+        }
+        hl[e].sidx = (hy + 1) * sp + hx + 1;
+        hl[e].gidx = (int)g.at(ilo + hx, jlo + hy);
+        int si = ilo + hx, sj = jlo + hy;  // the interior point the halo position copies
+        if (si < 1) si += g.nx;
+        if (si > g.nx) si -= g.nx;
+        if (sj < 1) sj += g.ny;
+        if (sj > g.ny) sj -= g.ny;
+        hl[e].z = op.W[g.at(si, sj)];
+      }
+    }
+
+    double p[P], s[P];  // direction and A p
+    // Exchange records alternate between two buffers by reduction parity: a
+    // record written before reduction e is rewritten only before e+2, which
+    // needs every reader's slot of e+1, published after its loads returned.
+    unsigned wep = 0;  // reduction the next copy-out precedes
+    auto xbuf = [&](unsigned e) { return Pm.hx + (size_t)(e & 1u) * 4 * (size_t)Pm.hsize; };
+
+    // w = A u on this thread's points (u = Z res in ss, halo included) into
+    // TMEM and the boundary staging; adds the partials (w, u) and (p, w)
+    auto stencil = [&](double& delta, double& pw_dot) {
+      const int lx = opaque(lx_), ly0 = opaque(ly0_), nrow = opaque(nrow_);
+      const int pw = opaque(pw_), ph = opaque(ph_), sp = pw + 2;
+      double fys = 0.0, uc = 0.0, us = 0.0;
+      if (nrow > 0) {
+        fys = sfy[ly0 * pw + lx];
+        uc = ss[(ly0 + 1) * sp + lx + 1];
+        us = ss[ly0 * sp + lx + 1];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        uint32_t bw[CW];
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+          const int u = c * CH + k;
+          double a = 0.0;
+          if (u < nrow) {
+            const int ly = ly0 + u;
+            const int kk = (ly + 1) * sp + lx + 1;
+            const double ue = ss[kk + 1], uw = ss[kk - 1], un = ss[kk + sp];
+            const double fxw = sfx[ly * (pw + 1) + lx], fxe = sfx[ly * (pw + 1) + lx + 1];
+            const double fyn = sfy[(ly + 1) * pw + lx];
+            a = axi * sbx[ly] * (fxe * (ue - uc) + fxw * (uw - uc)) +
+                sbx[ph + ly] * (fyn * (un - uc) + fys * (us - uc));
+            delta += a * uc;
+            pw_dot += p[u] * a;
+            stage_one(spub + 2 * (pw + ph), pw, ph, lx, ly, a);
+            fys = fyn;
+            us = uc;
+            uc = un;
+          }
+          col_put(bw, k, a);
+        }
+        tm_st<CW>(t_w + c * CW, bw);
+      }
+      tm_wait_st();
+    };
+
+    // ---------------------------------------------------------------- init
+    // res = forc - A sol, solve_streamfct.f90:196-201; u = Z res
+    {
+      double v[4] = {0.0, 0.0, 0.0, 0.0};  // (Z res, res), bb, rr, max|Z res|
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        uint32_t br[CW], bz[CW], bx[CW];
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+          const int u = c * CH + k;
+          double rv = 0.0, w = 0.0, x = 0.0;
+          p[u] = 0.0;
+          s[u] = 0.0;
+          if (u < nrow) {
+            const int ly = ly0 + u, j = jlo + ly;
+            const double f = Pm.forc[fidx(g.nx, i, j)];
+            rv = f - apply_point(op, g, Pm.sol, i, j);
+            w = op.W[g.at(i, j)];
+            x = Pm.sol[g.at(i, j)];
+            const double zr = w * rv;
+            v[0] += zr * rv;
+            if (w != 0.0) {
+              v[1] += f * f;
+              v[2] += rv * rv;
+            }
+            v[3] = fmax(v[3], fabs(zr));
+            ss[(ly + 1) * sp + lx + 1] = zr;
+            stage_one(spub, pw, ph, lx, ly, rv);
+          }
+          col_put(br, k, rv);
+          col_put(bz, k, w);
+          col_put(bx, k, x);
+        }
+        tm_st<CW>(t_res + c * CW, br);
+        tm_st<CW>(t_z + c * CW, bz);
+        tm_st<CW>(t_sol + c * CW, bx);
+      }
+      tm_wait_st();
+      worker_partials<4, 3>(v, wred);
+    }
+    workers_sync();
+    copy_out<3>(Pm, xbuf(wep), spub, ilo, ihi, jlo, jhi, wt);
+    __syncthreads();                       // S1
+    if (!__syncthreads_and(1)) goto out;  // S2
+    if (C.act != kRun) goto done;
+    // u on the halo (Z res of the neighbours), then w = A u and delta of the first direction
+#pragma unroll
+    for (int e = 0; e < 2; e++)
+      if (hl[e].sidx >= 0) ss[hl[e].sidx] = hl[e].z * __ldcg(xbuf(wep) + 4 * (long long)hl[e].gidx);
+    ++wep;
+    workers_sync();
+    {
+      double v[2] = {0.0, 0.0};
+      double unused = 0.0;
+      stencil(v[0], unused);
+      worker_partials<2, -1>(v, wred);
+    }
+    workers_sync();
+    copy_out<3>(Pm, xbuf(wep), spub, ilo, ihi, jlo, jhi, wt);
+    __syncthreads();                       // S1
+    if (!__syncthreads_and(1)) goto out;  // S2
+
+    for (;;) {
+      if (C.act == kNeedMaxp) {
+        // the breakdown estimate needs max|p| of the direction that was to be used
+        double v[2] = {0.0, 0.0};
+        const double bq = C.bq;
+        nrow = opaque(nrow_);
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          uint32_t br[CW], bz[CW];
+          tm_ld<CW>(t_res + c * CW, br);
+          tm_ld<CW>(t_z + c * CW, bz);
+          tm_wait_ld();
+#pragma unroll
+          for (int k = 0; k < CH; k++) {
+            const int u = c * CH + k;
+            if (u < nrow) v[0] = fmax(v[0], fabs(col_get(bz, k) * col_get(br, k) + bq * p[u]));
+          }
+        }
+        worker_partials<2, 0>(v, wred);
+        __syncthreads();                       // S1
+        if (!__syncthreads_and(1)) goto out;  // S2
+        goto done;
+      }
+      if (C.act != kRun) goto done;
+      // ------------------------------------------------- update and u = Z res
+      lx = opaque(lx_);
+      ly0 = opaque(ly0_);
+      nrow = opaque(nrow_);
+      const double alpha = C.alpha, bq = C.bq;
+      // the neighbours' (res, w, s) records land in shared memory during the update
+#pragma unroll
+      for (int e = 0; e < 2; e++)
+        if (hl[e].sidx >= 0) {
+          const double* src = xbuf(wep) + 4 * (long long)hl[e].gidx;
+          double* dst = shalo + 4 * (wt + e * kResWorkers);
+          cp_async16(dst, src);
+          cp_async16(dst + 2, src + 2);
+        }
+      // (u, res), (u, w), (u, s), (p, w), (p, s), rr, max|p| of the new u, w and this sweep's p, s
+      double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      {
+        const int pw = opaque(pw_), ph = opaque(ph_), sp = pw + 2;
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          {
+            uint32_t bw[CW];
+            tm_ld<CW>(t_w + c * CW, bw);
+            tm_wait_ld();
+#pragma unroll
+            for (int k = 0; k < CH; k++) s[c * CH + k] = col_get(bw, k) + bq * s[c * CH + k];
+          }
+          uint32_t br[CW], bz[CW];
+          tm_ld<CW>(t_res + c * CW, br);
+          tm_ld<CW>(t_z + c * CW, bz);
+          tm_wait_ld();
+#pragma unroll
+          for (int k = 0; k < CH; k++) {
+            const int u = c * CH + k;
+            if (u < nrow) {
+              const int ly = ly0 + u;
+              const double z = col_get(bz, k);
+              const double uo = z * col_get(br, k);
+              p[u] = uo + bq * p[u];
+              const double rv = col_get(br, k) - alpha * s[u];
+              const double un = z * rv;
+              ss[(ly + 1) * sp + lx + 1] = un;
+              v[0] += un * rv;
+              v[2] += un * s[u];
+              v[4] += p[u] * s[u];
+              if (z != 0.0) v[5] += rv * rv;
+              v[6] = fmax(v[6], fabs(p[u]));
+              col_put(br, k, rv);
+              stage_one(spub, pw, ph, lx, ly, rv);
+              stage_one(spub + 4 * (pw + ph), pw, ph, lx, ly, s[u]);
+            }
+          }
+          tm_st<CW>(t_res + c * CW, br);
+        }
+      }
+      cp_async_wait();
+#pragma unroll
+      for (int e = 0; e < 2; e++)
+        if (hl[e].sidx >= 0) {
+          const double* rec = shalo + 4 * (wt + e * kResWorkers);
+          const double sh = rec[1] + bq * rec[2];
+          ss[hl[e].sidx] = hl[e].z * (rec[0] - alpha * sh);
+        }
+      workers_sync();
+      stencil(v[1], v[3]);
+      worker_partials<7, 6>(v, wred);
+      workers_sync();
+      ++wep;
+      copy_out<3>(Pm, xbuf(wep), spub, ilo, ihi, jlo, jhi, wt);
+      __syncthreads();  // S1
+      // sol += alpha p (solve_streamfct.f90:278), while the other blocks finish
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        uint32_t bx[CW];
+        tm_ld<CW>(t_sol + c * CW, bx);
+        tm_wait_ld();
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+          const int u = c * CH + k;
+          if (u < nrow) col_put(bx, k, col_get(bx, k) + alpha * p[u]);
+        }
+        tm_st<CW>(t_sol + c * CW, bx);
+      }
+      tm_wait_st();
+      if (!__syncthreads_and(1)) goto out;  // S2
+    }
+
+  done:
+    // the residual and solution of the last iterate back to global memory
+    nrow = opaque(nrow_);
+    ly0 = opaque(ly0_);
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      uint32_t br[CW], bx[CW];
+      tm_ld<CW>(t_res + c * CW, br);
+      tm_ld<CW>(t_sol + c * CW, bx);
+      tm_wait_ld();
+#pragma unroll
+      for (int k = 0; k < CH; k++) {
+        const int u = c * CH + k;
+        if (u < nrow) {
+          const int j = jlo + ly0 + u;
+          store_cyclic(Pm.res, g, i, j, col_get(br, k));
+          Pm.sol[g.at(i, j)] = col_get(bx, k);
+        }
+      }
+    }
+  }
+out:
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(s_tmem, 512);
+}
+
+template __global__ void cg_res1_kernel<4>(const __grid_constant__ CGResParams);
+template __global__ void cg_res1_kernel<8>(const __grid_constant__ CGResParams);
+template __global__ void cg_res1_kernel<16>(const __grid_constant__ CGResParams);
+
+const void* cg_res_kernel_ptr(int p, bool single) {
   switch (p) {
-    case 4: return (const void*)cg_res_kernel<4>;
-    case 8: return (const void*)cg_res_kernel<8>;
-    case 16: return (const void*)cg_res_kernel<16>;
+    case 4: return single ? (const void*)cg_res1_kernel<4> : (const void*)cg_res_kernel<4>;
+    case 8: return single ? (const void*)cg_res1_kernel<8> : (const void*)cg_res_kernel<8>;
+    case 16: return single ? (const void*)cg_res1_kernel<16> : (const void*)cg_res_kernel<16>;
     default: return nullptr;
   }
 }

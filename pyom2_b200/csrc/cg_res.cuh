@@ -8,6 +8,7 @@ namespace pyomgpu {
 constexpr int kResThreads = 512;
 constexpr int kResWorkers = kResThreads - 32;  // warps 1-15 own the points; warp 0 runs the reductions
 constexpr int kResMaxSlots = 160;              // reduction slots warp 0 polls (blocks + 1)
+constexpr int kResSlotWords = 8;               // words per reduction slot (at most 7 partial sums)
 // Points per thread along a column segment (template instances of the kernel).
 constexpr int kResP[] = {4, 8, 16};
 constexpr int kResNP = 3;
@@ -22,9 +23,11 @@ struct CGResParams {
   const double* forc;  // Fortran layout (ld nx+4), device
   double* sol;         // padded, halo valid on entry; interior updated
   double* res;         // padded; the residual of the last iterate on exit (with setcyclic copies)
-  double* hx;          // halo exchange: a 4-word record per padded position (Z*res, direction)
+  double* hx;          // halo exchange: a 4-word record per padded position, (Z*res, direction) for
+                       // the two-reduction kernel, (res, A Z res, A p) in two alternating buffers
+                       // (8 words per position) for the single-reduction one
   long long hsize;     // padded positions (records)
-  double* slots;       // 3 buffers x nslot x 4 reduction words, all empty on entry
+  double* slots;       // 3 buffers x nslot x kResSlotWords reduction words, all empty on entry
   int nslot;           // gridDim.x + 1
   int npx, npy;        // pieces in x and y (gridDim.x = npx * npy)
   int wmax, hmax;      // largest piece extents: shared-memory layout and thread columns
@@ -37,17 +40,22 @@ struct CGResParams {
   CGResult* out;
 };
 
-// Dynamic shared memory of a w x h piece: the direction with its one-cell
-// halo, the x- and y-face couplings, the row factors bx, by and the staged
-// boundary values (2 per boundary entry).
+// Dynamic shared memory of a w x h piece (the larger of the two kernels'
+// needs): the stencil operand with its one-cell halo, the x- and y-face
+// couplings, the row factors bx, by, the staged boundary values (up to 3 per
+// boundary entry) and the received halo records (4 words each, 16-byte
+// aligned, single-reduction kernel).
 __host__ __device__ constexpr size_t res_smem_bytes(int w, int h) {
-  return 8 * ((size_t)(w + 2) * (h + 2) + (size_t)(w + 1) * h + (size_t)w * (h + 1) + 2 * (size_t)h +
-              4 * (size_t)(w + h));
+  return 8 * ((((size_t)(w + 2) * (h + 2) + (size_t)(w + 1) * h + (size_t)w * (h + 1) + 2 * (size_t)h +
+                6 * (size_t)(w + h)) + 1) / 2 * 2 + 8 * (size_t)(w + h));
 }
 
 // Threads that a w x h piece needs with p points per thread.
 __host__ __device__ constexpr int res_threads(int w, int h, int p) { return w * ((h + p - 1) / p); }
 
-const void* cg_res_kernel_ptr(int p);
+// The resident kernel for p points per thread: two reductions per iteration
+// (the reference's recurrences) or one (single = true: A p by recurrence and
+// (p, Ap) by its exact expansion in products of the sweep before).
+const void* cg_res_kernel_ptr(int p, bool single);
 
 }  // namespace pyomgpu

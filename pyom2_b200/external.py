@@ -151,14 +151,20 @@ class ExternalMode:
     def set_cg_kernel(self, kernel: str = "auto"):
         """CG kernel of the streamfunction solves: ``"tiled"`` (any grid),
         ``"resident"`` (one piece of the grid per SM, held on chip for the
-        whole solve; raises on a grid that does not fit) or ``"auto"``."""
-        code = {"auto": 0, "tiled": 1, "resident": 2}[kernel]
+        whole solve, two reductions per iteration as the reference),
+        ``"resident1"`` (the same with one reduction per iteration) or
+        ``"auto"``; the resident ones raise on a grid that does not fit."""
+        code = {"auto": 0, "tiled": 1, "resident": 2, "resident1": 3}[kernel]
         _abi.check(self._L.pyomgpu_set_cg_kernel(self._ctx, code))
+        self._cg_kernel = kernel
 
     def resident_kernel_name(self):
-        """Name of the resident kernel instance the automatic choice launches."""
+        """Name of the resident kernel instance the current choice launches."""
         lay = self.resident_layout()
-        return None if lay is None else f"cg_res_kernel<{lay[2]}>"
+        if lay is None:
+            return None
+        single = getattr(self, "_cg_kernel", "auto") == "resident1"
+        return f"cg_res{'1' if single else ''}_kernel<{lay[2]}>"
 
     def resident_layout(self):
         """(pieces in x, pieces in y, points per thread) of the resident

@@ -1,4 +1,6 @@
-"""The on-chip-resident streamfunction CG kernel (csrc/cg_res.cu) against the
+"""The on-chip-resident streamfunction CG kernels (csrc/cg_res.cu: two
+reductions per iteration, and one with A p by recurrence and (p, Ap) by its
+exact expansion) against the
 CPU oracle and against the tiled kernel (csrc/cg_ref.cu) on the same inputs.
 
 Tolerances: both kernels run congrad_streamfunction's algorithm in FP64 with
@@ -15,6 +17,15 @@ from pyom2_b200.external import ExternalMode
 pytestmark = pytest.mark.gpu
 
 RTOL_SOL = 1e-10
+
+
+def it_tol(kernel, it_ref):
+    """Iteration-count tolerance: the kernels with the reference's recurrences
+    stop within one iteration of the oracle; the single-reduction form computes
+    A p by recurrence and (p, Ap) by expansion, so its iterates drift at rounding level and the
+    reference's extrapolated stopping estimate may cross its threshold a few
+    iterations apart (the converged solution is held to RTOL_SOL all the same)."""
+    return max(3, it_ref // 100) if kernel == "resident1" else 1
 
 
 def rel(a, b, mask=None):
@@ -46,7 +57,7 @@ def setup(name, oracle_lib, kernel):
     return W, O, E
 
 
-@pytest.mark.parametrize("kernel", ["resident", "tiled"])
+@pytest.mark.parametrize("kernel", ["resident1", "resident", "tiled"])
 @pytest.mark.parametrize("name", list(WORLDS))
 def test_congrad_streamfunction_matches_oracle(oracle_lib, name, kernel):
     W, O, E = setup(name, oracle_lib, kernel)
@@ -57,8 +68,10 @@ def test_congrad_streamfunction_matches_oracle(oracle_lib, name, kernel):
     ro = O.congrad_streamfunction(cf, W.forc, so)
     sg = sol0.copy(order="F")
     it, conv, info = E.congrad_streamfunction(W.forc, sg)
-    assert conv == ro["converged"] and abs(it - ro["iterations"]) <= 1, (it, ro["iterations"])
+    print(f"{name} {kernel}: iterations {it} (oracle {ro['iterations']}), rel {rel(sg, so):.2e}")
     assert rel(sg, so) < RTOL_SOL
+    assert conv == ro["converged"] and abs(it - ro["iterations"]) <= it_tol(kernel, ro["iterations"]), (
+        it, ro["iterations"])
     # halo as the reference leaves it (set once at entry)
     assert rel(sg[:2], so[:2]) < RTOL_SOL or np.array_equal(sg[:2], so[:2])
 
@@ -76,30 +89,34 @@ def test_solve_rtol_resident(oracle_lib, name):
 
 def test_headline_grid_layout_and_kernels_agree():
     """1440 x 720 (20 islands): 37 x 4 pieces of at most 39 x 180 points, 16
-    points per thread; the resident and tiled kernels reach the same solution
-    and the same iteration count within one."""
+    points per thread; the resident kernels (two reductions and one per
+    iteration) and the tiled kernel reach the same solution and the same
+    iteration count within one."""
     W = synth.config1()
     E = ExternalMode(W.M)
     E.streamfunction_init(maxipp=10**6, maxq=10**6)
     assert E.resident_layout() == (37, 4, 16)
     out = {}
-    for kernel in ("tiled", "resident"):
+    for kernel in ("tiled", "resident", "resident1"):
         E.set_cg_kernel(kernel)
         sol = np.zeros(W.M.shape2d, order="F")
         info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=_abi.PREC_F64)
         assert info["status"] == 0 and info["rel_residual"] <= 1e-10, (kernel, info)
         out[kernel] = (sol, info)
-    (st, it_t), (sr, it_r) = [(out[k][0], out[k][1]) for k in ("tiled", "resident")]
-    assert abs(it_t["iterations"] - it_r["iterations"]) <= 1
-    assert rel(sr, st) < 1e-8
-    print("1440x720 device ms: tiled %.2f, resident %.2f" % (it_t["device_ms"], it_r["device_ms"]))
+    st, it_t = out["tiled"]
+    for kernel in ("resident", "resident1"):
+        sr, it_r = out[kernel]
+        assert abs(it_t["iterations"] - it_r["iterations"]) <= it_tol(kernel, it_t["iterations"]), kernel
+        assert rel(sr, st) < 1e-8, kernel
+    print("1440x720 device ms: " + ", ".join(f"{k} {out[k][1]['device_ms']:.2f}" for k in out))
 
 
-def test_reruns_are_bit_identical():
+@pytest.mark.parametrize("kernel", ["resident1", "resident"])
+def test_reruns_are_bit_identical(kernel):
     W = WORLDS["cyclic200"]()
     E = ExternalMode(W.M)
     E.streamfunction_init(maxipp=10**6, maxq=10**6)
-    E.set_cg_kernel("resident")
+    E.set_cg_kernel(kernel)
     a = np.zeros(W.M.shape2d, order="F")
     b = np.zeros(W.M.shape2d, order="F")
     ia = E.congrad_streamfunction(W.forc, a)[0]
@@ -107,7 +124,7 @@ def test_reruns_are_bit_identical():
     assert ia == ib and np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("kernel", ["resident", "tiled"])
+@pytest.mark.parametrize("kernel", ["resident1", "resident", "tiled"])
 def test_status_paths(oracle_lib, kernel):
     W, O, E = setup("c0", oracle_lib, kernel)
     bad = W.forc.copy(order="F")
