@@ -34,8 +34,10 @@ METRIC = "ms/solve to FP64 rel. residual 1e-10: learned FCG vs plain PCG, 1 B200
 RTOL = 1e-10
 BYTES_PER_POINT_ITER = {"f64": 72, "f32": 36}  # algorithmic bytes, plain PCG iteration
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of this
-# workload (profiles/cg_ref_kernel_c1_1440x720.md), per iteration, keyed by kernel
-MEASURED_TRAFFIC_PER_ITER = {"cg_ref_kernel<false>": (3.47840256e8 + 1.744509e9) / 1760}
+# workload (profiles/cg_ref_kernel_c1_1440x720.md, profiles/cg_res_kernel_c1_1440x720.md),
+# per iteration, keyed by kernel
+MEASURED_TRAFFIC_PER_ITER = {"cg_ref_kernel<false>": (3.47840256e8 + 1.744509e9) / 1760,
+                             "cg_res_kernel<16>": (4.7075072e7 + 8.87296e5) / 1760}
 CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
            "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
