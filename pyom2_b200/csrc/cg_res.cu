@@ -88,6 +88,20 @@ __device__ __forceinline__ void publish_cyclic(double* a, const Geo& g, int i, i
   }
 }
 
+__device__ __forceinline__ void st_release_cta_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_cta_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_relaxed_cta_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+
 // 16 bytes global -> shared, asynchronous and not cached in L1 (both
 // addresses 16-byte aligned); completed by cp_async_wait.
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
@@ -380,7 +394,7 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // False on time-out.
 template <int NV, int kMaxSlot, int kStep>
 __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int npoll, ResCtl& C,
-                                                 const double (*wred)[kResSlotWords]) {
+                                                 const double (*wred)[kResSlotWords], unsigned* hflag = nullptr) {
   const int lane = threadIdx.x;
   {
     double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
@@ -428,6 +442,12 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       break;
     }
   }
+  if (hflag != nullptr) {
+    // every slot is acquired, so the exchange records released with them are
+    // visible: let the workers start loading their halo before the control step
+    __syncwarp();
+    if (lane == 0) st_release_cta_u32(hflag, ld_relaxed_cta_u32(hflag) + 1u);
+  }
   double out[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) {
@@ -461,6 +481,21 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
   return ok;
 }
 
+// Waits (bounded) until the controller has acquired every slot of the
+// reduction carrying the halo records (hflag reaches target), then loads them.
+// False on time-out.
+__device__ __forceinline__ bool worker_halo_early(const CGResParams& P, const unsigned* hflag, unsigned target,
+                                                  Halo (&hl)[2]) {
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned spin = 1; ld_acquire_cta_u32(hflag) < target; spin++)
+    if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
+      atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+      return false;
+    }
+  worker_halo_load(P, hl);
+  return true;
+}
+
 __device__ __forceinline__ void workers_sync() {
   asm volatile("bar.sync 1, %0;" ::"r"(kResWorkers) : "memory");
 }
@@ -483,6 +518,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
   __shared__ uint32_t s_tmem;
   __shared__ ResCtl C;
   __shared__ double wred[kResThreads / 32][kResSlotWords];
+  __shared__ unsigned s_hflag;  // reductions whose halo records the workers may load
   const Geo g = Pm.g;
   const OpDev<double> op = Pm.op;
   const int warp = threadIdx.x >> 5;
@@ -490,6 +526,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     tc::tmem_alloc(&s_tmem, 512);
     tc::tmem_relinquish();
   }
+  if (threadIdx.x == 0) s_hflag = 0u;
 
   const int nb = gridDim.x;
   const int px = blockIdx.x % Pm.npx, py = blockIdx.x / Pm.npx;
@@ -523,7 +560,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     unsigned ep = 0;
     bool stopped_after_update = false;  // the stop decided before sweep B (C stays as the workers read it)
     __syncthreads();  // S1
-    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred);
+    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred, &s_hflag);
     if (!__syncthreads_and(ok)) goto out;  // S2
     if (C.act == kRun) {
       for (;;) {
@@ -536,7 +573,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           break;
         }
         __syncthreads();  // S1: partials of sweep B
-        ok = controller_epoch<2, -1, kStepB>(Pm, ++ep, nb, C, wred);
+        ok = controller_epoch<2, -1, kStepB>(Pm, ++ep, nb, C, wred, &s_hflag);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
       }
@@ -595,6 +632,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     }
 
     double s[P], q[P];  // direction; q: Z*res before sweep A, As after it
+    unsigned hready = 0;  // halo-carrying reductions completed
 
     // ---------------------------------------------------------------- init
     // res = forc - A sol, solve_streamfct.f90:196-201
@@ -639,10 +677,9 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     }
     workers_sync();
     copy_out<2>(Pm, Pm.hx, spub, ilo, ihi, jlo, jhi, wt);
-    __syncthreads();                       // S1
-    if (!__syncthreads_and(1)) goto out;  // S2
+    __syncthreads();  // S1
+    if (!__syncthreads_and(worker_halo_early(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
     if (C.act != kRun) goto done;
-    worker_halo_load(Pm, hl);
 
     for (;;) {
       // ---------------------------------------------- sweep A: direction, As
@@ -755,9 +792,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         tm_wait_st();
         if (stop_after) goto done;
       }
-      if (!__syncthreads_and(1)) goto out;  // S2
+      if (!__syncthreads_and(worker_halo_early(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
       if (C.act != kRun) goto done;
-      worker_halo_load(Pm, hl);
     }
 
   done:
