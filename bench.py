@@ -58,10 +58,17 @@ class ClockSampler:
         self.p = None
 
     def __enter__(self):
+        # nvidia-smi takes a while to start: wait (at most 5 s) for its first line, and keep only
+        # the lines written after it, so every kept sample falls inside the timed region
+        self.start = 0
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={CLOCK_Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.f.name) == 0 and self.p.poll() is None:
+                time.sleep(0.01)
+            self.start = os.path.getsize(self.f.name)
         except Exception:
             self.p = None
         return self
@@ -78,7 +85,10 @@ class ClockSampler:
         self.f.flush()
         rows = []
         try:
-            for line in open(self.f.name):
+            with open(self.f.name) as fh:
+                fh.seek(self.start)
+                lines = fh.read().splitlines()
+            for line in lines:
                 parts = [x.strip() for x in line.split(",")]
                 if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
                     rows.append(parts)
