@@ -162,8 +162,8 @@ int32_t pyomgpu_inject_barrier_stall(pyomgpu_ctx* ctx, int32_t enable);
  *     recurrence and the reference's (p, Ap) by its exact bilinear expansion
  *     in products of the sweep before; the reference's stopping tests are
  *     evaluated one reduction later, on the same quantities),
- * 0 = automatic (2 wherever the grid fits: at 1440 x 720 it is faster than 3,
- *     whose seven-term reductions and register spills outweigh the saved one).  PYOMGPU_EINVAL for 2 or 3 on a
+ * 0 = automatic (2 wherever the grid fits: the reference's own recurrences;
+ *     at 1440 x 720 3 runs on par with it).  PYOMGPU_EINVAL for 2 or 3 on a
  * grid that does not fit.  The surface-pressure solve always uses 1.
  * Reduction order and recurrences differ between the kernels: results
  * change at rounding level. */

@@ -224,7 +224,7 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   P.out = c->d_result;
   void* args[] = {&P};
   CK(cudaEventRecord(c->e0, st));
-  const bool single = c->cg_kernel == 3;  // automatic: the two-reduction form (faster at 1440 x 720)
+  const bool single = c->cg_kernel == 3;  // automatic: the two-reduction form (the reference's recurrences)
   CK(cudaLaunchCooperativeKernel(cg_res_kernel_ptr(R.p, single), dim3(nb), dim3(kResThreads), args, R.smem, st));
   CK(cudaEventRecord(c->e1, st));
   return finish_cg(c, info, st);

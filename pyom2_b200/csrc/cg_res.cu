@@ -403,12 +403,16 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       const double x = (lane >= 1 && lane < kResThreads / 32) ? wred[lane][k] : 0.0;
       t[k] = (k == kMaxSlot) ? warp_max(x) : warp_sum(x);
     }
-    if (lane == 0) {
-      double* mine = res_slot(P, ep, blockIdx.x);
+    // one word per lane (a lone lane's stores go out one after another); the
+    // last word, released after a warp barrier, makes the others visible
+    double* mine = res_slot(P, ep, blockIdx.x);
+    double mv = 0.0;
 #pragma unroll
-      for (int k = 0; k < NV - 1; k++) st_weak_f64(mine + k, sendable(t[k]));
-      st_release_f64(mine + NV - 1, sendable(t[NV - 1]));
-    }
+    for (int k = 0; k < NV; k++)
+      if (lane == k) mv = t[k];
+    if (lane < NV - 1) st_weak_f64(mine + lane, sendable(mv));
+    __syncwarp();
+    if (lane == NV - 1) st_release_f64(mine + NV - 1, sendable(mv));
   }
   constexpr int kPer = kResMaxSlots / 32;
   double got[kPer][NV];
@@ -448,6 +452,12 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
     __syncwarp();
     if (lane == 0) st_release_cta_u32(hflag, ld_relaxed_cta_u32(hflag) + 1u);
   }
+  // once every lane has seen its slots of epoch ep, every block has finished
+  // reading epoch ep-1 (it published epoch ep), so this block's slot of that
+  // buffer (= the one of epoch ep+2) is free; the next publication's release
+  // orders these stores before it
+  __syncwarp();
+  if (lane < kResSlotWords) st_weak_f64(res_slot(P, ep + 2, blockIdx.x) + lane, empty_word());
   double out[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) {
@@ -472,11 +482,6 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       C.est = 100.0 * out[0];
       ctl_stop(C, kDoneOk, PYOMGPU_OK);
     }
-    // every block has finished reading epoch ep-1 (it published epoch ep),
-    // so this block's slot of that buffer (= the one of epoch ep+2) is free
-    double* mine = res_slot(P, ep + 2, blockIdx.x);
-#pragma unroll
-    for (int k = 0; k < kResSlotWords; k++) st_weak_f64(mine + k, empty_word());
   }
   return ok;
 }
