@@ -248,13 +248,19 @@ int32_t pyomgpu_congrad_streamfunction(pyomgpu_ctx* ctx, const double* forc, dou
  * (device int32, Fortran indices, nbnd of them: make_inv_sfc's Dirichlet
  * points), forc (device) and sol (device, in/out) are the only memory it
  * touches besides a static device array of PYOMGPU_NOALLOC_SCRATCH_BYTES that
- * the library reserves on every GPU that loads it, until the process exits.
+ * the library holds on every GPU it is used on, until the process exits.  All
+ * pointers must be memory of the current device (or managed memory).
  * Grids whose operator and work vectors exceed that array (about 1.0e6
  * padded points, e.g. 1000 x 1000) are rejected with PYOMGPU_EINVAL and a
- * message.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call reuses the same array and clears what must start at zero; calls
- * that overlap on the GPU (other streams or host threads) race on it.
+ * message.  CUDA loads device code lazily, so the array and the solver's
+ * kernels are placed on a device by the first call made there, which also
+ * looks up the array's device address (cudaGetSymbolAddress): make that first
+ * call at set-up, while device memory is free (it can fail with
+ * PYOMGPU_ECUDA under memory pressure) and before any stream capture.  Later
+ * calls take no device memory.  Every call reuses the same array and clears
+ * what must start at zero; calls that overlap on the GPU (other streams or
+ * host threads) race on it.  The call waits for `stream` before it returns,
+ * because it reads the iteration count and status back to the host.
  * Results equal pyomgpu_congrad_streamfunction's on the same inputs. */
 #define PYOMGPU_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* grid, const int32_t* bnd_i, const int32_t* bnd_j,

@@ -26,8 +26,9 @@ MNISLE, MAXIPP, MAXQ = 1000, 20000, 10000
 
 def build(force: bool = False) -> str:
     src = os.path.join(HERE, "pyom_oracle.c")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(
-            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "pyom_oracle.h"))):
+    deps = [src, os.path.join(HERE, "pyom_oracle_mt.c"), os.path.join(HERE, "pyom_oracle.h"),
+            os.path.join(HERE, "Makefile")]
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(map(os.path.getmtime, deps)):
         subprocess.check_call(["make", "-s", "-C", HERE])
     return LIB_PATH
 
@@ -96,6 +97,8 @@ def lib():
             "o_absmax_sfp": (d, [p, p, p]),
             "o_congrad_streamfunction": (i, [p, p, p, p, p, d, i, d, p]),
             "o_congrad_surf_press": (i, [p, p, p, p, p, d, i, d, p]),
+            "o_congrad_streamfunction_mt": (i, [p, p, p, p, p, d, i, d, i, p]),
+            "o_max_threads": (i, []),
             "o_rel_residual": (d, [p, p, p, p, p]),
             "o_isleperim": (i, [p, p, i, i, i, i, i, i, p, p, p, p, p, p]),
             "o_island_map": (i, [p, p, i, i, i, p, p, p]),
@@ -193,6 +196,22 @@ class Oracle:
                                        float(M.congr_epsilon if eps is None else eps),
                                        int(M.congr_max_iterations if max_it is None else max_it),
                                        float(rtol), C.byref(info))
+        return dict(iterations=info.iterations, converged=bool(info.converged), status=info.status,
+                    estimated_error=info.estimated_error)
+
+    def congrad_streamfunction_mt(self, cf, forc, sol, eps=None, max_it=None, rtol=0.0, threads=0):
+        """congrad_streamfunction as the reference's MPI build runs it on
+        ``threads`` processes (row bands, partial sums combined in rank order),
+        on OpenMP threads; in place on ``sol``.  For timing the reference
+        algorithm on the host cores."""
+        M = self.M
+        s, keep = self.islands_struct()
+        info = OInfo()
+        lib().o_congrad_streamfunction_mt(self.gp, _p(cf), C.byref(s) if s is not None else None,
+                                          _p(_f64(forc)), _p(_f64(sol)),
+                                          float(M.congr_epsilon if eps is None else eps),
+                                          int(M.congr_max_iterations if max_it is None else max_it),
+                                          float(rtol), int(threads), C.byref(info))
         return dict(iterations=info.iterations, converged=bool(info.converged), status=info.status,
                     estimated_error=info.estimated_error)
 

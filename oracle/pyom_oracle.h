@@ -84,6 +84,12 @@ int o_congrad_streamfunction(const o_grid *g, const double *cf, const o_islands 
                              double *sol, double eps, int max_it, double rtol, o_info *info);
 int o_congrad_surf_press(const o_grid *g, const double *cf, const double *maskM, const double *forc,
                          double *psi, double eps, int max_it, double rtol, o_info *info);
+/* congrad_streamfunction as the reference's MPI build runs it on nthreads
+ * processes (pyom_oracle_mt.c; nthreads <= 0: one per CPU of the process) -- for
+ * timing the reference algorithm on every host core */
+int o_congrad_streamfunction_mt(const o_grid *g, const double *cf, const o_islands *isl, const double *forc,
+                                double *sol, double eps, int max_it, double rtol, int nthreads, o_info *info);
+int o_max_threads(void);
 
 double o_rel_residual(const o_grid *g, const double *cf, const double *Z, const double *forc, const double *sol);
 

@@ -7,9 +7,13 @@
 // allocator from its time-stepping loop (an allocation there can synchronise
 // the device or fail under memory pressure half-way through a run).  For
 // them this file provides one entry point that solves with scratch memory
-// the library reserves when it is loaded: a file-scope __device__ array of
-// kNoAllocBytes (64 MiB) on every GPU that loads the library, held until the
-// process exits.
+// the library holds itself: a file-scope __device__ array of kNoAllocBytes
+// (64 MiB) on every GPU that uses it, held until the process exits.  CUDA
+// loads a library's device code lazily by default, so the array (and this
+// file's kernels) are materialised on the device by the first call made on
+// it: make that call at set-up, while device memory is still free and before
+// any stream capture.  Under memory pressure that first call can fail with
+// PYOMGPU_ECUDA; later calls take no device memory.
 //
 // The caller passes only inputs and outputs (device pointers): the grid
 // metrics and hur/hvr, the island perimeter points, forc and sol.  The
@@ -56,14 +60,17 @@ int nfail(int code, const char* fmt, ...) {
   return code;
 }
 
-bool on_device(const void* p) {
+// Device memory of the current device, or managed memory.  Memory of another
+// GPU is refused: the kernels would read it over the peer path, or fault where
+// peer access is off.
+bool on_device(const void* p, int dev) {
   if (!p) return false;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
 }
 
 // Device address of the scratch array on the current device (set-up on the
@@ -111,11 +118,14 @@ extern "C" int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* gr
   if (!gr || !forc || !sol || nbnd < 0 || (nbnd > 0 && (!bnd_i || !bnd_j)))
     return nfail(PYOMGPU_EINVAL, "null argument");
   if (gr->onx != 2 || gr->nx < 4 || gr->ny < 4) return nfail(PYOMGPU_EINVAL, "bad grid size");
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return nfail(PYOMGPU_ECUDA, "cudaGetDevice failed");
   const void* need[] = {gr->dxt, gr->dxu, gr->dyt, gr->dyu, gr->cost, gr->cosu, gr->hur, gr->hvr, forc, sol};
   for (const void* p : need)
-    if (!on_device(p)) return nfail(PYOMGPU_EINVAL, "every array must be a device pointer (no staging here)");
-  if (nbnd > 0 && (!on_device(bnd_i) || !on_device(bnd_j)))
-    return nfail(PYOMGPU_EINVAL, "island points must be device pointers");
+    if (!on_device(p, cur))
+      return nfail(PYOMGPU_EINVAL, "every array must be device memory of the current device (no staging here)");
+  if (nbnd > 0 && (!on_device(bnd_i, cur) || !on_device(bnd_j, cur)))
+    return nfail(PYOMGPU_EINVAL, "island points must be device memory of the current device");
   cudaStream_t st = (cudaStream_t)stream;
 
   Geo g{};

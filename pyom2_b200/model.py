@@ -5,8 +5,9 @@ pyOM2 keeps its state in the Fortran module ``main_module``
 (for_src/main/main_module.f90) and f2py exposes every array to Python as an
 F-contiguous numpy view with the Fortran shape (py_src/pyOM.py:39).  This class
 carries the same names, shapes and memory order so that the solver entry points
-in :mod:`pyom2_b200.streamfunction` and :mod:`pyom2_b200.pressure` can be used
-on either an f2py module object or on this stand-in.
+in :mod:`pyom2_b200.external` (streamfunction and surface-pressure solves) and
+:mod:`pyom2_b200.non_hydrostatic` can be used on either an f2py module object or
+on this stand-in.
 
 Index conventions (py_src/pyOM.py:234-252): Fortran index ``i`` in
 ``is_pe-onx .. ie_pe+onx`` is Python index ``i + onx - is_pe``; time level

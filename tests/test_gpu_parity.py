@@ -260,17 +260,20 @@ def test_solve_pressure_step(oracle_lib, name, free_surface):
 @pytest.mark.parametrize("name", list(WORLDS))
 @pytest.mark.parametrize("precision", [_abi.PREC_F64, _abi.PREC_F32])
 def test_solve_rtol_reaches_1e10(oracle_lib, name, precision):
+    """Solved to the residual the benchmark uses (2e-11, which on these
+    operators leaves a solution error below 1e-10), the solution matches the
+    oracle's tight (1e-14) solution to 1e-10 relative."""
     W, Mg, Mo, O, E, _ = setup(name, oracle_lib)
     sol = np.zeros(Mg.shape2d, order="F")
-    info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=precision)
-    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
+    info = E.solve_rtol(W.forc, sol, rtol=2e-11, precision=precision)
+    assert info["status"] == 0 and info["rel_residual"] <= 2e-11, info
     cf = O.make_coeff_streamfunction()
     Z = O.make_inv_sfc(cf)
-    assert O.rel_residual(cf, Z, W.forc, sol) <= 1.5e-10
+    assert O.rel_residual(cf, Z, W.forc, sol) <= 3e-11
     so = np.zeros(Mg.shape2d, order="F")
-    O.congrad_streamfunction(cf, W.forc, so, eps=0.0, max_it=100000, rtol=1e-12)
+    O.congrad_streamfunction(cf, W.forc, so, eps=0.0, max_it=100000, rtol=1e-14)
     O.setcyclic_xy(so)
-    assert rel(sol, so, Z != 0) < 1e-8
+    assert rel(sol, so, Z != 0) < 1e-10
 
 
 def test_status_nan_maxiter_timeout(oracle_lib):
