@@ -171,6 +171,21 @@ int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* ctx, int32_t kernel);
 /* Piece layout the resident kernel uses on this grid: pieces in x and y and
  * points per thread; PYOMGPU_EINVAL when the grid does not fit. */
 int32_t pyomgpu_resident_layout(pyomgpu_ctx* ctx, int32_t* npx, int32_t* npy, int32_t* points_per_thread);
+/* Diagnostics, no counterpart in the reference: one pyomgpu_solve_rtol (FP64)
+ * in an instantiation of the resident kernel that records %globaltimer (ns)
+ * at 18 phase boundaries of loop trips it0 .. it0+nit-1 in every block (the
+ * same arithmetic and iterates).  out: host array of nblocks x nit x 18
+ * words, [(block * nit + trip - it0) * 18 + phase]; phases: 0 sweep A start,
+ * 1 direction in shared memory, 2 stencil and partials done, 3 after the
+ * first block barrier, 4 after the second (alpha known), 5 residual updated,
+ * 6 exchange records written, 7 after the first barrier of sweep B, 8
+ * solution updated, 9 after the second (beta known, halo loaded); control
+ * warp: 10/14 after the first barrier of reduction A/B, 11/15 its slot
+ * published, 12/16 all slots acquired, 13/17 control step done.  nblocks
+ * receives the block count (at most 160).  Zero words: phase not reached. */
+int32_t pyomgpu_resident_trace(pyomgpu_ctx* ctx, const double* forc, double* sol, double rtol, int32_t it0,
+                               int32_t nit, uint64_t* out, int32_t* nblocks, pyomgpu_solve_info* info,
+                               pyomgpu_stream stream);
 
 /* Autotuner of the solve kernel: times `iterations` iterations of the
  * Jacobi-PCG kernel on this grid (a fixed pseudo-random right-hand side) for

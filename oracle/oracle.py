@@ -4,10 +4,13 @@ The oracle is a plain-C FP64 restatement of pyOM2's external-mode solve
 (pyom_oracle.c).  Only tests/, ``__graft_entry__.smoke()`` and the CPU
 baseline leg of bench.py import this module; the product package never does.
 
-Parity status: no Fortran compiler exists in this image, so the restatement
-cannot be run side by side with the reference binary; it is pinned by
-known-answer tests (manufactured solutions, hand-built island maps,
-operator identities) and by committed golden fixtures.
+Parity status: pinned to the reference's own source.  No Fortran compiler
+exists in this image, so tests/golden/make_ref_golden.py runs pyOM2's Fortran
+routines through the Fortran-subset translator oracle/f90sub.py and commits
+their outputs; tests/test_oracle_vs_reference_source.py holds this oracle to
+them bit for bit (rounding level only where LAPACK's DGESV enters).
+Known-answer tests (manufactured solutions, hand-built island maps, operator
+identities) and further committed fixtures check it as well.
 """
 from __future__ import annotations
 

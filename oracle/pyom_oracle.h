@@ -6,14 +6,20 @@
  * CPU-baseline leg of bench.py may load it; the product library never links
  * or calls it.
  *
- * Parity status: the reference is Fortran and no Fortran compiler exists in
- * this image, so this restatement cannot be run against the reference binary
- * ("parity unpinned" against the reference itself).  The reference ships no
- * tests or golden vectors for this path.  The restatement is pinned instead by
- * known-answer tests that need no reference binary: manufactured solutions
- * (x* -> b = A x* -> solve), hand-checked island maps, the algebraic identities
- * of the operator and the island integrals, and committed fixtures generated
- * by tests/golden/make_golden.py.
+ * Parity status: pinned to the reference's own source.  No Fortran compiler
+ * exists in this image (none can be installed: no network, and the offline
+ * wheelhouse carries no gfortran, flang or LFortran), and the reference ships
+ * no tests or golden vectors for this path.  tests/golden/make_ref_golden.py
+ * therefore runs pyOM2's Fortran routines (main_module, parallel_none,
+ * numerics, island_module, streamfct_init, solve_streamfct, solve_pressure)
+ * through the Fortran-subset translator oracle/f90sub.py and commits their
+ * outputs; tests/test_oracle_vs_reference_source.py requires this restatement
+ * to reproduce them bit for bit (grid metrics, masks, island lists, psin,
+ * line_psin, CG iterates and iteration counts, solve_streamfunction and
+ * solve_pressure steps), except where LAPACK's DGESV enters (scipy's LAPACK
+ * there, the LU of o_dgesv here: rounding level).  Known-answer tests
+ * (manufactured solutions, hand-checked island maps, operator identities)
+ * and tests/golden/make_golden.py's fixtures remain as further checks.
  *
  * Layout: every 2-D array is Fortran-ordered with extents
  * (1-onx:nx+onx, 1-onx:ny+onx), onx = 2 (main_module.f90:35), i fastest.

@@ -172,6 +172,10 @@ int res_plan(pyomgpu_ctx* c) {
       if (cudaFuncSetAttribute(cg_res_kernel_ptr(kResP[k], single), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)cap) != cudaSuccess)
         return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the resident kernel");
+  for (int k = 0; k < kResNP; k++)
+    if (cudaFuncSetAttribute(cg_res_trace_kernel_ptr(kResP[k]), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)cap) != cudaSuccess)
+      return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the resident kernel");
   for (bool single : {false, true}) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_res_kernel_ptr(R.p, single), kResThreads,
@@ -222,10 +226,15 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   P.stall_extra = c->stall_next;
   c->stall_next = 0;
   P.out = c->d_result;
+  const bool trace = R.trace_nit > 0 && c->cg_kernel != 3;
+  P.trace = trace ? R.trace : nullptr;
+  P.trace_it0 = R.trace_it0;
+  P.trace_nit = trace ? R.trace_nit : 0;
   void* args[] = {&P};
   CK(cudaEventRecord(c->e0, st));
   const bool single = c->cg_kernel == 3;  // automatic: the two-reduction form (the reference's recurrences)
-  CK(cudaLaunchCooperativeKernel(cg_res_kernel_ptr(R.p, single), dim3(nb), dim3(kResThreads), args, R.smem, st));
+  const void* kern = trace ? cg_res_trace_kernel_ptr(R.p) : cg_res_kernel_ptr(R.p, single);
+  CK(cudaLaunchCooperativeKernel(kern, dim3(nb), dim3(kResThreads), args, R.smem, st));
   CK(cudaEventRecord(c->e1, st));
   return finish_cg(c, info, st);
 }
@@ -926,6 +935,38 @@ int32_t pyomgpu_resident_layout(pyomgpu_ctx* c, int32_t* npx, int32_t* npy, int3
   if (npy) *npy = c->resd.npy;
   if (points_per_thread) *points_per_thread = c->resd.p;
   return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_resident_trace(pyomgpu_ctx* c, const double* forc, double* sol, double rtol, int32_t it0,
+                               int32_t nit, uint64_t* out, int32_t* nblocks, pyomgpu_solve_info* info,
+                               pyomgpu_stream stream) {
+  if (!c || !out || it0 < 0 || nit < 1 || nit > 4096) return fail(PYOMGPU_EINVAL, "resident trace: bad arguments");
+  if (int rc = res_plan(c)) return rc;
+  if (!c->resd.ok) return fail(PYOMGPU_EINVAL, "the grid does not fit the resident kernel");
+  auto& R = c->resd;
+  const int nb = R.npx * R.npy;
+  const size_t words = (size_t)nb * nit * kResTracePhases;
+  if (words > R.trace_cap) {
+    if (R.trace) cudaFree(R.trace);
+    R.trace = nullptr;
+    R.trace_cap = 0;
+    if (int rc = dalloc(&R.trace, words)) return rc;
+    R.trace_cap = words;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(R.trace, 0, words * sizeof(uint64_t), st));
+  const int saved = c->cg_kernel;
+  c->cg_kernel = 2;
+  R.trace_it0 = it0;
+  R.trace_nit = nit;
+  const int rc = pyomgpu_solve_rtol(c, forc, sol, rtol, PYOMGPU_PREC_F64, 1000000, info, stream);
+  R.trace_nit = 0;
+  c->cg_kernel = saved;
+  if (rc != PYOMGPU_OK && rc != PYOMGPU_MAXITER) return rc;
+  CK(cudaMemcpyAsync(out, R.trace, words * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (nblocks) *nblocks = nb;
+  return rc;
 }
 
 int32_t pyomgpu_autotune(pyomgpu_ctx* c, int32_t iterations, int32_t* tile_x, int32_t* tile_y, int32_t* grid,

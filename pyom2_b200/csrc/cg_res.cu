@@ -394,7 +394,8 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // False on time-out.
 template <int NV, int kMaxSlot, int kStep>
 __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int npoll, ResCtl& C,
-                                                 const double (*wred)[kResSlotWords], unsigned* hflag = nullptr) {
+                                                 const double (*wred)[kResSlotWords], unsigned* hflag = nullptr,
+                                                 unsigned long long* tr = nullptr) {
   const int lane = threadIdx.x;
   {
     double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
@@ -413,6 +414,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
     if (lane < NV - 1) st_weak_f64(mine + lane, sendable(mv));
     __syncwarp();
     if (lane == NV - 1) st_release_f64(mine + NV - 1, sendable(mv));
+    if (tr != nullptr && lane == 0) tr[0] = globaltimer_ns();
   }
   constexpr int kPer = kResMaxSlots / 32;
   double got[kPer][NV];
@@ -446,6 +448,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       break;
     }
   }
+  if (tr != nullptr && lane == 0) tr[1] = globaltimer_ns();
   if (hflag != nullptr) {
     // every slot is acquired, so the exchange records released with them are
     // visible: let the workers start loading their halo before the control step
@@ -482,6 +485,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       C.est = 100.0 * out[0];
       ctl_stop(C, kDoneOk, PYOMGPU_OK);
     }
+    if (tr != nullptr) tr[2] = globaltimer_ns();
   }
   return ok;
 }
@@ -513,7 +517,7 @@ __device__ __forceinline__ void workers_sync() {
 // memory) and S2 (the controller's decision is in shared memory, or a wait
 // timed out).  Work that overlaps the wait of the other blocks (the solution
 // update) runs between S1 and S2.
-template <int P>
+template <int P, bool TRACE>
 __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_constant__ CGResParams Pm) {
   constexpr int CH = P == 8 ? 8 : 4;  // points per TMEM chunk (tcgen05 .x16 / .x8; .x16 at P = 16 spills)
   constexpr int NC = P / CH;  // chunks per field
@@ -532,6 +536,13 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     tc::tmem_relinquish();
   }
   if (threadIdx.x == 0) s_hflag = 0u;
+  // traced instantiation: this block's timestamps of loop trip t (nullptr outside the window)
+  auto trace_row = [&](unsigned t) -> unsigned long long* {
+    if (!TRACE) return nullptr;
+    const int k = (int)t - Pm.trace_it0;
+    if (k < 0 || k >= Pm.trace_nit) return nullptr;
+    return Pm.trace + ((size_t)blockIdx.x * Pm.trace_nit + k) * kResTracePhases;
+  };
 
   const int nb = gridDim.x;
   const int px = blockIdx.x % Pm.npx, py = blockIdx.x / Pm.npx;
@@ -568,9 +579,11 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred, &s_hflag);
     if (!__syncthreads_and(ok)) goto out;  // S2
     if (C.act == kRun) {
-      for (;;) {
+      for (unsigned trip = 0;; trip++) {
+        unsigned long long* tr = threadIdx.x == 0 ? trace_row(trip) : nullptr;
         __syncthreads();  // S1: partials of sweep A
-        ok = controller_epoch<2, 1, kStepA>(Pm, ++ep, nb, C, wred);
+        if (TRACE && tr) tr[10] = globaltimer_ns();
+        ok = controller_epoch<2, 1, kStepA>(Pm, ++ep, nb, C, wred, nullptr, TRACE && tr ? tr + 11 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
         if (C.stop_after) {  // the workers finish sweep B and stop
@@ -578,7 +591,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           break;
         }
         __syncthreads();  // S1: partials of sweep B
-        ok = controller_epoch<2, -1, kStepB>(Pm, ++ep, nb, C, wred, &s_hflag);
+        if (TRACE && tr) tr[14] = globaltimer_ns();
+        ok = controller_epoch<2, -1, kStepB>(Pm, ++ep, nb, C, wred, &s_hflag, TRACE && tr ? tr + 15 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
       }
@@ -686,7 +700,9 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     if (!__syncthreads_and(worker_halo_early(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
     if (C.act != kRun) goto done;
 
-    for (;;) {
+    for (unsigned trip = 0;; trip++) {
+      unsigned long long* tr = threadIdx.x == 32 ? trace_row(trip) : nullptr;
+      if (TRACE && tr) tr[0] = globaltimer_ns();
       // ---------------------------------------------- sweep A: direction, As
       lx = opaque(lx_);
       ly0 = opaque(ly0_);
@@ -705,6 +721,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           if (hl[e].sidx >= 0) ss[hl[e].sidx] = hl[e].q + bq * hl[e].s;
       }
       workers_sync();
+      if (TRACE && tr) tr[1] = globaltimer_ns();
       lx = opaque(lx_);
       ly0 = opaque(ly0_);
       nrow = opaque(nrow_);
@@ -734,8 +751,11 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         }
         worker_partials<2, 1>(v, wred);
       }
+      if (TRACE && tr) tr[2] = globaltimer_ns();
       __syncthreads();                           // S1
+      if (TRACE && tr) tr[3] = globaltimer_ns();
       if (!__syncthreads_and(1)) goto out;      // S2
+      if (TRACE && tr) tr[4] = globaltimer_ns();
       if (C.act != kRun) goto done;
       // ---------------------------------------------- sweep B: residual update
       lx = opaque(lx_);
@@ -775,11 +795,14 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
             stage_one(spub, pw, ph, lx, ly0 + u, q[u]);
             stage_one(spub + 2 * (pw + ph), pw, ph, lx, ly0 + u, s[u]);
           }
+        if (TRACE && tr) tr[5] = globaltimer_ns();
         workers_sync();
         copy_out<2>(Pm, Pm.hx, spub, ilo, ihi, jlo, jhi, wt);
+        if (TRACE && tr) tr[6] = globaltimer_ns();
         if (!stop_after) {
           worker_partials<2, -1>(v, wred);
           __syncthreads();  // S1
+          if (TRACE && tr) tr[7] = globaltimer_ns();
         }
         // sol += alpha*s (solve_streamfct.f90:278), while the other blocks finish
 #pragma unroll
@@ -795,9 +818,11 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           tm_st<CW>(t_sol + c * CW, bx);
         }
         tm_wait_st();
+        if (TRACE && tr) tr[8] = globaltimer_ns();
         if (stop_after) goto done;
       }
       if (!__syncthreads_and(worker_halo_early(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
+      if (TRACE && tr) tr[9] = globaltimer_ns();
       if (C.act != kRun) goto done;
     }
 
@@ -826,9 +851,12 @@ out:
   if (warp == 0) tc::tmem_dealloc(s_tmem, 512);
 }
 
-template __global__ void cg_res_kernel<4>(const __grid_constant__ CGResParams);
-template __global__ void cg_res_kernel<8>(const __grid_constant__ CGResParams);
-template __global__ void cg_res_kernel<16>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<4, false>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<8, false>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<16, false>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<4, true>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<8, true>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_kernel<16, true>(const __grid_constant__ CGResParams);
 
 // Single-reduction variant (one cross-block reduction per iteration) of the
 // same Jacobi-PCG, in the style of Chronopoulos and Gear but with the exact
@@ -1229,9 +1257,18 @@ template __global__ void cg_res1_kernel<16>(const __grid_constant__ CGResParams)
 
 const void* cg_res_kernel_ptr(int p, bool single) {
   switch (p) {
-    case 4: return single ? (const void*)cg_res1_kernel<4> : (const void*)cg_res_kernel<4>;
-    case 8: return single ? (const void*)cg_res1_kernel<8> : (const void*)cg_res_kernel<8>;
-    case 16: return single ? (const void*)cg_res1_kernel<16> : (const void*)cg_res_kernel<16>;
+    case 4: return single ? (const void*)cg_res1_kernel<4> : (const void*)cg_res_kernel<4, false>;
+    case 8: return single ? (const void*)cg_res1_kernel<8> : (const void*)cg_res_kernel<8, false>;
+    case 16: return single ? (const void*)cg_res1_kernel<16> : (const void*)cg_res_kernel<16, false>;
+    default: return nullptr;
+  }
+}
+
+const void* cg_res_trace_kernel_ptr(int p) {
+  switch (p) {
+    case 4: return (const void*)cg_res_kernel<4, true>;
+    case 8: return (const void*)cg_res_kernel<8, true>;
+    case 16: return (const void*)cg_res_kernel<16, true>;
     default: return nullptr;
   }
 }

@@ -38,7 +38,22 @@ struct CGResParams {
   unsigned long long timeout_ns;
   unsigned stall_extra;  // test hook: the first reduction also awaits a slot nobody writes
   CGResult* out;
+  // phase timestamps of the traced instantiation (cg_res_kernel<P, true>):
+  // %globaltimer at kResTracePhases points of loop trips trace_it0 ..
+  // trace_it0 + trace_nit - 1, per block: trace[(block * trace_nit + trip -
+  // trace_it0) * kResTracePhases + phase]
+  unsigned long long* trace;
+  int trace_it0, trace_nit;
 };
+
+// Phases of the trace (worker warp 1 lane 0 unless noted "ctl": warp 0 lane 0):
+//  0 sweep A start, 1 direction in shared memory (workers' barrier), 2 stencil
+//  and partials done, 3 after S1, 4 after S2 (alpha known), 5 residual updated
+//  and boundary staged, 6 exchange records written, 7 after S1, 8 solution
+//  updated, 9 after S2 (halo loaded, beta known); ctl: 10 after S1 (A), 11 slot
+//  published, 12 all slots acquired, 13 control step done, 14 after S1 (B),
+//  15 slot published, 16 all slots acquired, 17 control step done.
+constexpr int kResTracePhases = 18;
 
 // Dynamic shared memory of a w x h piece (the larger of the two kernels'
 // needs): the stencil operand with its one-cell halo, the x- and y-face
@@ -57,5 +72,7 @@ __host__ __device__ constexpr int res_threads(int w, int h, int p) { return w * 
 // (the reference's recurrences) or one (single = true: A p by recurrence and
 // (p, Ap) by its exact expansion in products of the sweep before).
 const void* cg_res_kernel_ptr(int p, bool single);
+// The traced instantiation of the two-reduction kernel (same arithmetic).
+const void* cg_res_trace_kernel_ptr(int p);
 
 }  // namespace pyomgpu

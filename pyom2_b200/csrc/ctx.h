@@ -97,6 +97,11 @@ struct pyomgpu_ctx {
     int npx = 0, npy = 0, wmax = 0, hmax = 0, p = 0;
     size_t smem = 0;
     double *hx = nullptr, *slots = nullptr;
+    // phase trace of the next resident solve (pyomgpu_resident_trace): device
+    // buffer of trace_cap words, loop trips trace_it0 .. trace_it0 + trace_nit - 1
+    unsigned long long* trace = nullptr;
+    size_t trace_cap = 0;
+    int trace_it0 = 0, trace_nit = 0;
   } resd;
 
   // work-queue batch (pyomgpu_congrad_streamfunction_batch and the psin
@@ -127,7 +132,7 @@ struct pyomgpu_ctx {
     if (batch.h_probs) cudaFreeHost(batch.h_probs);
     if (batch.h_state) cudaFreeHost(batch.h_state);
     if (batch.h_rr) cudaFreeHost(batch.h_rr);
-    for (void* p : {(void*)resd.hx, (void*)resd.slots})
+    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace})
       if (p) cudaFree(p);
     void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
                     sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,
