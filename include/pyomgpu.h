@@ -232,6 +232,17 @@ int32_t pyomgpu_island_boundaries_gpu(int32_t nx, int32_t ny, int32_t cyclic_x, 
 int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* ctx, const int32_t* kbot, int32_t mnisle, int32_t maxipp,
                                     int32_t maxq, double congr_epsilon, int32_t congr_max_iterations,
                                     pyomgpu_stream stream);
+/* Stop of the psin solves of the next pyomgpu_streamfunction_init.  No
+ * counterpart in the reference, which solves them with congrad_streamfunction
+ * and its own stop (streamfct_init.f90:283): rtol = 0 (the default) keeps
+ * that.  rtol > 0 solves each to ||res|| <= rtol ||res_0|| over the unknowns
+ * instead (the forcing is zero) with the reference's stopping estimate off;
+ * weighted = 1 then takes the inner products with the cell area dxu dyu cosu,
+ * in which the operator A = D^-1 S is self-adjoint, so the iteration is
+ * exact Jacobi-PCG on the symmetric S and converges where the reference's
+ * Euclidean products stagnate (on grids whose cell area varies strongly,
+ * e.g. 80S-80N).  PYOMGPU_EINVAL for rtol outside [0, 1). */
+int32_t pyomgpu_set_psin_solve(pyomgpu_ctx* ctx, double rtol, int32_t weighted);
 int32_t pyomgpu_island_sizes(pyomgpu_ctx* ctx, int32_t* nisle, int32_t* max_boundary);
 /* Copies out boundary/line_dir/nr_boundary (host), psin (host or device,
  * (nx+4,ny+4,nisle)), line_psin (host, (nisle,nisle)) and the psin iteration

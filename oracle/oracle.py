@@ -107,7 +107,8 @@ def lib():
             "o_island_map": (i, [p, p, i, i, i, p, p, p]),
             "o_island_trace": (i, [p, p, i, i, i, i, i, p, p, p]),
             "o_line_integral": (d, [p, p, i, p, p, p]),
-            "o_psin_solve": (i, [p, p, p, d, i, p, p]),
+            "o_psin_solve": (i, [p, p, p, d, i, d, i, p, p]),
+            "o_congrad_streamfunction_w": (i, [p, p, p, p, p, d, i, d, p]),
             "o_line_psin": (i, [p, p, p, p, p, p, p, p]),
             "o_dgesv": (i, [i, p, p, p]),
             "o_solve_streamfunction": (i, [p, p, p, p]),
@@ -202,6 +203,17 @@ class Oracle:
         return dict(iterations=info.iterations, converged=bool(info.converged), status=info.status,
                     estimated_error=info.estimated_error)
 
+    def congrad_streamfunction_w(self, cf, forc, sol, eps=0.0, max_it=10**6, rtol=0.0):
+        """congrad_streamfunction with cell-area-weighted inner products (exact
+        Jacobi-PCG on the symmetric S = D A), in place on ``sol``."""
+        s, keep = self.islands_struct()
+        info = OInfo()
+        lib().o_congrad_streamfunction_w(self.gp, _p(cf), C.byref(s) if s is not None else None,
+                                         _p(_f64(forc)), _p(_f64(sol)), float(eps), int(max_it), float(rtol),
+                                         C.byref(info))
+        return dict(iterations=info.iterations, converged=bool(info.converged), status=info.status,
+                    estimated_error=info.estimated_error)
+
     def congrad_streamfunction_mt(self, cf, forc, sol, eps=None, max_it=None, rtol=0.0, threads=0):
         """congrad_streamfunction as the reference's MPI build runs it on
         ``threads`` processes (row bands, partial sums combined in rank order),
@@ -272,8 +284,12 @@ class Oracle:
             raise RuntimeError("line integral: missing line_dir")
         return v
 
-    def streamfunction_init(self, eps=None, max_it=None, mnisle=MNISLE, maxipp=MAXIPP, maxq=MAXQ):
-        """streamfct_init.f90:7-304 on the oracle; fills M's island arrays."""
+    def streamfunction_init(self, eps=None, max_it=None, mnisle=MNISLE, maxipp=MAXIPP, maxq=MAXQ, psin_rtol=0.0,
+                            psin_weighted=False):
+        """streamfct_init.f90:7-304 on the oracle; fills M's island arrays.
+        ``psin_rtol`` > 0: the psin solves stop at that residual relative to
+        the initial one (reference stop off), with cell-area-weighted inner
+        products if ``psin_weighted`` (not in the reference)."""
         M = self.M
         rc, allmap, nisle, maxb = self.island_map(mnisle, maxipp, maxq)
         if rc:
@@ -288,8 +304,11 @@ class Oracle:
         cf = self.make_coeff_streamfunction()
         s, keep = self.islands_struct()
         iters = np.zeros(nisle, dtype=np.int32)
+        if psin_rtol > 0:
+            eps, max_it = 0.0, max(10**6, max_it or 0)
         st = lib().o_psin_solve(self.gp, _p(cf), C.byref(s), float(M.congr_epsilon if eps is None else eps),
-                                int(M.congr_max_iterations if max_it is None else max_it), _p(M.psin), _p(iters))
+                                int(M.congr_max_iterations if max_it is None else max_it), float(psin_rtol),
+                                int(bool(psin_weighted)), _p(M.psin), _p(iters))
         mU = np.asfortranarray(M.maskU[:, :, -1])
         mV = np.asfortranarray(M.maskV[:, :, -1])
         err = lib().o_line_psin(self.gp, C.byref(s), _p(M.psin), _p(_f64(M.hur)), _p(_f64(M.hvr)), _p(mU), _p(mV),

@@ -194,14 +194,41 @@ double o_rel_residual(const o_grid *g, const double *cf, const double *Z, const 
   return bb > 0 ? sqrt(rr / bb) : sqrt(rr);
 }
 
+/* dot_sfc with every product weighted by the cell area dxu(i) dyu(j) cosu(j)
+ * (the D of A = D^-1 S; not in the reference) */
+static double dot_area(const o_grid *g, const double *p1, const double *p2) {
+  double s2 = 0;
+  for (int j = 1; j <= g->ny; j++)
+    for (int i = 1; i <= g->nx; i++)
+      s2 = s2 + (g->dxu[X1(g, i)] * (g->dyu[Y1(g, j)] * g->cosu[Y1(g, j)])) * p1[IX(g, i, j)] * p2[IX(g, i, j)];
+  return s2;
+}
+
+static int congrad_core(const o_grid *g, const double *cf, const o_islands *isl, const double *forc, double *sol,
+                        double eps, int max_it, double rtol, int weighted, o_info *info);
+
 /*
  * solve_streamfct.f90:153-327 (congrad_streamfunction).
  * Extension for measurement only: rtol > 0 adds a stop on the recursively
  * updated residual, sqrt(sum_{Z!=0} res^2 / sum_{Z!=0} forc^2) <= rtol
- * (eps is then normally passed as 0 so the reference criterion never fires).
+ * (sum_{Z!=0} res_0^2 of the initial residual in place of the forcing's when
+ * the forcing is zero; eps is then normally passed as 0 so the reference
+ * criterion never fires).
  */
 int o_congrad_streamfunction(const o_grid *g, const double *cf, const o_islands *isl, const double *forc,
                              double *sol, double eps, int max_it, double rtol, o_info *info) {
+  return congrad_core(g, cf, isl, forc, sol, eps, max_it, rtol, 0, info);
+}
+
+/* The same with the inner products (beta, (s, As)) weighted by the cell area:
+ * exact Jacobi-PCG on the symmetric S = D A (not in the reference). */
+int o_congrad_streamfunction_w(const o_grid *g, const double *cf, const o_islands *isl, const double *forc,
+                               double *sol, double eps, int max_it, double rtol, o_info *info) {
+  return congrad_core(g, cf, isl, forc, sol, eps, max_it, rtol, 1, info);
+}
+
+static int congrad_core(const o_grid *g, const double *cf, const o_islands *isl, const double *forc, double *sol,
+                        double eps, int max_it, double rtol, int weighted, o_info *info) {
   size_t n2 = N2(g);
   double *res = (double *)calloc(n2, sizeof(double));
   double *Z = (double *)calloc(n2, sizeof(double));
@@ -222,6 +249,10 @@ int o_congrad_streamfunction(const o_grid *g, const double *cf, const o_islands 
     for (int j = 1; j <= ny; j++)
       for (int i = 1; i <= nx; i++)
         if (Z[IX(g, i, j)] != 0.0) bnorm2 += forc[IX(g, i, j)] * forc[IX(g, i, j)];
+    if (bnorm2 == 0.0)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++)
+          if (Z[IX(g, i, j)] != 0.0) bnorm2 += res[IX(g, i, j)] * res[IX(g, i, j)];
   }
   n = 0;
   for (int j = 1; j <= ny; j++)
@@ -235,7 +266,7 @@ int o_congrad_streamfunction(const o_grid *g, const double *cf, const o_islands 
   for (n = 1; n <= max_it; n++) {
     for (int j = 1; j <= ny; j++)
       for (int i = 1; i <= nx; i++) Zres[IX(g, i, j)] = Z[IX(g, i, j)] * res[IX(g, i, j)];
-    betak = o_dot_sfc(g, Zres, res);
+    betak = weighted ? dot_area(g, Zres, res) : o_dot_sfc(g, Zres, res);
     if (n == 1) {
       betak_min = fabs(betak);
     } else if (n > 2) {
@@ -250,7 +281,7 @@ int o_congrad_streamfunction(const o_grid *g, const double *cf, const o_islands 
       for (int i = 1; i <= nx; i++) ss[IX(g, i, j)] = Zres[IX(g, i, j)] + betaquot * ss[IX(g, i, j)];
     o_setcyclic_xy(g, ss);
     o_apply_op(g, cf, ss, As);
-    s_dot_As = o_dot_sfc(g, ss, As);
+    s_dot_As = weighted ? dot_area(g, ss, As) : o_dot_sfc(g, ss, As);
     if (fabs(s_dot_As) < fabs(betak) * F_1EM10) {
       smax = o_absmax_sfc(g, ss);
       estimated_error = 100.0 * smax;
@@ -793,8 +824,8 @@ double o_line_integral(const o_grid *g, const o_islands *isl, int isle, const do
 
 /* streamfct_init.f90:272-287: one CG solve per island with forc = 0 and
  * psin = 1 on the island's own perimeter.  psin is (nx+4, ny+4, nisle). */
-int o_psin_solve(const o_grid *g, const double *cf, const o_islands *isl, double eps, int max_it, double *psin,
-                 int *iterations) {
+int o_psin_solve(const o_grid *g, const double *cf, const o_islands *isl, double eps, int max_it, double rtol,
+                 int weighted, double *psin, int *iterations) {
   size_t n2 = N2(g);
   double *forc = (double *)calloc(n2, sizeof(double));
   int worst = 0;
@@ -808,7 +839,7 @@ int o_psin_solve(const o_grid *g, const double *cf, const o_islands *isl, double
     }
     o_setcyclic_xy(g, p);
     o_info info;
-    int st = o_congrad_streamfunction(g, cf, isl, forc, p, eps, max_it, 0.0, &info);
+    int st = congrad_core(g, cf, isl, forc, p, eps, max_it, rtol, weighted, &info);
     if (iterations) iterations[isle - 1] = info.iterations;
     if (st > worst) worst = st;
     o_setcyclic_xy(g, p);

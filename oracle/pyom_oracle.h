@@ -90,6 +90,10 @@ int o_congrad_streamfunction(const o_grid *g, const double *cf, const o_islands 
                              double *sol, double eps, int max_it, double rtol, o_info *info);
 int o_congrad_surf_press(const o_grid *g, const double *cf, const double *maskM, const double *forc,
                          double *psi, double eps, int max_it, double rtol, o_info *info);
+/* o_congrad_streamfunction with cell-area-weighted inner products (exact
+ * Jacobi-PCG on the symmetric S = D A; not in the reference) */
+int o_congrad_streamfunction_w(const o_grid *g, const double *cf, const o_islands *isl, const double *forc,
+                               double *sol, double eps, int max_it, double rtol, o_info *info);
 /* congrad_streamfunction as the reference's MPI build runs it on nthreads
  * processes (pyom_oracle_mt.c; nthreads <= 0: one per CPU of the process) -- for
  * timing the reference algorithm on every host core */
@@ -107,8 +111,8 @@ int o_island_trace(const o_grid *g, const int *allmap, int nisle, int max_bounda
                    int maxq, int *boundary, int *line_dir, int *nr_boundary);
 double o_line_integral(const o_grid *g, const o_islands *isl, int isle, const double *uloc, const double *vloc,
                        int *err);
-int o_psin_solve(const o_grid *g, const double *cf, const o_islands *isl, double eps, int max_it, double *psin,
-                 int *iterations);
+int o_psin_solve(const o_grid *g, const double *cf, const o_islands *isl, double eps, int max_it, double rtol,
+                 int weighted, double *psin, int *iterations);
 int o_line_psin(const o_grid *g, const o_islands *isl, const double *psin, const double *hur, const double *hvr,
                 const double *maskU_top, const double *maskV_top, double *line_psin);
 int o_dgesv(int n, double *a, int *ipiv, double *b);

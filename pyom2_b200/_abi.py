@@ -26,7 +26,7 @@ STATUS_NAMES = {OK: "ok", MAXITER: "max iterations exceeded", DIVERGED: "solver 
 # every symbol include/pyomgpu.h declares
 EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomgpu_ctx_destroy",
            "pyomgpu_set_sync_timeout", "pyomgpu_inject_barrier_stall", "pyomgpu_set_cg_kernel",
-           "pyomgpu_resident_layout", "pyomgpu_resident_trace", "pyomgpu_autotune", "pyomgpu_isleperim",
+           "pyomgpu_resident_layout", "pyomgpu_resident_trace", "pyomgpu_set_psin_solve", "pyomgpu_autotune", "pyomgpu_isleperim",
            "pyomgpu_island_boundaries", "pyomgpu_island_boundaries_gpu", "pyomgpu_streamfunction_init",
            "pyomgpu_island_sizes", "pyomgpu_get_islands", "pyomgpu_set_islands",
            "pyomgpu_congrad_streamfunction", "pyomgpu_congrad_streamfunction_noalloc",
@@ -125,6 +125,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_inject_barrier_stall": (i32, [vp, i32]),
         "pyomgpu_set_cg_kernel": (i32, [vp, i32]),
         "pyomgpu_resident_layout": (i32, [vp, P(i32), P(i32), P(i32)]),
+        "pyomgpu_set_psin_solve": (i32, [vp, C.c_double, i32]),
         "pyomgpu_resident_trace": (i32, [vp, vp, vp, C.c_double, i32, i32, P(C.c_uint64), P(i32), P(SolveInfo), vp]),
         "pyomgpu_autotune": (i32, [vp, i32, P(i32), P(i32), P(i32), P(d), vp]),
         "pyomgpu_isleperim": (i32, [vp, i32, i32, i32, i32, i32, i32, vp, P(i32), vp]),

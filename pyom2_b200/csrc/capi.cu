@@ -463,7 +463,7 @@ int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
 // workspace of `o`.  infos (v.size() entries) get each solve's result; with
 // want_res the FP64 true relative residual of each solution as well.
 int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol, bool want_res,
-              pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st) {
+              pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st, int weighted = 0) {
   const int count = (int)v.size();
   size_t pool = 0, tasks = 0;
   for (const BatchSpec& b : v) {
@@ -493,6 +493,7 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
     pr.eps = eps;
     pr.rtol = rtol;
     pr.max_it = max_it;
+    pr.weighted = weighted;
     pr.ntx = (b.c->nx + kTileX - 1) / kTileX;
     pr.nty = (b.c->ny + kTileY - 1) / kTileY;
     pr.tile0 = tile0;
@@ -681,7 +682,8 @@ int psin_and_line_psin(pyomgpu_ctx* c, double eps, int max_it, cudaStream_t st) 
     std::vector<BatchSpec> v;
     for (int k = k0; k < k1; ++k) v.push_back(BatchSpec{c, nullptr, c->psin + (size_t)k * c->n2});
     std::vector<pyomgpu_solve_info> infos(v.size());
-    int rc = run_batch(c, v, eps, max_it, 0.0, false, infos.data(), nullptr, st);
+    int rc = run_batch(c, v, c->psin_rtol > 0.0 ? 0.0 : eps, c->psin_rtol > 0.0 ? std::max(max_it, 1000000) : max_it,
+                       c->psin_rtol, false, infos.data(), nullptr, st, c->psin_weighted);
     if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
     for (int k = k0; k < k1; ++k) {
       const pyomgpu_solve_info& info = infos[k - k0];
@@ -934,6 +936,14 @@ int32_t pyomgpu_resident_layout(pyomgpu_ctx* c, int32_t* npx, int32_t* npy, int3
   if (npx) *npx = c->resd.npx;
   if (npy) *npy = c->resd.npy;
   if (points_per_thread) *points_per_thread = c->resd.p;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_set_psin_solve(pyomgpu_ctx* c, double rtol, int32_t weighted) {
+  if (!c || rtol < 0.0 || rtol >= 1.0 || (weighted != 0 && weighted != 1))
+    return fail(PYOMGPU_EINVAL, "set_psin_solve: bad arguments");
+  c->psin_rtol = rtol;
+  c->psin_weighted = weighted;
   return PYOMGPU_OK;
 }
 

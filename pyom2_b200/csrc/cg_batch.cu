@@ -91,7 +91,7 @@ __device__ void start_iteration(BatchState& st, const BatchProblem& pr, int n) {
 // v = (beta, ||forc||^2, ||res||^2, max|Z res|) of the initial residual
 __device__ void after_init(BatchState& st, const BatchProblem& pr, const double* v) {
   st.beta = v[0];
-  st.bb = v[1];
+  st.bb = v[1] > 0.0 ? v[1] : v[2];  // the rtol reference: ||forc||, or ||res_0|| for a zero forcing
   st.betam1 = 1.0;
   st.est = 0.0;
   st.stop_after = 0;
@@ -239,7 +239,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
       store_cyclic(pr.res, g, i, j, r);
       const double w = pr.op.W[q];
       const double zr = w * r;
-      v[0] += zr * r;
+      const double wd = pr.weighted ? 1.0 / (pr.op.ax[i + 1] * pr.op.by[j + 1]) : 1.0;
+      v[0] += (wd * zr) * r;
       if (w != 0.0) {
         v[1] += f * f;
         v[2] += r * r;
@@ -296,7 +297,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
                          op.by[j + 1] * (b_FY[k + kBX] * (b_s[k + kBX] - sc) + b_FY[k] * (b_s[k - kBX] - sc));
         store_cyclic(sn, g, i, j, sc);
         pr.As[g.at(i, j)] = a;
-        v[0] += sc * a;
+        const double wd = pr.weighted ? 1.0 / (op.ax[i + 1] * op.by[j + 1]) : 1.0;
+        v[0] += (wd * sc) * a;
         v[1] = fmax(v[1], fabs(sc));
       }
       double out[2];
@@ -328,7 +330,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
         const double r = pr.res[q] - alpha * pr.As[q];
         pr.sol[q] = pr.sol[q] + alpha * sn[q];
         store_cyclic(pr.res, g, i, j, r);
-        v[0] += w * r * r;
+        const double wd = pr.weighted ? 1.0 / (pr.op.ax[i + 1] * pr.op.by[j + 1]) : 1.0;
+        v[0] += (wd * w * r) * r;
         if (w != 0.0) v[1] += r * r;
       }
       double out[2];

@@ -19,8 +19,12 @@ struct BatchProblem {
   double* s[2];
   double* As;
   double eps;
-  double rtol;         // > 0: extra stop on ||res|| / ||forc|| over the unknowns
+  double rtol;         // > 0: extra stop on ||res|| / ||forc|| over the unknowns (||res|| / ||res_0||
+                       // for a zero forcing, e.g. the psin solves)
   int max_it;
+  int weighted;        // 1: inner products weighted by the cell area D = 1/(ax by) = dxu dyu cosu, in
+                       // which A = D^-1 S is self-adjoint (exact Jacobi-PCG on the symmetric S); 0: the
+                       // reference's Euclidean products
   int tile0, ntx, nty; // first task index, tiles in x and y
 };
 

@@ -91,6 +91,10 @@ struct pyomgpu_ctx {
 
   // on-chip-resident kernel of the streamfunction solves (cg_res.cu): piece
   // layout planned on first use, exchange buffers allocated with it
+  // psin solves of streamfunction_init: the reference's stop (psin_rtol = 0), or
+  // to ||res|| <= psin_rtol ||res_0||, with cell-area-weighted products if psin_weighted
+  double psin_rtol = 0.0;
+  int psin_weighted = 0;
   int cg_kernel = 0;  // 0 automatic, 1 tiled cg_ref_kernel, 2 resident cg_res_kernel
   struct Resident {
     bool planned = false, ok = false;

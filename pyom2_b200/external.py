@@ -177,11 +177,16 @@ class ExternalMode:
         return a.value, b.value, c.value
 
     # ---- islands -----------------------------------------------------------------
-    def streamfunction_init(self, M=None, mnisle=0, maxipp=0, maxq=0, eps=None, max_it=None):
+    def streamfunction_init(self, M=None, mnisle=0, maxipp=0, maxq=0, eps=None, max_it=None, psin_rtol=0.0,
+                            psin_weighted=False):
         """streamfct_init.f90:7-304; fills ``nisle, boundary, line_dir,
         nr_boundary, psin, dpsin, line_psin`` of the model (allocated here,
-        :87-93).  ``mnisle/maxipp/maxq`` = 0 keep the reference's limits."""
+        :87-93).  ``mnisle/maxipp/maxq`` = 0 keep the reference's limits.
+        ``psin_rtol`` > 0 solves the psin problems to that residual relative
+        to the initial one instead of the reference's stop, with cell-area
+        weighted products if ``psin_weighted`` (pyomgpu_set_psin_solve)."""
         M = M or self.M
+        _abi.check(self._L.pyomgpu_set_psin_solve(self._ctx, float(psin_rtol), int(bool(psin_weighted))))
         kbot = np.asfortranarray(_host(M.kbot), dtype=np.int32)
         rc = self._L.pyomgpu_streamfunction_init(
             self._ctx, C.c_void_p(kbot.ctypes.data), int(mnisle), int(maxipp), int(maxq),
