@@ -418,6 +418,9 @@ int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
         per_sm < 1)
       return fail(PYOMGPU_ECUDA, "occupancy query of the batch kernel failed");
     B.max_blocks = per_sm * o->nsm;
+    int l2 = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, o->device) != cudaSuccess) l2 = 0;
+    B.l2_bytes = (size_t)std::max(l2, 0);
     if (int rc = dalloc(&B.sync, 8)) return rc;
   }
   if (pool > B.cap) {
@@ -434,18 +437,23 @@ int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
     if (B.h_state) cudaFreeHost(B.h_state);
     if (B.d_rr) cudaFree(B.d_rr);
     if (B.h_rr) cudaFreeHost(B.h_rr);
+    if (B.d_group) cudaFree(B.d_group);
+    if (B.h_group) cudaFreeHost(B.h_group);
     B.d_probs = nullptr;
     B.h_probs = nullptr;
     B.d_state = nullptr;
     B.h_state = nullptr;
     B.d_rr = B.h_rr = nullptr;
+    B.d_group = B.h_group = nullptr;
     B.cap_probs = 0;
     if (int rc = dalloc(&B.d_probs, (size_t)count)) return rc;
     if (int rc = dalloc(&B.d_state, (size_t)count)) return rc;
     if (int rc = dalloc(&B.d_rr, (size_t)count * 2)) return rc;
+    if (int rc = dalloc(&B.d_group, (size_t)count + 1)) return rc;
     if (cudaMallocHost((void**)&B.h_probs, sizeof(BatchProblem) * count) != cudaSuccess ||
         cudaMallocHost((void**)&B.h_state, sizeof(BatchState) * count) != cudaSuccess ||
-        cudaMallocHost((void**)&B.h_rr, sizeof(double) * 2 * count) != cudaSuccess)
+        cudaMallocHost((void**)&B.h_rr, sizeof(double) * 2 * count) != cudaSuccess ||
+        cudaMallocHost((void**)&B.h_group, sizeof(int) * (count + 1)) != cudaSuccess)
       return fail(PYOMGPU_ENOMEM, "cudaMallocHost");
     B.cap_probs = count;
   }
@@ -475,9 +483,32 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   auto& B = o->batch;
   CK(cudaMemsetAsync(B.pool, 0, pool * sizeof(double), st));
   CK(cudaMemsetAsync(B.sync, 0, 8 * sizeof(unsigned long long), st));
+  // groups whose fields (about 72 bytes per padded point: sol, res, two directions, As,
+  // FX, FY, Z, forc) stay in L2: largest problems first, packed greedily into 60 % of L2;
+  // the kernel solves the groups one after another
+  std::vector<int> order((size_t)count);
+  for (int k = 0; k < count; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return v[a].c->g.size() > v[b].c->g.size(); });
+  const size_t budget = B.l2_bytes ? B.l2_bytes * 6 / 10 : ((size_t)64 << 20);
+  int ngroup = 0;
+  {
+    size_t acc = 0;
+    B.h_group[0] = 0;
+    for (int pos = 0; pos < count; ++pos) {
+      const size_t ws = 72 * v[order[pos]].c->g.size();
+      if (pos > B.h_group[ngroup] && acc + ws > budget) {
+        B.h_group[++ngroup] = pos;
+        acc = 0;
+      }
+      acc += ws;
+    }
+    B.h_group[++ngroup] = count;
+  }
   double* cur = B.pool;
   int tile0 = 0;
-  for (int k = 0; k < count; ++k) {
+  for (int pos = 0; pos < count; ++pos) {
+    const int k = order[pos];
     const BatchSpec& b = v[k];
     const size_t P = align32(b.c->g.size());
     BatchProblem pr{};
@@ -498,16 +529,19 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
     pr.nty = (b.c->ny + kTileY - 1) / kTileY;
     pr.tile0 = tile0;
     tile0 += pr.ntx * pr.nty;
-    B.h_probs[k] = pr;
+    B.h_probs[pos] = pr;
     launch_pack(b.c->g, b.sol, pr.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
   }
   CK(cudaMemcpyAsync(B.d_probs, B.h_probs, sizeof(BatchProblem) * count, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(B.d_group, B.h_group, sizeof(int) * (ngroup + 1), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(B.d_state, 0, sizeof(BatchState) * count, st));
   BatchParams P{};
   P.probs = B.d_probs;
   P.state = B.d_state;
   P.nprob = count;
   P.ntasks = tile0;
+  P.ngroup = ngroup;
+  P.group = B.d_group;
   P.part = B.part;
   P.ctl = reinterpret_cast<SyncCtl*>(B.sync);
   P.gen = B.sync + 2;
@@ -521,8 +555,9 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   CK(cudaEventRecord(o->e1, st));
   CK(cudaMemcpyAsync(B.h_state, B.d_state, sizeof(BatchState) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(o->h_scal, &P.ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
-  for (int k = 0; k < count; ++k) {
-    const BatchProblem& pr = B.h_probs[k];
+  for (int pos = 0; pos < count; ++pos) {
+    const int k = order[pos];
+    const BatchProblem& pr = B.h_probs[pos];
     if (want_res) {
       launch_fill_cyclic(pr.g, pr.sol, st);
       launch_residual(pr.g, pr.op, pr.forc, pr.sol, v[k].c->part, 1024, B.d_rr + 2 * k, st);
@@ -539,8 +574,9 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   CK(cudaEventElapsedTime(&ms, o->e0, o->e1));
   if (ms_out) *ms_out = ms;
   int worst = PYOMGPU_OK;
-  for (int k = 0; k < count; ++k) {
-    const BatchState& S = B.h_state[k];
+  for (int pos = 0; pos < count; ++pos) {
+    const int k = order[pos];
+    const BatchState& S = B.h_state[pos];
     worst = std::max(worst, S.status);
     if (!infos) continue;
     pyomgpu_solve_info& I = infos[k];

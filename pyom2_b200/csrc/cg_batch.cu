@@ -33,8 +33,8 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ int task_problem(const BatchParams& P, int task) {
-  int lo = 0, hi = P.nprob - 1;  // last problem with tile0 <= task
+__device__ __forceinline__ int task_problem(const BatchParams& P, int task, int p0, int p1) {
+  int lo = p0, hi = p1 - 1;  // last problem of the group with tile0 <= task
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (P.probs[mid].tile0 <= task)
@@ -141,7 +141,8 @@ __device__ void after_b(BatchState& st, const BatchProblem& pr, const double* v)
 // Grid barrier whose last arrival reduces the partials of every problem that
 // took part in the sweep just finished and advances its state.  Returns false
 // on time-out.
-__device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, int kind, unsigned extra = 0) {
+__device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, int kind, int p0, int p1,
+                               unsigned extra = 0) {
   __shared__ int s_last, s_ok, s_any;
   __syncthreads();
   epoch += 1;
@@ -155,7 +156,7 @@ __device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, 
     // every partial of this sweep is visible (acquire side of the arrivals)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int any = 0;
-    for (int p = warp; p < P.nprob; p += kBatchThreads / 32) {
+    for (int p = p0 + warp; p < p1; p += kBatchThreads / 32) {
       const BatchProblem& pr = P.probs[p];
       const int phase = __ldcg(&P.state[p].phase);
       if (kind != kInit && phase != kind) {  // finished earlier (init reduces every problem)
@@ -165,12 +166,26 @@ __device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, 
       const int nt = pr.ntx * pr.nty;
       const int nv = (kind == kInit) ? 4 : 2;
       double v[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int t = lane; t < nt; t += 32) {
-        const double* q = P.part + (size_t)(pr.tile0 + t) * 4;
-        for (int k = 0; k < nv; k++) {
-          const double x = __ldcg(q + k);
-          const bool is_max = (kind == kInit && k == 3) || (kind == kSweepA && k == 1);
-          v[k] = is_max ? fmax(v[k], x) : v[k] + x;
+      // lane l sums tiles l, l+32, l+64, ... in that order; four tiles' partials are
+      // loaded before they are added, so the loads overlap
+      for (int t0 = lane; t0 < nt; t0 += 128) {
+        double x[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int t = t0 + 32 * u;
+          const double* q = P.part + (size_t)(pr.tile0 + (t < nt ? t : 0)) * 4;
+#pragma unroll
+          for (int k = 0; k < 4; k++) x[u][k] = (t < nt && k < nv) ? __ldcg(q + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (t0 + 32 * u >= nt) break;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            if (k >= nv) break;
+            const bool is_max = (kind == kInit && k == 3) || (kind == kSweepA && k == 1);
+            v[k] = is_max ? fmax(v[k], x[u][k]) : v[k] + x[u][k];
+          }
         }
       }
       for (int k = 0; k < nv; k++) {
@@ -222,9 +237,13 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
   __shared__ double b_s[kBoxN], b_FX[kBoxN], b_FY[kBoxN];
   unsigned long long epoch = 0;
 
+  for (int grp = 0; grp < P.ngroup; grp++) {
+  const int p0 = P.group[grp], p1 = P.group[grp + 1];
+  const int t_lo = P.probs[p0].tile0;
+  const int t_hi = P.probs[p1 - 1].tile0 + P.probs[p1 - 1].ntx * P.probs[p1 - 1].nty;
   // ---- init: res = forc - A sol -------------------------------------------------
-  for (int task = blockIdx.x; task < P.ntasks; task += gridDim.x) {
-    const int p = task_problem(P, task);
+  for (int task = t_lo + blockIdx.x; task < t_hi; task += gridDim.x) {
+    const int p = task_problem(P, task, p0, p1);
     const BatchProblem& pr = P.probs[p];
     const Geo g = pr.g;
     const int lt = task - pr.tile0;
@@ -252,13 +271,13 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
     if (threadIdx.x == 0)
       for (int k = 0; k < 4; k++) P.part[(size_t)task * 4 + k] = out[k];
   }
-  if (!reduce_barrier(P, epoch, kInit, P.stall_extra)) return;
+  if (!reduce_barrier(P, epoch, kInit, p0, p1, grp == 0 ? P.stall_extra : 0u)) return;
 
   for (;;) {
     if (!__ldcg(P.any_active)) break;
     // ---- sweep A: s_new = Z res + bq s_old on tile + halo, As = A s_new ---------------
-    for (int task = blockIdx.x; task < P.ntasks; task += gridDim.x) {
-      const int p = task_problem(P, task);
+    for (int task = t_lo + blockIdx.x; task < t_hi; task += gridDim.x) {
+      const int p = task_problem(P, task, p0, p1);
       if (__ldcg(&P.state[p].phase) != 1) continue;
       const BatchProblem& pr = P.probs[p];
       const Geo g = pr.g;
@@ -308,11 +327,11 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
         P.part[(size_t)task * 4 + 1] = out[1];
       }
     }
-    if (!reduce_barrier(P, epoch, kSweepA)) return;
+    if (!reduce_barrier(P, epoch, kSweepA, p0, p1)) return;
     if (!__ldcg(P.any_active)) break;
     // ---- sweep B: sol += alpha s, res -= alpha As ------------------------------------------
-    for (int task = blockIdx.x; task < P.ntasks; task += gridDim.x) {
-      const int p = task_problem(P, task);
+    for (int task = t_lo + blockIdx.x; task < t_hi; task += gridDim.x) {
+      const int p = task_problem(P, task, p0, p1);
       if (__ldcg(&P.state[p].phase) != 2) continue;
       const BatchProblem& pr = P.probs[p];
       const Geo g = pr.g;
@@ -341,8 +360,9 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
         P.part[(size_t)task * 4 + 1] = out[1];
       }
     }
-    if (!reduce_barrier(P, epoch, kSweepB)) return;
+    if (!reduce_barrier(P, epoch, kSweepB, p0, p1)) return;
   }
+  }  // groups
 }
 
 const void* cg_batch_kernel_ptr() { return (const void*)cg_batch_kernel; }

@@ -42,6 +42,11 @@ struct BatchParams {
   BatchState* state;     // zero on entry
   int nprob;
   int ntasks;            // total tiles of all problems
+  // problems are solved in ngroup groups, one after another, each small enough
+  // for its fields to stay in L2: group g holds problems group[g] ..
+  // group[g+1]-1 (problems and their tiles are stored group by group)
+  int ngroup;
+  const int* group;      // ngroup + 1 problem offsets
   double* part;          // per task, 4 partials
   SyncCtl* ctl;
   unsigned long long* gen;  // release flag of the reducing block

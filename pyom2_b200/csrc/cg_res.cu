@@ -62,6 +62,15 @@ __device__ __forceinline__ double ld_acquire_f64(const double* p) {
 // Plain store, cached in L2 only (ordered before a later st.release of the
 // same thread, or of thread 0 after a block barrier).
 __device__ __forceinline__ void st_weak_f64(double* p, double v) { __stcg(p, v); }
+// Relaxed (morally strong) store at GPU scope: a reader may observe it with a
+// relaxed load and validate it on its own.
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+// Acquire side of the slot protocol: after relaxed loads have observed the
+// released words of every slot, one fence makes everything released before
+// them visible (the acquire pattern of the PTX memory model).
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release_f64(double* p, double v) {
   asm volatile("st.release.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
@@ -411,7 +420,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
 #pragma unroll
     for (int k = 0; k < NV; k++)
       if (lane == k) mv = t[k];
-    if (lane < NV - 1) st_weak_f64(mine + lane, sendable(mv));
+    if (lane < NV - 1) st_relaxed_f64(mine + lane, sendable(mv));
     __syncwarp();
     if (lane == NV - 1) st_release_f64(mine + NV - 1, sendable(mv));
     if (tr != nullptr && lane == 0) tr[0] = globaltimer_ns();
@@ -427,19 +436,25 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
   }
   bool ok = true;
   const unsigned long long t0 = globaltimer_ns();
+  // every word of every slot this lane polls is loaded relaxed in one pass (the
+  // loads are independent: one L2 round trip per pass) and validated on its own:
+  // a word is either empty or this epoch's value (a slot is emptied two epochs
+  // ahead, and the fence below orders those stores before the next poll)
   for (unsigned spin = 1; have != want; spin++) {
 #pragma unroll
     for (int m = 0; m < kPer; m++) {
       if (!((want & ~have) >> m & 1u)) continue;
       const double* sl = res_slot(P, ep, lane + 32 * m);
+#pragma unroll
+      for (int k = 0; k < NV; k++) got[m][k] = ld_relaxed_f64(sl + k);
+    }
+#pragma unroll
+    for (int m = 0; m < kPer; m++) {
+      if (!((want & ~have) >> m & 1u)) continue;
       bool all = true;
 #pragma unroll
-      for (int k = 0; k < NV - 1; k++) {
-        got[m][k] = ld_relaxed_f64(sl + k);
-        all = all && !is_empty(got[m][k]);
-      }
-      got[m][NV - 1] = ld_acquire_f64(sl + NV - 1);
-      if (all && !is_empty(got[m][NV - 1])) have |= 1u << m;
+      for (int k = 0; k < NV; k++) all = all && !is_empty(got[m][k]);
+      if (all) have |= 1u << m;
     }
     if (have != want && (spin & 31u) == 0u &&
         (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
@@ -448,6 +463,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       break;
     }
   }
+  fence_acq_rel_gpu();
   if (tr != nullptr && lane == 0) tr[1] = globaltimer_ns();
   if (hflag != nullptr) {
     // every slot is acquired, so the exchange records released with them are

@@ -123,6 +123,9 @@ struct pyomgpu_ctx {
     size_t cap_tasks = 0;
     double* d_rr = nullptr;  // 2 per solve: true residual, forcing norm
     double* h_rr = nullptr;  // pinned
+    int* d_group = nullptr;  // cap_probs + 1 problem offsets of the L2-sized groups
+    int* h_group = nullptr;  // pinned
+    size_t l2_bytes = 0;     // L2 size of the device
     unsigned long long* sync = nullptr;  // SyncCtl, gen, any_active
   } batch;
 
@@ -136,7 +139,8 @@ struct pyomgpu_ctx {
     if (batch.h_probs) cudaFreeHost(batch.h_probs);
     if (batch.h_state) cudaFreeHost(batch.h_state);
     if (batch.h_rr) cudaFreeHost(batch.h_rr);
-    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace})
+    if (batch.h_group) cudaFreeHost(batch.h_group);
+    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace, (void*)batch.d_group})
       if (p) cudaFree(p);
     void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
                     sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,
