@@ -563,7 +563,7 @@ def main():
             dist.barrier()
         err = None
         if tight is not None:
-            x = sol_d.cpu().numpy().T[2:-2, 2:-2]
+            x = sol_d.cpu().numpy()[2:-2, 2:-2]  # the Fortran-ordered view already has shape (nx+4, ny+4)
             t_in = tight[2:-2, 2:-2]
             err = float(np.linalg.norm(x - t_in) / np.linalg.norm(t_in))
         it_med = int(statistics.median(iters))

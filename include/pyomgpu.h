@@ -131,6 +131,29 @@ typedef struct pyomgpu_state {
   double* dpsin;                /* (nisle,3), streamfunction only */
 } pyomgpu_state;
 
+/* Inputs and outputs of the momentum tendencies (momentum.f90:4-152) of a
+ * hydrostatic configuration without turbulence closures (vertical viscosity
+ * kappaM given, as the reference's kappaM_0 set-ups without TKE).  All
+ * DEVICE pointers, Fortran layout with the module's halo; the 1-D grid
+ * metrics dxt, dxu, dyt, dyu, cost, cosu come from the context. */
+typedef struct pyomgpu_momentum {
+  int32_t nz, taum1, tau, taup1;  /* 1-based time levels */
+  int32_t coord_degree;           /* metric terms of momentum.f90:19-30 */
+  int32_t enable_hor_friction, enable_hor_friction_cos_scaling, hor_friction_cospower;
+  int32_t enable_bottom_friction, enable_implicit_vert_friction;
+  double dt_mom, A_h, r_bot;
+  const double *dzt, *dzw;        /* [nz] */
+  const double* tantr;            /* [ny+4] */
+  const double *maskT, *maskU, *maskV, *maskW; /* (nx+4,ny+4,nz) */
+  const int32_t* kbot;            /* (nx+4,ny+4) */
+  const double *coriolis_t, *area_t, *area_u, *area_v; /* (nx+4,ny+4) */
+  const double *surface_taux, *surface_tauy;          /* (nx+4,ny+4) */
+  const double* kappaM;           /* (nx+4,ny+4,nz) */
+  double *u, *v, *w;              /* (nx+4,ny+4,nz,3); u, v(taup1) are the implicit friction's scratch */
+  double *du, *dv;                /* (nx+4,ny+4,nz,3): du, dv(tau) written */
+  double *du_mix, *dv_mix;        /* (nx+4,ny+4,nz) written */
+} pyomgpu_momentum;
+
 /* ---- library -------------------------------------------------------------- */
 int32_t pyomgpu_version(void);
 const char* pyomgpu_last_error(void);
@@ -232,6 +255,21 @@ int32_t pyomgpu_island_boundaries_gpu(int32_t nx, int32_t ny, int32_t cyclic_x, 
 int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* ctx, const int32_t* kbot, int32_t mnisle, int32_t maxipp,
                                     int32_t maxq, double congr_epsilon, int32_t congr_max_iterations,
                                     pyomgpu_stream stream);
+/* momentum (momentum.f90:4-152) up to the external-mode solve, for the
+ * hydrostatic case without closures: Coriolis and metric terms, surface wind
+ * stress, momentum_advection (momentum_advection.f90:1-76), implicit
+ * vertical friction with the given kappaM (vertical_friction.f90:109-226),
+ * harmonic friction (harmonic_friction.f90:4-124) and linear bottom friction
+ * (bottom_friction.f90:48-135), each as enabled in `m`.  Writes du, dv at
+ * tau and du_mix, dv_mix on the interior points, bit for bit the reference's
+ * serial arithmetic (the energy-dissipation diagnostics K_diss_* are not
+ * formed).  The caller then runs pyomgpu_solve_streamfunction. */
+int32_t pyomgpu_momentum_tendencies(pyomgpu_ctx* ctx, const pyomgpu_momentum* m, pyomgpu_stream stream);
+/* vertical_velocity (vertical_velocity.f90:4-25): w(:,:,:,level) from u, v at
+ * `level` (uses m->u, m->v, m->w, m->maskW, m->dzt, m->nz only). */
+int32_t pyomgpu_vertical_velocity(pyomgpu_ctx* ctx, const pyomgpu_momentum* m, int32_t level,
+                                  pyomgpu_stream stream);
+
 /* Stop of the psin solves of the next pyomgpu_streamfunction_init.  No
  * counterpart in the reference, which solves them with congrad_streamfunction
  * and its own stop (streamfct_init.f90:283): rtol = 0 (the default) keeps

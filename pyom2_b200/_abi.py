@@ -26,7 +26,8 @@ STATUS_NAMES = {OK: "ok", MAXITER: "max iterations exceeded", DIVERGED: "solver 
 # every symbol include/pyomgpu.h declares
 EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomgpu_ctx_destroy",
            "pyomgpu_set_sync_timeout", "pyomgpu_inject_barrier_stall", "pyomgpu_set_cg_kernel",
-           "pyomgpu_resident_layout", "pyomgpu_resident_trace", "pyomgpu_set_psin_solve", "pyomgpu_autotune", "pyomgpu_isleperim",
+           "pyomgpu_resident_layout", "pyomgpu_resident_trace", "pyomgpu_set_psin_solve",
+           "pyomgpu_momentum_tendencies", "pyomgpu_vertical_velocity", "pyomgpu_autotune", "pyomgpu_isleperim",
            "pyomgpu_island_boundaries", "pyomgpu_island_boundaries_gpu", "pyomgpu_streamfunction_init",
            "pyomgpu_island_sizes", "pyomgpu_get_islands", "pyomgpu_set_islands",
            "pyomgpu_congrad_streamfunction", "pyomgpu_congrad_streamfunction_noalloc",
@@ -82,6 +83,18 @@ class Islands(C.Structure):
                 ("line_dir", C.c_void_p), ("nr_boundary", C.c_void_p)]
 
 
+class Momentum(C.Structure):
+    """pyomgpu_momentum (include/pyomgpu.h)."""
+    _fields_ = [("nz", C.c_int32), ("taum1", C.c_int32), ("tau", C.c_int32), ("taup1", C.c_int32),
+                ("coord_degree", C.c_int32), ("enable_hor_friction", C.c_int32),
+                ("enable_hor_friction_cos_scaling", C.c_int32), ("hor_friction_cospower", C.c_int32),
+                ("enable_bottom_friction", C.c_int32), ("enable_implicit_vert_friction", C.c_int32),
+                ("dt_mom", C.c_double), ("A_h", C.c_double), ("r_bot", C.c_double)] + [
+        (n, C.c_void_p) for n in ("dzt", "dzw", "tantr", "maskT", "maskU", "maskV", "maskW", "kbot", "coriolis_t",
+                                  "area_t", "area_u", "area_v", "surface_taux", "surface_tauy", "kappaM", "u", "v",
+                                  "w", "du", "dv", "du_mix", "dv_mix")]
+
+
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("status", C.c_int32),
                 ("outer_iterations", C.c_int32), ("estimated_error", C.c_double),
@@ -126,6 +139,8 @@ def load(path: str = LIB_PATH):
         "pyomgpu_set_cg_kernel": (i32, [vp, i32]),
         "pyomgpu_resident_layout": (i32, [vp, P(i32), P(i32), P(i32)]),
         "pyomgpu_set_psin_solve": (i32, [vp, C.c_double, i32]),
+        "pyomgpu_momentum_tendencies": (i32, [vp, P(Momentum), vp]),
+        "pyomgpu_vertical_velocity": (i32, [vp, P(Momentum), i32, vp]),
         "pyomgpu_resident_trace": (i32, [vp, vp, vp, C.c_double, i32, i32, P(C.c_uint64), P(i32), P(SolveInfo), vp]),
         "pyomgpu_autotune": (i32, [vp, i32, P(i32), P(i32), P(i32), P(d), vp]),
         "pyomgpu_isleperim": (i32, [vp, i32, i32, i32, i32, i32, i32, vp, P(i32), vp]),

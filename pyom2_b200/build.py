@@ -20,6 +20,9 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpyomgpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# per-file flags: the momentum tendencies reproduce the reference's serial
+# arithmetic, so no multiply-add contraction there
+FILE_FLAGS = {"momentum.cu": ["-fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -57,7 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
-            cmd = [nvcc] + common + ["-c", src, "-o", obj]
+            cmd = [nvcc] + common + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
             if src.endswith(".cpp"):
                 cmd = [shutil.which("g++") or "g++", "-O3", "-std=c++17", "-fPIC", "-I", INCLUDE, "-c", src, "-o", obj]
             jobs.append(cmd)

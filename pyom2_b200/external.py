@@ -327,6 +327,52 @@ class ExternalMode:
         M = M or self.M
         return self._run_step(M, self._L.pyomgpu_solve_pressure, ("du", "dv", "u", "v", "p_hydro", "psi"))
 
+    _MOM_IN = ("dzt", "dzw", "tantr", "maskT", "maskU", "maskV", "maskW", "coriolis_t", "area_t", "area_u", "area_v",
+               "surface_taux", "surface_tauy", "kappaM", "u", "v", "w", "du", "dv", "du_mix", "dv_mix")
+
+    def _momentum_struct(self, M):
+        import torch
+        dev = torch.device("cuda")
+        D = {n: _to_device_f(getattr(M, n), dev) for n in self._MOM_IN}
+        kb = M.kbot
+        D["kbot"] = kb if _is_torch(kb) else torch.from_numpy(
+            np.ascontiguousarray(np.asfortranarray(kb, dtype=np.int32).T)).to(dev)
+        m = _abi.Momentum()
+        m.nz, m.taum1, m.tau, m.taup1 = int(M.nz), int(M.taum1), int(M.tau), int(M.taup1)
+        m.coord_degree = int(bool(M.coord_degree))
+        m.enable_hor_friction = int(bool(M.enable_hor_friction))
+        m.enable_hor_friction_cos_scaling = int(bool(M.enable_hor_friction_cos_scaling))
+        m.hor_friction_cospower = int(M.hor_friction_cosPower)
+        m.enable_bottom_friction = int(bool(M.enable_bottom_friction))
+        m.enable_implicit_vert_friction = int(bool(M.enable_implicit_vert_friction))
+        m.dt_mom, m.A_h, m.r_bot = float(M.dt_mom), float(M.A_h), float(M.r_bot)
+        for n, t in D.items():
+            setattr(m, n, t.data_ptr())
+        return m, D
+
+    def momentum(self, M=None):
+        """momentum.f90:4-152 up to the external-mode solve (Coriolis, metric
+        terms, wind stress, advection, implicit vertical friction with
+        M.kappaM, harmonic and linear bottom friction as enabled on M):
+        writes du, dv at tau, du_mix and dv_mix (pyomgpu_momentum_tendencies).
+        Host arrays are copied in and out; CUDA tensors are used in place."""
+        M = M or self.M
+        m, D = self._momentum_struct(M)
+        _abi.check(self._L.pyomgpu_momentum_tendencies(self._ctx, C.byref(m), _stream()))
+        for n in ("du", "dv", "du_mix", "dv_mix", "u", "v"):
+            a = getattr(M, n)
+            if not _is_torch(a):
+                a[...] = _from_device_f(D[n])
+
+    def vertical_velocity(self, M=None, level=None):
+        """vertical_velocity.f90: w(:,:,:,level) from u, v at level (default taup1)."""
+        M = M or self.M
+        m, D = self._momentum_struct(M)
+        lev = int(M.taup1 if level is None else level)
+        _abi.check(self._L.pyomgpu_vertical_velocity(self._ctx, C.byref(m), lev, _stream()))
+        if not _is_torch(M.w):
+            M.w[...] = _from_device_f(D["w"])
+
 
 # ---------------------------------------------------------------------------
 def _host(a):

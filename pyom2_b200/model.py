@@ -109,6 +109,20 @@ class ModelState:
         self.dw_mix = zeros_f(X, Y, nz)
         self.psi = zeros_f(X, Y, 3)
         self.dpsi = zeros_f(X, Y, 3)
+        # momentum inputs (main_module.f90:113-114,109-112,160-161,210): metric and
+        # box areas of calc_grid, Coriolis frequency, wind stress, vertical viscosity
+        self.tantr = np.zeros(Y)
+        for name in ("area_t", "area_u", "area_v", "area_z", "coriolis_t", "surface_taux", "surface_tauy"):
+            setattr(self, name, zeros_f(X, Y))
+        self.kappaM = zeros_f(X, Y, nz)
+        # physics switches and parameters of momentum (main_module.f90:196-203), the reference's defaults
+        self.enable_hor_friction = False
+        self.enable_hor_friction_cos_scaling = False
+        self.hor_friction_cosPower = 3
+        self.enable_bottom_friction = False
+        self.enable_implicit_vert_friction = False
+        self.A_h = 0.0
+        self.r_bot = 0.0
         # island variables, allocated by streamfunction_init (streamfct_init.f90:87-93)
         self.nisle = 0
         self.boundary = None

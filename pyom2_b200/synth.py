@@ -30,10 +30,12 @@ streamfunction forcing ``forc``.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 import scipy.ndimage as ndi
 
-from .model import ModelState, DEGTOM, PI_F, ONX
+from .model import ModelState, DEGTOM, PI_F, ONX, RADIUS
 
 
 # ----------------------------------------------------------------------------
@@ -112,9 +114,17 @@ def calc_grid(M: ModelState):
     if M.coord_degree:
         M.cost[:] = np.cos(yt / 180.0 * PI_F)
         M.cosu[:] = np.cos(yu / 180.0 * PI_F)
+        # tan of the C library, element by element, as the Fortran intrinsic
+        M.tantr[:] = [math.tan(y / 180.0 * PI_F) / RADIUS for y in yt]
     else:
         M.cost[:] = 1.0
         M.cosu[:] = 1.0
+        M.tantr[:] = 0.0
+    # box areas (numerics.f90:160-167)
+    M.area_t[...] = (M.dxt[:, None] * M.cost[None, :]) * M.dyt[None, :]
+    M.area_u[...] = (M.dxu[:, None] * M.cost[None, :]) * M.dyt[None, :]
+    M.area_v[...] = (M.dxt[:, None] * M.cosu[None, :]) * M.dyu[None, :]
+    M.area_z[...] = (M.dxu[:, None] * M.cosu[None, :]) * M.dyu[None, :]
 
 
 def setcyclic_xy(M: ModelState, a):

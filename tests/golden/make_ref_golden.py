@@ -19,15 +19,19 @@ records what the reference computes:
   with a free surface and with a rigid lid;
 * congrad_non_hydro (for_src/non_hydrostatic/non_hydrostatic.f90:146-242)
   from a seeded first guess and one step of solve_non_hydrostatic (:5-63) on
-  a closed tank and a cyclic x-z slice.
+  a closed tank and a cyclic x-z slice;
+* one call of momentum (for_src/main/momentum.f90:4-168: Coriolis and metric
+  terms, wind stress, momentum_advection, implicit vertical friction,
+  harmonic and linear bottom friction, then solve_streamfunction) on a small
+  re-entrant channel, with w(tau) from vertical_velocity_tau.
 
 LAPACK's DGESV (called by solve_streamfunction, solve_streamfct.f90:81) is
 not part of the reference; scipy's LAPACK dgesv stands in for the system
 library the reference links.  The open-boundary hooks (set_obc_*) are not
 loaded: open boundaries are off in every case, where they do nothing.
 
-Output: tests/golden/ref_f90_<case>.npz, ref_f90_pressure.npz and
-ref_f90_nh.npz.  Arrays of
+Output: tests/golden/ref_f90_<case>.npz, ref_f90_pressure.npz,
+ref_f90_nh.npz and ref_f90_momentum.npz.  Arrays of
 at most 60000 values are stored whole, larger ones as a SHA-256 digest of
 their bytes, their L2 norm and a strided sample.
 
@@ -45,7 +49,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
 from oracle import f90sub  # noqa: E402
-from ref_cases import CASES, GRID_OUT, GRID_WIDTHS, NH_CASES, PRESSURE, STEP_OUT_2D, STEP_OUT_3D, digest, random_state  # noqa: E402
+from ref_cases import (CASES, GRID_OUT, GRID_WIDTHS, MOMENTUM_CASE, MOMENTUM_OUT_3D, NH_CASES, PRESSURE,  # noqa: E402
+                       STEP_OUT_2D, STEP_OUT_3D, digest, momentum_state, random_state)
 
 REF = os.environ.get("PYOM2_REFERENCE", "/root/reference")
 SOURCES = ["for_src/main/main_module.f90", "for_src/parallel/parallel_none.f90", "for_src/main/numerics.f90",
@@ -79,6 +84,39 @@ EXTERNALS = {"dgesv": _dgesv, "set_obc_streamfct": _nothing, "set_obc_topo": _no
 
 def program():
     return f90sub.translate([os.path.join(REF, p) for p in SOURCES], EXTERNALS)
+
+
+# momentum (momentum.f90) and the modules it uses; the timers of timing_module
+# (tic/toc) do nothing here, and the routines of features that are off in the
+# momentum case are not loaded (a call would stop the generator)
+MOMENTUM_SOURCES = ["for_src/isoneutral/isoneutral_module.f90", "for_src/idemix/idemix_module.f90",
+                    "for_src/rossmix/rossmix_module.f90", "for_src/rossmix2/rossmix2_module.f90",
+                    "for_src/etc/py_stuff.f90", "for_src/main/momentum.f90", "for_src/main/momentum_advection.f90",
+                    "for_src/main/harmonic_friction.f90", "for_src/main/bottom_friction.f90",
+                    "for_src/main/vertical_friction.f90", "for_src/main/vertical_velocity.f90"]
+
+
+def _not_loaded(name):
+    def f(prog, *args):
+        raise f90sub.F90Error(f"{name} is not loaded: its feature is off in these cases")
+    return f
+
+
+def momentum_program():
+    prog = f90sub.Program()
+    prog.add_source("module timing_module\nend module timing_module\n", "timing_module (timers only)")
+    for p in SOURCES[:1] + MOMENTUM_SOURCES + SOURCES[1:]:
+        with open(os.path.join(REF, p)) as fh:
+            prog.add_source(fh.read(), p.split("/")[-1])
+    ext = dict(EXTERNALS)
+    ext.update({"tic": _nothing, "toc": _nothing, "set_obc_momentum": _nothing})
+    for n in ("isoneutral_friction", "idemix_friction", "idemix_friction_lee", "rossmix_friction",
+              "rossmix2_friction", "biharmonic_friction", "momentum_sources_with_euler",
+              "momentum_sources_with_ab"):
+        ext[n] = _not_loaded(n)
+    prog.externals.update(ext)
+    prog.compile()
+    return prog
 
 
 def put(out, key, a):
@@ -249,12 +287,57 @@ def nonhydro():
     np.savez_compressed(os.path.join(HERE, "ref_f90_nh.npz"), **out)
 
 
+def momentum_case():
+    """momentum (momentum.f90:4-168: tendencies, then solve_streamfunction) on
+    the channel of MOMENTUM_CASE, one step from the seeded state, after
+    streamfunction_init and vertical_velocity_tau for w(tau)."""
+    t0 = time.time()
+    name, make = MOMENTUM_CASE
+    W = make()
+    M = W.M
+    momentum_state(M, 31)
+    prog = momentum_program()
+    setup_model(prog, M, GRID_WIDTHS[name])
+    S = prog.state["main_module"]
+    out = {"kbot__digest": np.array(digest(M.kbot))}
+    for n in GRID_OUT + ("tantr", "area_t", "area_u", "area_v"):
+        put(out, "grid_" + n, S[n.lower()].a)
+    prog.set("main_module", "enable_streamfunction", True)
+    prog.call("streamfunction_init")
+    for n in ("enable_hor_friction", "enable_hor_friction_cos_scaling", "hor_friction_cosPower",
+              "enable_bottom_friction", "enable_implicit_vert_friction", "A_h", "r_bot", "dt_mom"):
+        prog.set("main_module", n.lower(), getattr(M, n))
+    prog.set("main_module", "enable_conserve_energy", False)
+    for n in ("u", "v", "coriolis_t", "surface_taux", "surface_tauy", "kappaM", "du", "dv"):
+        S[n.lower()].a[...] = getattr(M, n)
+    for n in ("taum1", "tau", "taup1"):
+        prog.set("main_module", n, getattr(M, n))
+    prog.call("vertical_velocity_tau", int(S["tau"]))
+    put(out, "w_tau", S["w"].a[:, :, :, S["tau"] - 1])
+    prog.call("momentum")
+    tau, tp1 = S["tau"] - 1, S["taup1"] - 1
+    for n in MOMENTUM_OUT_3D:
+        a = S[n].a
+        put(out, n, a[:, :, :, tau] if a.ndim == 4 else a)
+    out["itts"] = np.array(S["congr_itts"])
+    for n in ("psi", "dpsi"):
+        put(out, n, S[n].a[:, :, tp1])
+    put(out, "dpsin", S["dpsin"].a)
+    for n in ("u", "v"):
+        put(out, n + "_taup1", S[n].a[:, :, :, tp1])
+    np.savez_compressed(os.path.join(HERE, "ref_f90_momentum.npz"), **out)
+    print(f"momentum {name}: nisle {int(S['nisle'])}, solve {int(S['congr_itts'])} iterations, "
+          f"{time.time() - t0:.0f} s", flush=True)
+
+
 def main():
-    for name in (sys.argv[1:] or list(CASES) + ["pressure", "nh"]):
+    for name in (sys.argv[1:] or list(CASES) + ["pressure", "nh", "momentum"]):
         if name == "pressure":
             pressure()
         elif name == "nh":
             nonhydro()
+        elif name == "momentum":
+            momentum_case()
         else:
             case(name)
 

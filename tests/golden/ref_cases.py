@@ -27,11 +27,15 @@ NH_CASES = {
     "nh_slice": lambda: synth.nonhydro_tank(24, 1, 10, 12, cyclic_x=True, dx=0.5, first_guess=True),
 }
 
+# momentum tendencies + solve_streamfunction (momentum.f90:4-168): a small
+# re-entrant channel (config 4's recipe: 60S-30S, cyclic in x, one ridge)
+MOMENTUM_CASE = ("channel", lambda: synth.config4(1004, nx=32, ny=24, nz=6))
+
 # the cell widths the cases' set_grid step hands to calc_grid: degrees where
 # coord_degree is set (pyOM2 converts them to metres there), metres otherwise;
 # dzt is in metres
 GRID_WIDTHS = {"c0": (2.0, 2.0), "cyclic96": (360.0 / 96, 160.0 / 48), "nh_closed": (0.5, 0.5),
-               "nh_slice": (0.5, 0.5)}
+               "nh_slice": (0.5, 0.5), "channel": (64.0 / 32, 30.0 / 24)}
 
 # one-step cases of solve_pressure: (case, free surface, max iterations)
 PRESSURE = [("c0", True, None), ("c0", False, 300), ("cyclic96", True, None)]
@@ -69,3 +73,45 @@ def digest(a):
 
 STEP_OUT_2D = ("dpsi", "psi")
 STEP_OUT_3D = ("u", "v", "du", "dv", "p_hydro")
+
+
+# parameters of the momentum case: the reference's channel set-up
+# (py_config/acc2.py:41-49: harmonic friction with cos scaling, linear bottom
+# friction, implicit vertical friction), with a given vertical viscosity in
+# place of the TKE closure
+MOMENTUM_PARAMS = dict(enable_hor_friction=True, enable_hor_friction_cos_scaling=True, hor_friction_cosPower=1,
+                       enable_bottom_friction=True, r_bot=1e-5, enable_implicit_vert_friction=True, dt_mom=1800.0)
+OMEGA = np.float64(np.float32(np.pi)) / 43082.0  # main_module.f90:16 (pi a default real)
+
+
+def momentum_state(M, seed):
+    """The inputs of the momentum case: smooth masked u, v at the three time
+    levels with cyclic halos, Coriolis frequency 2 omega sin(lat), a zonal
+    wind stress of 0.1 N/m^2 / rho_0 with a sin^2 profile across the channel,
+    a seeded positive vertical viscosity around 1e-4 m^2/s, and the
+    reference's A_h = (2 degtom)^3 2e-11 scaled to this grid; seeded."""
+    from pyom2_b200.model import DEGTOM
+    rng = np.random.default_rng(seed)
+    X, Y = M.shape2d
+    nz = M.nz
+    for k, v in MOMENTUM_PARAMS.items():
+        setattr(M, k, v)
+    M.A_h = (2 * DEGTOM) ** 3 * 2e-11
+    shape3 = (X, Y, nz)
+    for lev in range(3):
+        for name, mask in (("u", M.maskU), ("v", M.maskV)):
+            f = synth.smooth_field(rng, shape3, (3.0, 3.0, 1.5), (True, False, False))
+            f = np.asfortranarray(f * (0.05 / np.sqrt(np.mean(f ** 2))) * mask)
+            synth.setcyclic_xy(M, f)
+            getattr(M, name)[..., lev] = f
+    M.coriolis_t[...] = (2 * OMEGA * np.sin(M.yt / 180.0 * np.pi))[None, :]
+    y0, y1 = M.yu[2], M.yu[M.ny + 1]
+    prof = np.sin(np.pi * (M.yt - y0) / (y1 - y0)) ** 2
+    M.surface_taux[...] = M.maskU[:, :, -1] * (1e-4 * prof)[None, :]
+    M.surface_tauy[...] = 0.0
+    M.kappaM[...] = 1e-4 * (1.0 + 0.5 * rng.uniform(size=shape3))
+    M.du[...] = 0.0
+    M.dv[...] = 0.0
+
+
+MOMENTUM_OUT_3D = ("du", "dv", "du_mix", "dv_mix")

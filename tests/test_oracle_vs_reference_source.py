@@ -24,7 +24,7 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
 
-from ref_cases import CASES, GRID_OUT, NH_CASES, PRESSURE, STEP_OUT_3D, digest, random_state  # noqa: E402
+from ref_cases import CASES, GRID_OUT, MOMENTUM_CASE, NH_CASES, PRESSURE, STEP_OUT_3D, digest, random_state  # noqa: E402
 
 LIMITS = dict(maxipp=10**6, maxq=10**6)
 
@@ -167,3 +167,14 @@ def test_oracle_non_hydrostatic_matches_reference(oracle_lib, name):
     assert M.congr_itts_non_hydro == int(g[f"{name}_step_itts"])
     for n in ("u", "v", "w", "p_non_hydro"):
         same(g, f"{name}_step_{n}", getattr(M, n))
+
+
+def test_channel_grid_matches_reference():
+    """synth's grid of the momentum case, with the metric term tantr and the
+    box areas of calc_grid (numerics.f90:147-167), is the reference's bit for
+    bit."""
+    g = fixture("momentum")
+    W = MOMENTUM_CASE[1]()
+    assert digest(W.M.kbot) == str(g["kbot__digest"])
+    for n in GRID_OUT + ("tantr", "area_t", "area_u", "area_v"):
+        same(g, "grid_" + n, getattr(W.M, n))
