@@ -295,12 +295,14 @@ def c3_learned(steps, warmup):
 
 
 def c4_sequence(steps, spinup=10, members=8, methods=("ref", "batch_ref", "batch", "pcg64", "mixed32", "fcg")):
-    """Config 4: consecutive solve_streamfunction steps of ``members``
-    re-entrant channel runs (256x256x20, 60S-30S, one 2000 m ridge) driven by
-    the seeded synthetic tendency sequence of pyom2_b200/sequence.py, each
-    solve warm-started from the reference's first guess.  Per method: a fresh
-    ensemble, ``spinup`` untimed steps, then ``steps`` steps timed with CUDA
-    events (the whole step: tendencies, begin, solve, end, for all members)."""
+    """Config 4: consecutive time steps of ``members`` re-entrant channel runs
+    (256x256x20, 60S-30S, one 2000 m ridge, 0.1 N/m^2 wind stress), each step
+    the model's own momentum tendencies on the GPU, then solve_streamfunction
+    warm-started from the reference's first guess (pyom2_b200/sequence.py);
+    the members differ by a seeded 0.1 K temperature perturbation.  Per
+    method: a fresh ensemble spun up from rest for ``spinup`` untimed steps,
+    then ``steps`` steps timed with CUDA events (the whole step: tendencies,
+    begin, solve, end, vertical velocity, for all members)."""
     import torch
     from pyom2_b200 import synth
     from pyom2_b200.sequence import ChannelEnsemble

@@ -265,8 +265,10 @@ int32_t pyomgpu_streamfunction_init(pyomgpu_ctx* ctx, const int32_t* kbot, int32
  * serial arithmetic (the energy-dissipation diagnostics K_diss_* are not
  * formed).  The caller then runs pyomgpu_solve_streamfunction. */
 int32_t pyomgpu_momentum_tendencies(pyomgpu_ctx* ctx, const pyomgpu_momentum* m, pyomgpu_stream stream);
-/* vertical_velocity (vertical_velocity.f90:4-25): w(:,:,:,level) from u, v at
- * `level` (uses m->u, m->v, m->w, m->maskW, m->dzt, m->nz only). */
+/* The end of the reference's time step for u, v at `level`: their cyclic
+ * halo copies (setcyclic_xyz, main.f90:114-117), then vertical_velocity
+ * (vertical_velocity.f90:4-25, main.f90:147): w(:,:,:,level) from u, v at
+ * `level`.  Uses m->u, m->v, m->w, m->maskW, m->dzt, m->nz only. */
 int32_t pyomgpu_vertical_velocity(pyomgpu_ctx* ctx, const pyomgpu_momentum* m, int32_t level,
                                   pyomgpu_stream stream);
 

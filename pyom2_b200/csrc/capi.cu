@@ -66,10 +66,12 @@ namespace pyomgpu {
 // lets other translation units of the library report through pyomgpu_last_error()
 void set_last_error(const char* msg) { g_last_error = msg; }
 // grid size and the 1-D device metrics (dxt, dxu, dyt, dyu, cost, cosu; index Fortran + 1) of a context
-int ctx_grid1d(pyomgpu_ctx* c, int* nx, int* ny, const double** out6) {
+int ctx_grid1d(pyomgpu_ctx* c, int* nx, int* ny, const double** out6, int* cyclic_x, int* cyclic_y) {
   if (!c) return fail(PYOMGPU_EINVAL, "null context");
   *nx = c->nx;
   *ny = c->ny;
+  if (cyclic_x) *cyclic_x = c->g.cyclic_x;
+  if (cyclic_y) *cyclic_y = c->g.cyclic_y;
   const double* a[6] = {c->dxt, c->dxu, c->dyt, c->dyu, c->cost, c->cosu};
   for (int k = 0; k < 6; k++) out6[k] = a[k];
   return PYOMGPU_OK;

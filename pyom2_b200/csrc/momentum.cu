@@ -25,7 +25,7 @@
 namespace pyomgpu {
 void set_last_error(const char* msg);  // capi.cu
 // grid size and the 1-D device metrics of a context (capi.cu)
-int ctx_grid1d(pyomgpu_ctx* c, int* nx, int* ny, const double** out6);
+int ctx_grid1d(pyomgpu_ctx* c, int* nx, int* ny, const double** out6, int* cyclic_x, int* cyclic_y);
 
 namespace {
 
@@ -288,6 +288,39 @@ __global__ void k_mom_lateral(MomDev m) {
   }
 }
 
+// ---- the cyclic halo copies of u and v at time level lev (parallel_none.f90:
+// setcyclic_xyz; the reference's time loop does them at main.f90:114-117) -----------
+__global__ void k_setcyclic_uv(MomDev m, int lev, int cyclic_x, int cyclic_y) {
+  const MG& g = m.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nrow = g.ny + 4;  // j = -1 .. ny+2
+  if (t >= 2 * nrow * g.nz) return;
+  const int f = t / (nrow * g.nz), r = t % (nrow * g.nz);
+  const int j = r % nrow - 1, k = 1 + r / nrow;
+  double* a = (f == 0 ? m.u : m.v) + (size_t)(lev - 1) * g.n2 * g.nz;
+  if (cyclic_x)
+    for (int i = 1; i <= 2; i++) {
+      a[g.k3(g.nx + i, j, k)] = a[g.k3(i, j, k)];
+      a[g.k3(1 - i, j, k)] = a[g.k3(g.nx - i + 1, j, k)];
+    }
+  (void)cyclic_y;
+}
+
+// rows of a cyclic-y domain, after every column has its x copies
+__global__ void k_setcyclic_uv_y(MomDev m, int lev) {
+  const MG& g = m.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ncol = g.nx + 4;  // i = -1 .. nx+2
+  if (t >= 2 * ncol * g.nz) return;
+  const int f = t / (ncol * g.nz), r = t % (ncol * g.nz);
+  const int i = r % ncol - 1, k = 1 + r / ncol;
+  double* a = (f == 0 ? m.u : m.v) + (size_t)(lev - 1) * g.n2 * g.nz;
+  for (int j = 1; j <= 2; j++) {
+    a[g.k3(i, g.ny + j, k)] = a[g.k3(i, j, k)];
+    a[g.k3(i, 1 - j, k)] = a[g.k3(i, g.ny - j + 1, k)];
+  }
+}
+
 // ---- vertical_velocity (vertical_velocity.f90:4-25) at time level lev --------------
 __global__ void k_vertical_velocity(MomDev m, int lev) {
   const MG& g = m.g;
@@ -378,7 +411,7 @@ extern "C" int32_t pyomgpu_momentum_tendencies(pyomgpu_ctx* c, const pyomgpu_mom
                                  "every array given)");
   int nx = 0, ny = 0;
   const double* g1[6];
-  if (int rc = ctx_grid1d(c, &nx, &ny, g1)) return rc;
+  if (int rc = ctx_grid1d(c, &nx, &ny, g1, nullptr, nullptr)) return rc;
   const MomDev m = to_dev(p, nx, ny, g1);
   cudaStream_t st = (cudaStream_t)stream;
   const int n = nx * ny, tb = 128, nb = (n + tb - 1) / tb;
@@ -395,9 +428,9 @@ extern "C" int32_t pyomgpu_vertical_velocity(pyomgpu_ctx* c, const pyomgpu_momen
                                             pyomgpu_stream stream) {
   if (!c || !p || !p->u || !p->v || !p->w || !p->maskW || !p->dzt || level < 1 || level > 3 || p->nz < 1)
     return mfail(PYOMGPU_EINVAL, "vertical_velocity: bad arguments");
-  int nx = 0, ny = 0;
+  int nx = 0, ny = 0, cx = 0, cy = 0;
   const double* g1[6];
-  if (int rc = ctx_grid1d(c, &nx, &ny, g1)) return rc;
+  if (int rc = ctx_grid1d(c, &nx, &ny, g1, &cx, &cy)) return rc;
   MomDev m{};
   m.g = MG{nx, ny, p->nz, (size_t)(nx + 4) * (ny + 4)};
   m.dxt = g1[0];
@@ -409,8 +442,18 @@ extern "C" int32_t pyomgpu_vertical_velocity(pyomgpu_ctx* c, const pyomgpu_momen
   m.u = p->u;
   m.v = p->v;
   m.w = p->w;
-  const int n = (nx + 3) * (ny + 3), tb = 128;
-  k_vertical_velocity<<<(n + tb - 1) / tb, tb, 0, (cudaStream_t)stream>>>(m, level);
+  const int tb = 128;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cx) {
+    const int nr = 2 * (ny + 4) * p->nz;
+    k_setcyclic_uv<<<(nr + tb - 1) / tb, tb, 0, st>>>(m, level, cx, cy);
+  }
+  if (cy) {
+    const int nc = 2 * (nx + 4) * p->nz;
+    k_setcyclic_uv_y<<<(nc + tb - 1) / tb, tb, 0, st>>>(m, level);
+  }
+  const int n = (nx + 3) * (ny + 3);
+  k_vertical_velocity<<<(n + tb - 1) / tb, tb, 0, st>>>(m, level);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return mfail(PYOMGPU_ECUDA, "vertical_velocity: %s", cudaGetErrorString(e));
   return PYOMGPU_OK;

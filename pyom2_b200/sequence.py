@@ -5,8 +5,11 @@ pyOM2's time step calls ``momentum`` (for_src/main/momentum.f90:4), which
 builds the momentum tendencies ``du, dv`` at ``tau`` (Coriolis, metric terms,
 the surface wind stress ``surface_taux/dzt(nz)`` at momentum.f90:86-93,
 advection, friction) and then ``solve_streamfunction`` (momentum.f90:159).
-Only the solve is rebuilt here, so the tendencies are a stated synthetic
-sequence instead of the model's own: per ensemble member,
+:class:`ChannelEnsemble` runs the model's own momentum tendencies on the GPU
+(pyomgpu_momentum_tendencies: Coriolis and metric terms, wind stress,
+advection, implicit vertical, harmonic and bottom friction with the
+reference's channel set-up, :func:`channel_physics`), or, with physics =
+"synthetic", a stated sequence: per ensemble member,
 
 * du(:,:,:,tau) = maskU * (sum_q a_q(t) Bu_q) plus, on the top level, the
   zonal wind stress 0.1 N/m^2 / rho_0 (1e-4 m^2/s^2) with a sin^2 profile
@@ -110,10 +113,47 @@ class TendencySequence:
         out_rho.copy_((a[2] @ Br).view(out_rho.shape) + rb)
 
 
-class ChannelEnsemble:
-    """``members`` copies of the config-4 channel, stepped together on the GPU."""
+KAPPA_M = 1e-4  # vertical viscosity (m^2/s): kappaM_0 of a set-up without the TKE closure
 
-    def __init__(self, W, members: int = 8, seed: int = 1004, limits=None):
+
+def channel_physics(M):
+    """The momentum set-up of the channel (the reference's channel set-up,
+    py_config/acc2.py:41-49,95, without its closures): Coriolis frequency
+    2 omega sin(lat); harmonic friction with cos scaling (power 1) and
+    A_h = (dx degtom)^3 2e-11 for the zonal cell width dx in degrees; linear
+    bottom friction r_bot = 1e-5 /s; implicit vertical friction with a
+    constant kappaM = KAPPA_M; zonal wind stress 0.1 N/m^2 / rho_0 with a sin^2
+    profile across the channel."""
+    from .model import DEGTOM
+    omega = float(np.float32(np.pi)) / 43082.0  # main_module.f90:16, pi a default real
+    M.coriolis_t[...] = (2 * omega * np.sin(M.yt / 180.0 * np.pi))[None, :]
+    dx_deg = float(M.dxt[2]) / DEGTOM
+    M.enable_hor_friction = True
+    M.enable_hor_friction_cos_scaling = True
+    M.hor_friction_cosPower = 1
+    M.A_h = (dx_deg * DEGTOM) ** 3 * 2e-11
+    M.enable_bottom_friction = True
+    M.r_bot = 1e-5
+    M.enable_implicit_vert_friction = True
+    M.kappaM[...] = KAPPA_M
+    y0, y1 = M.yu[2], M.yu[M.ny + 1]
+    prof = np.sin(np.pi * (M.yt - y0) / (y1 - y0)) ** 2
+    M.surface_taux[...] = M.maskU[:, :, -1] * (TAUX * prof)[None, :]
+    M.surface_tauy[...] = 0.0
+
+
+class ChannelEnsemble:
+    """``members`` copies of the config-4 channel, stepped together on the GPU.
+
+    physics = "momentum": every step runs the model's own momentum tendencies
+    (pyomgpu_momentum_tendencies with :func:`channel_physics`), the
+    external-mode solve, and the end of the reference's step (cyclic halos of
+    u, v and vertical_velocity); the members differ by their seeded density
+    perturbation (0.1 K of temperature noise), which stays fixed (the tracer
+    equations are outside this path).  physics = "synthetic": the stated
+    tendency sequence of :class:`TendencySequence`."""
+
+    def __init__(self, W, members: int = 8, seed: int = 1004, limits=None, physics: str = "momentum"):
         import torch
         self.W, self.M, self.members = W, W.M, int(members)
         M = self.M
@@ -130,16 +170,32 @@ class ChannelEnsemble:
         dev = torch.device("cuda")
         z = lambda *s: torch.zeros(tuple(reversed(s)), dtype=torch.float64, device=dev)
         H = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float64).T)).to(dev)
+        self.physics = physics
+        if physics not in ("momentum", "synthetic"):
+            raise ValueError(physics)
         self.shared = {"dzt": H(M.dzt), "dzw": H(M.dzw), "maskT": H(M.maskT), "maskU": H(M.maskU),
                        "maskV": H(M.maskV)}
+        if physics == "momentum":
+            channel_physics(M)
+            for n in ("tantr", "maskW", "coriolis_t", "area_t", "area_u", "area_v", "surface_taux",
+                      "surface_tauy", "kappaM"):
+                self.shared[n] = H(getattr(M, n))
+            self.kbot = torch.from_numpy(np.ascontiguousarray(np.asarray(M.kbot, dtype=np.int32).T)).to(dev)
         self.D = []
         for _ in range(self.members):
             d = {n: z(X, Y, nz, 3) for n in ("u", "v", "du", "dv", "rho")}
             d.update({n: z(X, Y, nz) for n in ("du_mix", "dv_mix", "p_hydro")})
             d.update({"psi": z(X, Y, 3), "dpsi": z(X, Y, 3), "dpsin": z(max(1, self.nisle), 3),
                       "forc": z(X, Y)})
+            if physics == "momentum":
+                d["w"] = z(X, Y, nz, 3)
             self.D.append(d)
         self.seq = TendencySequence(M, self.members, seed + 7)
+        if physics == "momentum":  # each member's density: background plus its own fixed perturbation
+            for m in range(self.members):
+                rho = self.seq.host_fields(m)[2]
+                for lev in range(3):
+                    self.D[m]["rho"][lev].copy_(torch.from_numpy(np.ascontiguousarray(rho.T)))
         self.taum1, self.tau, self.taup1 = 1, 2, 3
         self.itt = 0
         self._L = _abi.load()
@@ -157,6 +213,25 @@ class ChannelEnsemble:
             setattr(s, n, t.data_ptr())
         return s
 
+    def _momentum(self, m):
+        M, d = self.M, self.D[m]
+        p = _abi.Momentum()
+        p.nz, p.taum1, p.tau, p.taup1 = M.nz, self.taum1, self.tau, self.taup1
+        p.coord_degree = int(bool(M.coord_degree))
+        p.enable_hor_friction = int(M.enable_hor_friction)
+        p.enable_hor_friction_cos_scaling = int(M.enable_hor_friction_cos_scaling)
+        p.hor_friction_cospower = int(M.hor_friction_cosPower)
+        p.enable_bottom_friction = int(M.enable_bottom_friction)
+        p.enable_implicit_vert_friction = int(M.enable_implicit_vert_friction)
+        p.dt_mom, p.A_h, p.r_bot = float(M.dt_mom), float(M.A_h), float(M.r_bot)
+        for n, t in self.shared.items():
+            if hasattr(p, n):
+                setattr(p, n, t.data_ptr())
+        p.kbot = self.kbot.data_ptr()
+        for n in ("u", "v", "w", "du", "dv", "du_mix", "dv_mix"):
+            setattr(p, n, d[n].data_ptr())
+        return p
+
     def dpsi_taup1(self, m):
         """Fortran-ordered (nx+4, ny+4) view of dpsi(:,:,taup1) of member m."""
         return self.D[m]["dpsi"][self.taup1 - 1].T
@@ -165,13 +240,20 @@ class ChannelEnsemble:
         """One time step of every member; returns per-member solve infos.
         ``host_inputs`` (list of (du, dv, rho) numpy arrays per member)
         replaces the device-generated sequence (used by the parity tests)."""
-        self.seq.advance()
         st = _stream()
         states = []
+        moms = []
+        if self.physics == "synthetic":
+            self.seq.advance()
         for m in range(self.members):
             d = self.D[m]
             lv = self.tau - 1
-            if host_inputs is None:
+            if self.physics == "momentum" and host_inputs is None:
+                # momentum.f90:4-152: du, dv at tau, du_mix, dv_mix; rho stays the member's
+                p = self._momentum(m)
+                moms.append(p)
+                _abi.check(self._L.pyomgpu_momentum_tendencies(self.ems[m]._ctx, C.byref(p), st))
+            elif host_inputs is None:
                 self.seq.device_fields(m, d["du"][lv], d["dv"][lv], d["rho"][lv])
             else:
                 import torch
@@ -184,6 +266,8 @@ class ChannelEnsemble:
         infos = self._solve(method, rtol, states)
         for m in range(self.members):
             _abi.check(self._L.pyomgpu_solve_streamfunction_end(self.ems[m]._ctx, C.byref(states[m]), st))
+            if moms:  # the end of the reference's step (main.f90:114-117,147)
+                _abi.check(self._L.pyomgpu_vertical_velocity(self.ems[m]._ctx, C.byref(moms[m]), self.taup1, st))
         self.taum1, self.tau, self.taup1 = self.tau, self.taup1, self.taum1
         self.itt += 1
         return infos

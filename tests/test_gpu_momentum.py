@@ -61,3 +61,38 @@ def test_momentum_matches_reference_source():
     for n in ("u", "v"):
         assert rel(getattr(M, n)[:, :, :, tp1][IN], g[n + "_taup1"][IN]) < 1e-9, n
     E.close()
+
+
+def test_ensemble_with_momentum_physics_matches_the_host_path():
+    """Two steps of a member of the channel ensemble (device tensors, the
+    model's own tendencies, the reference's stop) equal the same steps run
+    through ExternalMode on host arrays: momentum, solve_streamfunction, the
+    cyclic halos and vertical_velocity of the new level."""
+    from pyom2_b200 import synth
+    from pyom2_b200.sequence import ChannelEnsemble, channel_physics
+
+    W = synth.config4(1004, nx=48, ny=32, nz=6)
+    ens = ChannelEnsemble(W, members=2, seed=1004)
+    M = W.M.copy()
+    channel_physics(M)
+    rho = ens.seq.host_fields(1)[2]
+    for lev in range(3):
+        M.rho[..., lev] = rho
+    E = ExternalMode(M)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        E.streamfunction_init(maxipp=10**6, maxq=10**6)
+    for step in range(2):
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            ens.step("ref")
+            E.momentum(M)
+            E.solve_streamfunction(M)
+        E.vertical_velocity(M, level=M.taup1)
+        M.taum1, M.tau, M.taup1 = M.tau, M.taup1, M.taum1
+        h = ens.host_state(1, names=("u", "v", "w", "psi", "dpsi"))
+        for n in ("u", "v", "w", "psi", "dpsi"):
+            assert np.array_equal(h[n], getattr(M, n)), (step, n, float(np.abs(h[n] - getattr(M, n)).max()))
+    assert np.abs(M.u).max() > 0
+    ens.close()
+    E.close()
