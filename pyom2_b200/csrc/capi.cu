@@ -494,28 +494,17 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   auto& B = o->batch;
   CK(cudaMemsetAsync(B.pool, 0, pool * sizeof(double), st));
   CK(cudaMemsetAsync(B.sync, 0, 8 * sizeof(unsigned long long), st));
-  // groups whose fields (about 72 bytes per padded point: sol, res, two directions, As,
-  // FX, FY, Z, forc) stay in L2: largest problems first, packed greedily into 60 % of L2;
-  // the kernel solves the groups one after another
+  // all problems in one group, largest first: every sweep and barrier serves every
+  // problem still running, so the barrier latency is shared by all of them (solving
+  // L2-sized groups one after another measured slower: each group then pays the
+  // latency-bound iterations of its slowest problem on its own)
   std::vector<int> order((size_t)count);
   for (int k = 0; k < count; ++k) order[k] = k;
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return v[a].c->g.size() > v[b].c->g.size(); });
-  const size_t budget = B.l2_bytes ? B.l2_bytes * 6 / 10 : ((size_t)64 << 20);
-  int ngroup = 0;
-  {
-    size_t acc = 0;
-    B.h_group[0] = 0;
-    for (int pos = 0; pos < count; ++pos) {
-      const size_t ws = 72 * v[order[pos]].c->g.size();
-      if (pos > B.h_group[ngroup] && acc + ws > budget) {
-        B.h_group[++ngroup] = pos;
-        acc = 0;
-      }
-      acc += ws;
-    }
-    B.h_group[++ngroup] = count;
-  }
+  const int ngroup = 1;
+  B.h_group[0] = 0;
+  B.h_group[1] = count;
   double* cur = B.pool;
   int tile0 = 0;
   for (int pos = 0; pos < count; ++pos) {

@@ -289,6 +289,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
       const int lt = task - pr.tile0;
       const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
       __syncthreads();  // shared boxes of the previous task are free
+      // four box points per thread in flight (the loads do not depend on the shared stores)
+#pragma unroll 4
       for (int e = threadIdx.x; e < kBoxN; e += kBatchThreads) {
         const int i = i0 - 1 + e % kBX, j = j0 - 1 + e / kBX;
         double r = 0.0, w = 0.0, s = 0.0, fx = 0.0, fy = 0.0;
@@ -341,6 +343,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
       const int lt = task - pr.tile0;
       const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
       double v[2] = {0.0, 0.0};
+#pragma unroll 4
       for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
         const int i = i0 + e % kTX, j = j0 + e / kTX;
         if (i > g.nx || j > g.ny) continue;
