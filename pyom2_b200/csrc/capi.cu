@@ -196,7 +196,7 @@ int res_plan(pyomgpu_ctx* c) {
   }
   const int nb = R.npx * R.npy;
   if (int rc = dalloc(&R.hx, 8 * c->g.size())) return rc;  // two record buffers
-  if (int rc = dalloc(&R.slots, (size_t)3 * (nb + 1) * kResSlotWords)) return rc;
+  if (int rc = dalloc(&R.slots, (size_t)4 * (nb + 1) * kResSlotWords)) return rc;
   R.ok = true;
   return PYOMGPU_OK;
 }
@@ -214,7 +214,7 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   const int nb = R.npx * R.npy;
   CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
   CK(cudaMemsetAsync(c->res, 0, bytes, st));
-  CK(cudaMemsetAsync(R.slots, 0xFF, (size_t)3 * (nb + 1) * kResSlotWords * sizeof(double), st));
+  CK(cudaMemsetAsync(R.slots, 0xFF, (size_t)4 * (nb + 1) * kResSlotWords * sizeof(double), st));
   CGResParams P{};
   P.g = c->g;
   P.op = c->sf.dev();
@@ -236,6 +236,8 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   P.timeout_ns = (unsigned long long)(c->timeout_s * 1e9);
   P.stall_extra = c->stall_next;
   c->stall_next = 0;
+  P.tag_gen = R.tag_gen;  // tags of this solve's slots and records differ from the previous solve's
+  R.tag_gen = (R.tag_gen + 1u) % 4095u;
   P.out = c->d_result;
   const bool trace = R.trace_nit > 0 && c->cg_kernel != 3;
   P.trace = trace ? R.trace : nullptr;

@@ -71,6 +71,36 @@ __device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
 // released words of every slot, one fence makes everything released before
 // them visible (the acquire pattern of the PTX memory model).
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// ---- tagged words (two-reduction kernel) --------------------------------------
+// A double travels as two 64-bit words, (tag << 32) | low half and (tag << 32) |
+// high half, stored and loaded relaxed.  64-bit accesses are single-copy atomic,
+// so a reader that sees the current tag in both words has both halves of the
+// current value; a stale word carries an older tag.  No ordering between words
+// is needed, hence no release, acquire or emptying.  The tag is the solve's
+// generation (12 bits) and the epoch (20 bits; a stale word is at most two epochs
+// old, so the wrap-around cannot confuse them).
+__device__ __forceinline__ unsigned res_tag(const CGResParams& P, unsigned ep) {
+  return (P.tag_gen << 20) | (ep & 0xFFFFFu);
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long tag_lo(unsigned tag, double v) {
+  return ((unsigned long long)tag << 32) | (unsigned)__double2loint(v);
+}
+__device__ __forceinline__ unsigned long long tag_hi(unsigned tag, double v) {
+  return ((unsigned long long)tag << 32) | (unsigned)__double2hiint(v);
+}
+__device__ __forceinline__ bool tag_ok(unsigned long long w, unsigned tag) { return (unsigned)(w >> 32) == tag; }
+__device__ __forceinline__ double untag(unsigned long long lo, unsigned long long hi) {
+  return __hiloint2double((int)(unsigned)hi, (int)(unsigned)lo);
+}
 __device__ __forceinline__ void st_release_f64(double* p, double v) {
   asm volatile("st.release.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
@@ -94,6 +124,27 @@ __device__ __forceinline__ void publish_cyclic(double* a, const Geo& g, int i, i
   if (yc != 0x7fffffff) {
     st_weak_f64(a + 4 * g.at(i, yc), v);
     if (xc != 0x7fffffff) st_weak_f64(a + 4 * g.at(xc, yc), v);
+  }
+}
+
+// Writes (q, s) as the tagged record of interior (i,j) -- 4 words at 4 * position:
+// q low, q high, s low, s high -- and of the halo positions setcyclic_xy fills from it.
+__device__ __forceinline__ void publish_cyclic_tagged(unsigned long long* a, const Geo& g, int i, int j, double q,
+                                                      double s, unsigned tag) {
+  const unsigned long long w0 = tag_lo(tag, q), w1 = tag_hi(tag, q), w2 = tag_lo(tag, s), w3 = tag_hi(tag, s);
+  auto put = [&](size_t pos) {
+    st_relaxed_u64(a + 4 * pos, w0);
+    st_relaxed_u64(a + 4 * pos + 1, w1);
+    st_relaxed_u64(a + 4 * pos + 2, w2);
+    st_relaxed_u64(a + 4 * pos + 3, w3);
+  };
+  put(g.at(i, j));
+  int xc, yc;
+  cyclic_copies(g, i, j, xc, yc);
+  if (xc != 0x7fffffff) put(g.at(xc, j));
+  if (yc != 0x7fffffff) {
+    put(g.at(i, yc));
+    if (xc != 0x7fffffff) put(g.at(xc, yc));
   }
 }
 
@@ -333,6 +384,33 @@ __device__ __forceinline__ void worker_halo_load(const CGResParams& P, Halo (&hl
     }
 }
 
+// Loads this thread's halo values from tagged records, polling (bounded) a
+// record until both of its values carry `tag`.  False on time-out.
+__device__ __forceinline__ bool worker_halo_load_tagged(const CGResParams& P, Halo (&hl)[2], unsigned tag) {
+  const unsigned long long* hx = reinterpret_cast<const unsigned long long*>(P.hx);
+  const unsigned long long t0 = globaltimer_ns();
+  // one record after the other (a worker rarely has two): four words live at a time
+#pragma unroll 1
+  for (int e = 0; e < 2; e++) {
+    if (hl[e].sidx < 0) continue;
+    const unsigned long long* r = hx + 4 * hl[e].gidx;
+    for (unsigned spin = 1;; spin++) {
+      const unsigned long long w0 = ld_relaxed_u64(r), w1 = ld_relaxed_u64(r + 1), w2 = ld_relaxed_u64(r + 2),
+                               w3 = ld_relaxed_u64(r + 3);
+      if (tag_ok(w0, tag) && tag_ok(w1, tag) && tag_ok(w2, tag) && tag_ok(w3, tag)) {
+        hl[e].q = untag(w0, w1);
+        hl[e].s = untag(w2, w3);
+        break;
+      }
+      if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
+        atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
 // Boundary staging: the values of a piece's boundary points in shared memory,
 // entries [0,ph) west column, [ph,2ph) east column, [2ph,2ph+pw) south row,
 // [2ph+pw,2ph+2pw) north row (a corner point in two entries); quantity k of
@@ -380,6 +458,37 @@ __device__ __forceinline__ void copy_out(const CGResParams& P, double* hx, const
   }
 }
 
+// copy_out<2> for tagged records: (Z res, direction) of each staged boundary entry.
+__device__ __forceinline__ void copy_out_tagged(const CGResParams& P, const double* spub, int ilo, int ihi, int jlo,
+                                                int jhi, int wt, unsigned tag) {
+  const Geo& g = P.g;
+  unsigned long long* hx = reinterpret_cast<unsigned long long*>(P.hx);
+  const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, nent = 2 * (pw + ph);
+#pragma unroll 1
+  for (int e = wt; e < nent; e += kResWorkers) {
+    int i, j;
+    bool need;
+    if (e < ph) {
+      i = ilo;
+      j = jlo + e;
+      need = ilo > 1 || g.cyclic_x;
+    } else if (e < 2 * ph) {
+      i = ihi;
+      j = jlo + e - ph;
+      need = ihi < g.nx || g.cyclic_x;
+    } else if (e < 2 * ph + pw) {
+      i = ilo + e - 2 * ph;
+      j = jlo;
+      need = jlo > 1 || g.cyclic_y;
+    } else {
+      i = ilo + e - 2 * ph - pw;
+      j = jhi;
+      need = jhi < g.ny || g.cyclic_y;
+    }
+    if (need) publish_cyclic_tagged(hx, g, i, j, spub[e], spub[nent + e], tag);
+  }
+}
+
 __device__ __forceinline__ double* res_slot(const CGResParams& P, unsigned ep, int b) {
   return P.slots + ((size_t)(ep % 3u) * P.nslot + b) * kResSlotWords;
 }
@@ -401,12 +510,32 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // blocks until no word is empty; the totals are formed in a fixed order, so
 // every block obtains the same bits, and lane 0 advances the control state.
 // False on time-out.
-template <int NV, int kMaxSlot, int kStep>
+template <int NV, int kMaxSlot, int kStep, bool TAG = false>
 __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int npoll, ResCtl& C,
                                                  const double (*wred)[kResSlotWords], unsigned* hflag = nullptr,
                                                  unsigned long long* tr = nullptr) {
   const int lane = threadIdx.x;
-  {
+  const unsigned tag = res_tag(P, ep);
+  // tagged slots: 2 buffers x nslot x 2 kResSlotWords words; a block overwrites its
+  // slot of epoch ep at ep+2, when every block has published ep+1, i.e. finished
+  // reading epoch ep
+  auto tslot = [&](unsigned e, int b) {
+    return reinterpret_cast<unsigned long long*>(P.slots) + ((size_t)(e & 1u) * P.nslot + b) * (2 * kResSlotWords);
+  };
+  if constexpr (TAG) {
+    double t[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const double x = (lane >= 1 && lane < kResThreads / 32) ? wred[lane][k] : 0.0;
+      t[k] = (k == kMaxSlot) ? warp_max(x) : warp_sum(x);
+    }
+    double mv = 0.0;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+      if ((lane >> 1) == k) mv = t[k];
+    if (lane < 2 * NV) st_relaxed_u64(tslot(ep, blockIdx.x) + lane, (lane & 1) ? tag_hi(tag, mv) : tag_lo(tag, mv));
+    if (tr != nullptr && lane == 0) tr[0] = globaltimer_ns();
+  } else {
     double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
 #pragma unroll
     for (int k = 0; k < NV; k++) {
@@ -436,6 +565,31 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
   }
   bool ok = true;
   const unsigned long long t0 = globaltimer_ns();
+  if constexpr (TAG) {
+    // every tagged word of every slot this lane polls in one pass of relaxed loads
+    for (unsigned spin = 1; have != want; spin++) {
+      const unsigned pend = want & ~have;
+#pragma unroll
+      for (int m = 0; m < kPer; m++) {
+        if (!(pend >> m & 1u)) continue;
+        const unsigned long long* sl = tslot(ep, lane + 32 * m);
+        bool all = true;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+          const unsigned long long lo = ld_relaxed_u64(sl + 2 * k), hi = ld_relaxed_u64(sl + 2 * k + 1);
+          all = all && tag_ok(lo, tag) && tag_ok(hi, tag);
+          got[m][k] = untag(lo, hi);  // kept only once every word of the slot is current
+        }
+        if (all) have |= 1u << m;
+      }
+      if (have != want && (spin & 31u) == 0u &&
+          (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
+        atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+        ok = false;
+        break;
+      }
+    }
+  } else {
   // every word of every slot this lane polls is loaded relaxed in one pass (the
   // loads are independent: one L2 round trip per pass) and validated on its own:
   // a word is either empty or this epoch's value (a slot is emptied two epochs
@@ -464,19 +618,23 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
     }
   }
   fence_acq_rel_gpu();
+  }
   if (tr != nullptr && lane == 0) tr[1] = globaltimer_ns();
   if (hflag != nullptr) {
-    // every slot is acquired, so the exchange records released with them are
-    // visible: let the workers start loading their halo before the control step
+    // every slot is acquired, so the exchange records written before them are
+    // visible (released with them, or tagged and validated by the readers): let
+    // the workers start loading their halo before the control step
     __syncwarp();
     if (lane == 0) st_release_cta_u32(hflag, ld_relaxed_cta_u32(hflag) + 1u);
   }
-  // once every lane has seen its slots of epoch ep, every block has finished
-  // reading epoch ep-1 (it published epoch ep), so this block's slot of that
-  // buffer (= the one of epoch ep+2) is free; the next publication's release
-  // orders these stores before it
-  __syncwarp();
-  if (lane < kResSlotWords) st_weak_f64(res_slot(P, ep + 2, blockIdx.x) + lane, empty_word());
+  if constexpr (!TAG) {
+    // once every lane has seen its slots of epoch ep, every block has finished
+    // reading epoch ep-1 (it published epoch ep), so this block's slot of that
+    // buffer (= the one of epoch ep+2) is free; the next publication's release
+    // orders these stores before it
+    __syncwarp();
+    if (lane < kResSlotWords) st_weak_f64(res_slot(P, ep + 2, blockIdx.x) + lane, empty_word());
+  }
   double out[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) {
@@ -519,6 +677,20 @@ __device__ __forceinline__ bool worker_halo_early(const CGResParams& P, const un
     }
   worker_halo_load(P, hl);
   return true;
+}
+
+// worker_halo_early for tagged records: waits (bounded) for the controller to
+// acquire every slot of the halo-carrying reduction `target`, then loads the
+// halo, polling each record until it carries that reduction's tag.
+__device__ __forceinline__ bool worker_halo_early_tagged(const CGResParams& P, const unsigned* hflag,
+                                                         unsigned target, Halo (&hl)[2]) {
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned spin = 1; ld_acquire_cta_u32(hflag) < target; spin++)
+    if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
+      atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+      return false;
+    }
+  return worker_halo_load_tagged(P, hl, res_tag(P, 2u * (target - 1u)));
 }
 
 __device__ __forceinline__ void workers_sync() {
@@ -592,14 +764,14 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     unsigned ep = 0;
     bool stopped_after_update = false;  // the stop decided before sweep B (C stays as the workers read it)
     __syncthreads();  // S1
-    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred, &s_hflag);
+    bool ok = controller_epoch<4, 3, kStepInit, true>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred, &s_hflag);
     if (!__syncthreads_and(ok)) goto out;  // S2
     if (C.act == kRun) {
       for (unsigned trip = 0;; trip++) {
         unsigned long long* tr = threadIdx.x == 0 ? trace_row(trip) : nullptr;
         __syncthreads();  // S1: partials of sweep A
         if (TRACE && tr) tr[10] = globaltimer_ns();
-        ok = controller_epoch<2, 1, kStepA>(Pm, ++ep, nb, C, wred, nullptr, TRACE && tr ? tr + 11 : nullptr);
+        ok = controller_epoch<2, 1, kStepA, true>(Pm, ++ep, nb, C, wred, nullptr, TRACE && tr ? tr + 11 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
         if (C.stop_after) {  // the workers finish sweep B and stop
@@ -608,7 +780,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         }
         __syncthreads();  // S1: partials of sweep B
         if (TRACE && tr) tr[14] = globaltimer_ns();
-        ok = controller_epoch<2, -1, kStepB>(Pm, ++ep, nb, C, wred, &s_hflag, TRACE && tr ? tr + 15 : nullptr);
+        ok = controller_epoch<2, -1, kStepB, true>(Pm, ++ep, nb, C, wred, &s_hflag,
+                                                   TRACE && tr ? tr + 15 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
       }
@@ -711,9 +884,9 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
       worker_partials<4, 3>(v, wred);
     }
     workers_sync();
-    copy_out<2>(Pm, Pm.hx, spub, ilo, ihi, jlo, jhi, wt);
+    copy_out_tagged(Pm, spub, ilo, ihi, jlo, jhi, wt, res_tag(Pm, 2u * hready));
     __syncthreads();  // S1
-    if (!__syncthreads_and(worker_halo_early(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
+    if (!__syncthreads_and(worker_halo_early_tagged(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
     if (C.act != kRun) goto done;
 
     for (unsigned trip = 0;; trip++) {
@@ -813,7 +986,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           }
         if (TRACE && tr) tr[5] = globaltimer_ns();
         workers_sync();
-        copy_out<2>(Pm, Pm.hx, spub, ilo, ihi, jlo, jhi, wt);
+        copy_out_tagged(Pm, spub, ilo, ihi, jlo, jhi, wt, res_tag(Pm, 2u * hready));
         if (TRACE && tr) tr[6] = globaltimer_ns();
         if (!stop_after) {
           worker_partials<2, -1>(v, wred);
@@ -837,7 +1010,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         if (TRACE && tr) tr[8] = globaltimer_ns();
         if (stop_after) goto done;
       }
-      if (!__syncthreads_and(worker_halo_early(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
+      if (!__syncthreads_and(worker_halo_early_tagged(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
       if (TRACE && tr) tr[9] = globaltimer_ns();
       if (C.act != kRun) goto done;
     }

@@ -27,7 +27,9 @@ struct CGResParams {
                        // the two-reduction kernel, (res, A Z res, A p) in two alternating buffers
                        // (8 words per position) for the single-reduction one
   long long hsize;     // padded positions (records)
-  double* slots;       // 3 buffers x nslot x kResSlotWords reduction words, all empty on entry
+  double* slots;       // 4 x nslot x kResSlotWords words: 3 rotating buffers of kResSlotWords words per
+                       // block (single-reduction kernel; all empty on entry), or 2 buffers of
+                       // 2 kResSlotWords tagged words per block (two-reduction kernel)
   int nslot;           // gridDim.x + 1
   int npx, npy;        // pieces in x and y (gridDim.x = npx * npy)
   int wmax, hmax;      // largest piece extents: shared-memory layout and thread columns
@@ -37,6 +39,8 @@ struct CGResParams {
   SyncCtl* ctl;
   unsigned long long timeout_ns;
   unsigned stall_extra;  // test hook: the first reduction also awaits a slot nobody writes
+  unsigned tag_gen;      // 0 .. 4094, different for consecutive solves of a context: the high bits of
+                         // the epoch tags of the two-reduction kernel's slots and exchange records
   CGResult* out;
   // phase timestamps of the traced instantiation (cg_res_kernel<P, true>):
   // %globaltimer at kResTracePhases points of loop trips trace_it0 ..

@@ -101,6 +101,7 @@ struct pyomgpu_ctx {
     int npx = 0, npy = 0, wmax = 0, hmax = 0, p = 0;
     size_t smem = 0;
     double *hx = nullptr, *slots = nullptr;
+    unsigned tag_gen = 0;  // generation of the next solve's epoch tags (0 .. 4094)
     // phase trace of the next resident solve (pyomgpu_resident_trace): device
     // buffer of trace_cap words, loop trips trace_it0 .. trace_it0 + trace_nit - 1
     unsigned long long* trace = nullptr;
