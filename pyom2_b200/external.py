@@ -365,13 +365,18 @@ class ExternalMode:
                 a[...] = _from_device_f(D[n])
 
     def vertical_velocity(self, M=None, level=None):
-        """vertical_velocity.f90: w(:,:,:,level) from u, v at level (default taup1)."""
+        """The end of the reference's step for ``level`` (default taup1): the
+        cyclic halos of u, v (main.f90:114-117), then vertical_velocity.f90:
+        w(:,:,:,level) from u, v at level.  Host arrays u, v, w are written
+        back; CUDA tensors are updated in place."""
         M = M or self.M
         m, D = self._momentum_struct(M)
         lev = int(M.taup1 if level is None else level)
         _abi.check(self._L.pyomgpu_vertical_velocity(self._ctx, C.byref(m), lev, _stream()))
-        if not _is_torch(M.w):
-            M.w[...] = _from_device_f(D["w"])
+        for n in ("u", "v", "w"):
+            a = getattr(M, n)
+            if not _is_torch(a):
+                a[...] = _from_device_f(D[n])
 
 
 # ---------------------------------------------------------------------------
