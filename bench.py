@@ -209,9 +209,12 @@ def run_reference(args, rank, world):
 
 def c2_batch(steps, warmup, count=64):
     """Config 2: 64 closed basins (128-1024 x 128-768, 10-40 % land, 0-12
-    islands), each solved to FP64 relative residual 1e-10 from zero: all 64 in
-    one work-queue launch (congrad_streamfunction_batch) against 64
-    sequential solve_rtol calls.  Device time by CUDA events."""
+    islands), each solved to the FP64 relative residual RTOL from zero, three
+    ways: congrad_streamfunction_batch on groups of SMs running on-chip
+    solves side by side (the automatic engine where every grid fits), the
+    same call on the work-queue kernel (all 64 grids streamed through HBM in
+    lockstep), and 64 sequential solve_rtol calls (each grid alone on all
+    SMs).  Device time by CUDA events."""
     import warnings
 
     import torch
@@ -244,23 +247,33 @@ def c2_batch(steps, warmup, count=64):
                 out.append(e0.elapsed_time(e1))
         return statistics.median(out), r
 
-    batch_ms, infos = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL))
+    batch_ms, infos = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL,
+                                                                 kernel="resident"))
+    queue_ms, qinfos = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL,
+                                                                  kernel="queue"))
     seq_ms, seq = timed(lambda: [E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64)
                                  for E, f, x in zip(ems, forcs, sols)])
     return {"grids": len(ws), "points": int(sum(w.M.nx * w.M.ny for w in ws)),
-            "islands": int(sum(int(w.M.nisle) for w in ws)), "batch_ms": batch_ms, "sequential_ms": seq_ms,
-            "speedup": seq_ms / batch_ms, "batch_max_rel_residual": max(i["rel_residual"] for i in infos),
+            "islands": int(sum(int(w.M.nisle) for w in ws)), "batch_ms": batch_ms, "queue_ms": queue_ms,
+            "sequential_ms": seq_ms, "speedup": seq_ms / batch_ms, "queue_speedup": seq_ms / queue_ms,
+            "batch_max_rel_residual": max(i["rel_residual"] for i in infos),
+            "queue_max_rel_residual": max(i["rel_residual"] for i in qinfos),
             "sequential_max_rel_residual": max(i["rel_residual"] for i in seq),
+            "batch_launches": int(infos[0]["kernel_launches"]) - len(ws) * 5,
             "iterations_max": max(i["iterations"] for i in infos),
             "iterations_sum": int(sum(i["iterations"] for i in infos)),
-            "note": "one launch for all 64 grids vs one launch per grid; FP64 Jacobi-PCG, same stop"}
+            "note": "batch: resident solves side by side on groups of SMs (one launch per group size); queue: "
+                    "one work-queue launch streaming all 64 grids; sequential: one resident launch per grid; "
+                    "FP64 Jacobi-PCG, same stop"}
 
 
 def c3_learned(steps, warmup):
-    """Config 3: the learned FCG on the 2048x1024 grid (config-1 recipe, seed
-    1003; the network is trained on the 1440x720 family and applied to this
-    larger grid unchanged) against FP64 Jacobi-PCG, both from zero to the FP64
-    true relative residual 1e-10.  Device time by CUDA events."""
+    """Config 3, the 2048x1024 grid (config-1 recipe, seed 1003): FP64
+    Jacobi-PCG (the tiled kernel: FP64 fields do not fit on chip), the mixed
+    path (FP32 correction solves on the FP32 resident kernel, which fits) and
+    the learned FCG (the network is trained on the 1440x720 family and
+    applied to this larger grid unchanged), each from zero to the FP64 true
+    relative residual RTOL.  Device time by CUDA events."""
     import warnings
 
     import torch
@@ -274,8 +287,10 @@ def c3_learned(steps, warmup):
     f = torch.from_numpy(np.ascontiguousarray(W.forc.T)).cuda().T
     x = torch.zeros_like(f.T).T
     stream = torch.cuda.current_stream()
-    out = {"workload": f"c3_{W.M.nx}x{W.M.ny}", "nisle": int(W.M.nisle), "rtol": RTOL}
+    out = {"workload": f"c3_{W.M.nx}x{W.M.ny}", "nisle": int(W.M.nisle), "rtol": RTOL,
+           "resident_fp64": E.resident_layout(), "resident_fp32": E.resident_layout(fp32=True)}
     for name, fn in (("pcg64", lambda: E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64)),
+                     ("mixed32", lambda: E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F32)),
                      ("fcg", lambda: learned.solve_fcg(E, pc, f, x, rtol=RTOL))):
         ms, info = [], None
         for k in range(warmup + steps):
@@ -290,6 +305,7 @@ def c3_learned(steps, warmup):
         out[name] = {"ms": statistics.median(ms), "iterations": info["iterations"],
                      "outer_iterations": info["outer_iterations"], "rel_residual": info["rel_residual"]}
     out["fcg_speedup_vs_pcg64"] = out["pcg64"]["ms"] / out["fcg"]["ms"]
+    out["mixed32_speedup_vs_pcg64"] = out["pcg64"]["ms"] / out["mixed32"]["ms"]
     pc.close()
     return out
 
@@ -420,7 +436,8 @@ METHODS = {
     # where the grid fits) and forced to the tiled kernel
     "pcg64": ("PREC_F64", "f64", "f64", None),
     "pcg64_tiled": ("PREC_F64", "f64", "f64", "cg_ref_kernel<false>"),
-    "mixed32": ("PREC_F32", "f32+f64", "f32", "cg_pipe_kernel<float>"),
+    # FP32 correction solves: the FP32 resident kernel where the grid fits, else the pipelined tile kernel
+    "mixed32": ("PREC_F32", "f32+f64", "f32", None),
     # flexible CG with the learned U-Net (bf16 tensor-core network, FP64 vectors)
     "fcg": (None, "f64+bf16", "f64", "conv3x3_tc_kernel"),
 }
@@ -531,7 +548,10 @@ def main():
     for name in [m for m in args.methods.split(",") if m]:
         code, dtype, bkey, kname = METHODS[name]
         E.set_cg_kernel("tiled" if name == "pcg64_tiled" else "auto")
-        if kname is None:
+        if kname is None and name == "mixed32":
+            lay32 = E.resident_layout(fp32=True)
+            kname = f"cg_res32_kernel<{lay32[2]}>" if lay32 else "cg_pipe_kernel<float>"
+        elif kname is None:
             kname = E.resident_kernel_name() if layout else "cg_ref_kernel<false>"
         for _ in range(args.warmup):
             sol_d.zero_()

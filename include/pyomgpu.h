@@ -194,6 +194,11 @@ int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* ctx, int32_t kernel);
 /* Piece layout the resident kernel uses on this grid: pieces in x and y and
  * points per thread; PYOMGPU_EINVAL when the grid does not fit. */
 int32_t pyomgpu_resident_layout(pyomgpu_ctx* ctx, int32_t* npx, int32_t* npy, int32_t* points_per_thread);
+/* The same for the FP32 resident kernel that runs the correction solves of
+ * pyomgpu_solve_rtol with PYOMGPU_PREC_F32 where the grid fits (FP32 fields
+ * take half the on-chip memory, so grids up to twice the size fit; elsewhere,
+ * or with set_cg_kernel 1, the pipelined tile kernel runs them). */
+int32_t pyomgpu_resident_layout32(pyomgpu_ctx* ctx, int32_t* npx, int32_t* npy, int32_t* points_per_thread);
 /* Diagnostics, no counterpart in the reference: one pyomgpu_solve_rtol (FP64)
  * in an instantiation of the resident kernel that records %globaltimer (ns)
  * at 18 phase boundaries of loop trips it0 .. it0+nit-1 in every block (the
@@ -348,10 +353,22 @@ int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* grid, const i
  * info's rel_residual with the FP64 true residual; congr_epsilon = 0 leaves
  * rtol as the only stop.  info: count entries or NULL; device_ms and
  * kernel_launches describe the whole call.  The work buffers live in ctx[0]
- * and grow to the largest batch it has run.  Returns the largest status. */
+ * and grow to the largest batch it has run.  Returns the largest status.
+ * Engine (pyomgpu_set_batch_kernel on ctx[0]): where every grid fits on chip,
+ * groups of SMs run on-chip-resident solves side by side (the SMs split into
+ * 1, 2, 4, 8 or 16 groups; each grid in the smallest groups it fits, longest
+ * solves first), else the work-queue kernel streams all solves through HBM
+ * in lockstep.  The rtol stop is relative to ||forc||, or to the initial
+ * residual for a zero forcing. */
 int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t count, const double* const* forc,
                                              double* const* sol, double congr_epsilon, int32_t congr_max_iterations,
                                              double rtol, pyomgpu_solve_info* info, pyomgpu_stream stream);
+
+/* Engine of pyomgpu_congrad_streamfunction_batch calls owned by ctx (ctx[0]):
+ * 0 automatic (resident groups where every grid fits on chip), 1 the
+ * work-queue kernel, 2 resident groups (PYOMGPU_EINVAL from the batch call
+ * when a grid does not fit).  No counterpart in the reference. */
+int32_t pyomgpu_set_batch_kernel(pyomgpu_ctx* ctx, int32_t kernel);
 
 /* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
  * products.  psi is psi(:,:,taup1), in/out, host or device. */

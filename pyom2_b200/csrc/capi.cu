@@ -130,53 +130,87 @@ int finish_cg(pyomgpu_ctx* c, pyomgpu_solve_info* info, cudaStream_t st) {
   return c->h_result->status;
 }
 
-// Piece layout of the resident kernel for this grid, planned once: among the
-// npx x npy cuts (at most one piece per SM, pieces at least 2 x 2) whose
-// largest piece fits in shared memory and in the worker threads, the one with
+// Cut of an nx x ny grid into npx x npy pieces for the resident kernel: among
+// the cuts into at most maxb pieces (pieces at least 2 x 2) whose largest piece
+// fits in `cap` bytes of dynamic shared memory and in the worker threads at p
+// points per thread (p = 0: the smallest instance that fits), the one with
 // the smallest estimated iteration time (shared-memory traffic of the largest
-// piece, ~0.27 ns per point, plus ~5 ns of reduction per block).  Allocates
-// the exchange buffers.  Returns PYOMGPU_OK with c->resd.ok telling whether
-// the grid fits, or an error code.
+// piece, ~0.27 ns per point, plus ~5 ns of reduction per block), or with
+// fewest_blocks the one with the fewest pieces.  False when none fits.
+struct ResCut {
+  int npx = 0, npy = 0, w = 0, h = 0, p = 0;
+  size_t smem = 0;
+  double cost = 1e300;
+};
+bool res_cut(int nx, int ny, int maxb, size_t cap, int p_fixed, bool fewest_blocks, ResCut& out, bool f32 = false) {
+  out = ResCut{};
+  static constexpr int kP32[] = {16, 32};  // FP32 instances (cg_res32_kernel)
+  const int* plist = f32 ? kP32 : kResP;
+  const int np = f32 ? 2 : kResNP;
+  for (int npx = 1; npx <= std::min(nx / 2, maxb); npx++)
+    for (int npy = 1; npy <= ny / 2 && npx * npy <= maxb; npy++) {
+      const int w = (nx + npx - 1) / npx, h = (ny + npy - 1) / npy;
+      const size_t bytes = f32 ? res32_smem_bytes(w, h) : res_smem_bytes(w, h);
+      if (bytes > cap || w + h > kResWorkers) continue;
+      int pp = 0;
+      for (int k = 0; k < np && !pp; k++)
+        if ((p_fixed == 0 || plist[k] == p_fixed) && res_threads(w, h, plist[k]) <= kResWorkers) pp = plist[k];
+      if (!pp) continue;
+      const double cost = (f32 ? 0.135 : 0.27) * w * h + 5.0 * npx * npy;
+      const bool better = fewest_blocks ? (npx * npy < out.npx * out.npy || out.npx == 0 ||
+                                           (npx * npy == out.npx * out.npy && cost < out.cost))
+                                        : cost < out.cost;
+      if (better) {
+        out.npx = npx;
+        out.npy = npy;
+        out.w = w;
+        out.h = h;
+        out.p = pp;
+        out.smem = bytes;
+        out.cost = cost;
+      }
+    }
+  return out.npx > 0;
+}
+
+// Dynamic shared memory the resident kernels may use on this device: the
+// opt-in limit less the largest static shared memory among them (0: none).
+size_t res_smem_cap(pyomgpu_ctx* c) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess) return 0;
+  size_t stat = 0;
+  std::vector<const void*> ks{cg_res_multi_kernel_ptr(), cg_res32_kernel_ptr(16), cg_res32_kernel_ptr(32)};
+  for (int k = 0; k < kResNP; k++)
+    for (bool single : {false, true}) ks.push_back(cg_res_kernel_ptr(kResP[k], single));
+  for (const void* k : ks) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) return 0;
+    stat = std::max(stat, fa.sharedSizeBytes);
+  }
+  return (size_t)optin > stat ? (size_t)optin - stat : 0;
+}
+
+// Piece layout of the resident kernel for this grid, planned once (res_cut
+// with at most one piece per SM).  Allocates the exchange buffers.  Returns
+// PYOMGPU_OK with c->resd.ok telling whether the grid fits, or an error code.
 int res_plan(pyomgpu_ctx* c) {
   auto& R = c->resd;
   if (R.planned) return PYOMGPU_OK;
   R.planned = true;
   R.ok = false;
-  int optin = 0;
-  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess)
-    return fail(PYOMGPU_ECUDA, "device attribute query failed");
-  size_t stat = 0;
-  for (int k = 0; k < kResNP; k++) {
-    for (bool single : {false, true}) {
-      cudaFuncAttributes fa{};
-      if (cudaFuncGetAttributes(&fa, cg_res_kernel_ptr(kResP[k], single)) != cudaSuccess)
-        return fail(PYOMGPU_ECUDA, "resident kernel attributes");
-      stat = std::max(stat, fa.sharedSizeBytes);
-    }
-  }
-  if ((size_t)optin <= stat) return PYOMGPU_OK;
-  const size_t cap = (size_t)optin - stat;
+  const size_t cap = res_smem_cap(c);
+  if (cap == 0) return PYOMGPU_OK;
   const int maxb = std::min(c->nsm, kResMaxSlots - 1);
-  double best = 1e300;
-  for (int npx = 1; npx <= std::min(c->nx / 2, maxb); npx++)
-    for (int npy = 1; npy <= c->ny / 2 && npx * npy <= maxb; npy++) {
-      const int w = (c->nx + npx - 1) / npx, h = (c->ny + npy - 1) / npy;
-      if (res_smem_bytes(w, h) > cap || w + h > kResWorkers) continue;
-      int pp = 0;
-      for (int k = 0; k < kResNP && !pp; k++)
-        if (res_threads(w, h, kResP[k]) <= kResWorkers) pp = kResP[k];
-      if (!pp) continue;
-      const double cost = 0.27 * w * h + 5.0 * npx * npy;
-      if (cost < best) {
-        best = cost;
-        R.npx = npx;
-        R.npy = npy;
-        R.wmax = w;
-        R.hmax = h;
-        R.p = pp;
-        R.smem = res_smem_bytes(w, h);
-      }
-    }
+  ResCut cut;
+  const double best = res_cut(c->nx, c->ny, maxb, cap, 0, false, cut) ? cut.cost : 1e300;
+  if (best < 1e300) {
+    R.npx = cut.npx;
+    R.npy = cut.npy;
+    R.wmax = cut.w;
+    R.hmax = cut.h;
+    R.p = cut.p;
+    R.smem = cut.smem;
+  }
   if (best == 1e300) return PYOMGPU_OK;
   for (int k = 0; k < kResNP; k++)
     for (bool single : {false, true})
@@ -215,6 +249,9 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
   CK(cudaMemsetAsync(c->res, 0, bytes, st));
   CK(cudaMemsetAsync(R.slots, 0xFF, (size_t)4 * (nb + 1) * kResSlotWords * sizeof(double), st));
+  // exchange records all-ones: a word whose tag no solve uses (fresh memory reads as zero, the tag of
+  // generation 0, epoch 0, and the untagged single-reduction kernel leaves arbitrary bits)
+  CK(cudaMemsetAsync(R.hx, 0xFF, 8 * c->g.size() * sizeof(double), st));
   CGResParams P{};
   P.g = c->g;
   P.op = c->sf.dev();
@@ -250,6 +287,85 @@ int run_cg_res(pyomgpu_ctx* c, const double* forc_dev, double eps, int max_it, d
   CK(cudaLaunchCooperativeKernel(kern, dim3(nb), dim3(kResThreads), args, R.smem, st));
   CK(cudaEventRecord(c->e1, st));
   return finish_cg(c, info, st);
+}
+
+// Piece layout of the FP32 resident kernel for this grid (res_cut with FP32
+// fields), planned once, with its exchange buffers.  c->resd.ok32 tells
+// whether the grid fits.
+int res_plan32(pyomgpu_ctx* c) {
+  auto& R = c->resd;
+  if (R.planned32) return PYOMGPU_OK;
+  R.planned32 = true;
+  R.ok32 = false;
+  const size_t cap = res_smem_cap(c);
+  if (cap == 0) return PYOMGPU_OK;
+  ResCut cut;
+  if (!res_cut(c->nx, c->ny, std::min(c->nsm, kResMaxSlots - 1), cap, 0, false, cut, true)) return PYOMGPU_OK;
+  for (int p : {16, 32})
+    if (cudaFuncSetAttribute(cg_res32_kernel_ptr(p), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) !=
+        cudaSuccess)
+      return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the FP32 resident kernel");
+  const int nb = cut.npx * cut.npy;
+  if (int rc = dalloc(&R.hx32, 2 * c->g.size())) return rc;  // two tagged words per position
+  if (int rc = dalloc(&R.slots32, (size_t)4 * (nb + 1) * kResSlotWords)) return rc;
+  if (int rc = dalloc(&R.res32, c->g.size())) return rc;
+  R.npx32 = cut.npx;
+  R.npy32 = cut.npy;
+  R.wmax32 = cut.w;
+  R.hmax32 = cut.h;
+  R.p32 = cut.p;
+  R.smem32 = cut.smem;
+  R.ok32 = true;
+  return PYOMGPU_OK;
+}
+
+// The FP32 correction solve of the mixed-precision path on the resident
+// kernel: A x = b with the FP32 operator copy, b and x padded (x halo valid,
+// here zero), to ||res|| <= rtol ||b|| over the unknowns.  Same result
+// fields as run_pipe.
+int run_cg_res32(pyomgpu_ctx* c, const OpDev<float>& op, const float* b, float* x, double rtol, int max_it,
+                 PipeResult* res, float* ms, cudaStream_t st) {
+  auto& R = c->resd;
+  const int nb = R.npx32 * R.npy32;
+  CK(cudaMemsetAsync(c->ctl, 0, sizeof(SyncCtl), st));
+  CK(cudaMemsetAsync(R.res32, 0, c->g.size() * sizeof(float), st));
+  CK(cudaMemsetAsync(R.slots32, 0xFF, (size_t)4 * (nb + 1) * kResSlotWords * sizeof(double), st));
+  CK(cudaMemsetAsync(R.hx32, 0xFF, 2 * c->g.size() * sizeof(double), st));
+  CGResParams P{};
+  P.g = c->g;
+  P.op32 = op;
+  P.forc32 = b;
+  P.sol32 = x;
+  P.res32 = R.res32;
+  P.hx = R.hx32;
+  P.hsize = (long long)c->g.size();
+  P.slots = R.slots32;
+  P.nslot = nb + 1;
+  P.npx = R.npx32;
+  P.npy = R.npy32;
+  P.wmax = R.wmax32;
+  P.hmax = R.hmax32;
+  P.eps = 0.0;
+  P.rtol = rtol;
+  P.max_it = max_it;
+  P.ctl = c->ctl;
+  P.timeout_ns = (unsigned long long)(c->timeout_s * 1e9);
+  P.out = c->d_result;
+  void* args[] = {&P};
+  CK(cudaEventRecord(c->e0, st));
+  CK(cudaLaunchCooperativeKernel(cg_res32_kernel_ptr(R.p32), dim3(nb), dim3(kResThreads), args, R.smem32, st));
+  CK(cudaEventRecord(c->e1, st));
+  CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CGResult), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_scal, &c->ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  int err = 0;
+  std::memcpy(&err, c->h_scal, sizeof(int));
+  if (err) return fail(PYOMGPU_TIMEOUT, "reduction wait exceeded %.3f s", c->timeout_s);
+  CK(cudaEventElapsedTime(ms, c->e0, c->e1));
+  res->iterations = c->h_result->iterations;
+  res->status = c->h_result->status;
+  res->rr = res->bb = -1.0;
+  return 0;
 }
 
 // Runs the persistent CG kernel on c->sol (padded, already packed) with the
@@ -589,6 +705,218 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
     I.estimated_error = S.est;
     I.device_ms = ms;
     I.kernel_launches = 1;
+    if (want_res) {
+      const double rr = B.h_rr[2 * k], bb = B.h_rr[2 * k + 1];
+      I.rel_residual = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+    } else {
+      I.rel_residual = -1.0;
+    }
+  }
+  return worst;
+}
+
+// Index words of the multi-solve launches: group_base and job_first of each of
+// at most kResSplits launches (2^t groups in launch t).
+constexpr int kResSplits = 5;
+inline size_t rmulti_idx_words(int count) {
+  (void)count;
+  size_t n = 0;
+  for (int t = 0; t < kResSplits; ++t) n += 2 * ((size_t(1) << t) + 1);
+  return n;
+}
+
+// Grows the owner's table for `count` resident jobs.
+int rmulti_reserve(pyomgpu_ctx* o, int count) {
+  auto& R = o->rmulti;
+  if (count <= R.cap) return 0;
+  for (void* p : {(void*)R.d_jobs, (void*)R.d_idx, (void*)R.d_out, (void*)R.d_ctl})
+    if (p) cudaFree(p);
+  for (void* p : {(void*)R.h_jobs, (void*)R.h_idx, (void*)R.h_out, (void*)R.h_ctl})
+    if (p) cudaFreeHost(p);
+  R.d_jobs = nullptr;
+  R.h_jobs = nullptr;
+  R.d_idx = R.h_idx = nullptr;
+  R.d_out = R.h_out = nullptr;
+  R.d_ctl = R.h_ctl = nullptr;
+  R.cap = 0;
+  if (int rc = dalloc(&R.d_jobs, (size_t)count)) return rc;
+  if (int rc = dalloc(&R.d_idx, rmulti_idx_words(count))) return rc;
+  if (int rc = dalloc(&R.d_out, (size_t)count)) return rc;
+  if (int rc = dalloc(&R.d_ctl, (size_t)count)) return rc;
+  if (cudaMallocHost((void**)&R.h_jobs, sizeof(CGResParams) * count) != cudaSuccess ||
+      cudaMallocHost((void**)&R.h_idx, sizeof(int) * rmulti_idx_words(count)) != cudaSuccess ||
+      cudaMallocHost((void**)&R.h_out, sizeof(CGResult) * count) != cudaSuccess ||
+      cudaMallocHost((void**)&R.h_ctl, sizeof(SyncCtl) * count) != cudaSuccess)
+    return fail(PYOMGPU_ENOMEM, "cudaMallocHost");
+  R.cap = count;
+  return 0;
+}
+
+// The solves of `v` on the resident kernel, several at once: the SMs are split
+// into 2^t groups of nsm / 2^t blocks (t = 0 .. 4), every solve goes to the
+// split with the smallest groups it fits in (res_cut with the fewest pieces,
+// 16 points per thread), and one launch of cg_res_multi_kernel per split runs
+// its solves, assigned to the groups longest first (estimated time: the
+// square root of the point count for the iterations, times the cut's
+// iteration estimate plus ~6 us of reduction latency) to the least loaded.
+// *used = false (nothing run) when a grid does not fit on chip or the
+// resident kernel is unavailable; the caller then runs the work-queue kernel.
+int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol,
+                  bool want_res, pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st, bool* used) {
+  *used = false;
+  const int count = (int)v.size();
+  auto& R = o->rmulti;
+  if (R.smem_cap == 0) {
+    const size_t cap = res_smem_cap(o);
+    if (cap == 0) return PYOMGPU_OK;
+    if (cudaFuncSetAttribute(cg_res_multi_kernel_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) !=
+        cudaSuccess)
+      return PYOMGPU_OK;
+    R.smem_cap = cap;
+  }
+  const int nsm = std::min(o->nsm, kResMaxSlots - 1);
+  std::vector<int> tier((size_t)count);
+  for (int k = 0; k < count; ++k) {
+    const pyomgpu_ctx* c = v[k].c;
+    ResCut cut;
+    if (!res_cut(c->nx, c->ny, nsm, R.smem_cap, 16, true, cut)) return PYOMGPU_OK;
+    int t = 0;
+    while (t + 1 < kResSplits && cut.npx * cut.npy <= nsm >> (t + 1)) t++;
+    tier[k] = t;
+  }
+  // workspace per solve: padded sol and res, 4 record words per position, the slots
+  size_t pool = 0;
+  for (int k = 0; k < count; ++k)
+    pool += 6 * align32(v[k].c->g.size()) + align32((size_t)4 * (nsm + 1) * kResSlotWords);
+  if (int rc = batch_reserve(o, count, pool, 1)) return rc;
+  if (int rc = rmulti_reserve(o, count)) return rc;
+  *used = true;
+  auto& B = o->batch;
+  CK(cudaMemsetAsync(R.d_ctl, 0, sizeof(SyncCtl) * count, st));
+  // jobs in launch order: split by split, group by group
+  std::vector<int> order;
+  std::vector<int> launch_jobs, launch_groups, launch_gs;  // per launch: first job, groups, blocks per group
+  std::vector<int> idx_base;                    // per launch: offset of its group_base / job_first in h_idx
+  int nidx = 0;
+  size_t smem = 0;
+  double* cur = B.pool;
+  for (int t = 0; t < kResSplits; ++t) {
+    const int ng = 1 << t, gs = nsm >> t;
+    std::vector<int> mine;
+    std::vector<double> est((size_t)count, 0.0);
+    for (int k = 0; k < count; ++k)
+      if (tier[k] == t) {
+        const pyomgpu_ctx* c = v[k].c;
+        ResCut cut;
+        res_cut(c->nx, c->ny, gs, R.smem_cap, 16, false, cut);
+        est[k] = std::sqrt((double)c->nx * c->ny) * (cut.cost + 6000.0);
+        mine.push_back(k);
+      }
+    if (mine.empty()) continue;
+    std::stable_sort(mine.begin(), mine.end(), [&](int a, int b) { return est[a] > est[b]; });
+    std::vector<std::vector<int>> groups((size_t)ng);
+    std::vector<double> load((size_t)ng, 0.0);
+    for (int k : mine) {
+      const int gi = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      groups[gi].push_back(k);
+      load[gi] += est[k];
+    }
+    launch_jobs.push_back((int)order.size());
+    launch_groups.push_back(ng);
+    launch_gs.push_back(gs);
+    idx_base.push_back(nidx);
+    int* gb = R.h_idx + nidx;
+    int* jf = gb + ng + 1;
+    for (int gi = 0; gi <= ng; ++gi) gb[gi] = gi * gs;
+    jf[0] = (int)order.size() - launch_jobs.back();
+    for (int gi = 0; gi < ng; ++gi) {
+      for (int k : groups[gi]) {
+        const pyomgpu_ctx* c = v[k].c;
+        ResCut cut;
+        res_cut(c->nx, c->ny, gs, R.smem_cap, 16, false, cut);
+        const size_t P = align32(c->g.size());
+        CGResParams& J = R.h_jobs[order.size()];
+        J = CGResParams{};
+        J.g = c->g;
+        J.op = c->sf.dev();
+        J.forc = v[k].forc ? v[k].forc : c->zeros;
+        J.sol = cur;
+        J.res = cur + P;
+        J.hx = cur + 2 * P;
+        J.hsize = (long long)c->g.size();
+        J.slots = cur + 6 * P;
+        J.nslot = cut.npx * cut.npy + 1;
+        J.npx = cut.npx;
+        J.npy = cut.npy;
+        J.wmax = cut.w;
+        J.hmax = cut.h;
+        J.eps = eps;
+        J.rtol = rtol;
+        J.max_it = max_it;
+        J.ctl = R.d_ctl + k;
+        J.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
+        J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
+        J.out = R.d_out + k;
+        smem = std::max(smem, cut.smem);
+        CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
+        // records and slots all-ones: no tag of the solve (generation 0)
+        CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + align32((size_t)4 * (nsm + 1) * kResSlotWords)) * sizeof(double),
+                           st));
+        launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
+        cur += 6 * P + align32((size_t)4 * (nsm + 1) * kResSlotWords);
+        order.push_back(k);
+      }
+      jf[gi + 1] = (int)order.size() - launch_jobs.back();
+    }
+    nidx += 2 * (ng + 1);
+  }
+  o->stall_next = 0;
+  CK(cudaMemcpyAsync(R.d_jobs, R.h_jobs, sizeof(CGResParams) * order.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(R.d_idx, R.h_idx, sizeof(int) * nidx, cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(o->e0, st));
+  for (size_t L = 0; L < launch_jobs.size(); ++L) {
+    ResMultiParams M{};
+    M.jobs = R.d_jobs + launch_jobs[L];
+    M.group_base = R.d_idx + idx_base[L];
+    M.job_first = M.group_base + launch_groups[L] + 1;
+    M.ngroup = launch_groups[L];
+    void* args[] = {&M};
+    const int grid = launch_groups[L] * launch_gs[L];
+    CK(cudaLaunchCooperativeKernel(cg_res_multi_kernel_ptr(), dim3(grid), dim3(kResThreads), args, smem, st));
+  }
+  CK(cudaEventRecord(o->e1, st));
+  CK(cudaMemcpyAsync(R.h_out, R.d_out, sizeof(CGResult) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(R.h_ctl, R.d_ctl, sizeof(SyncCtl) * count, cudaMemcpyDeviceToHost, st));
+  for (size_t pos = 0; pos < order.size(); ++pos) {
+    const int k = order[pos];
+    const CGResParams& J = R.h_jobs[pos];
+    if (want_res) {
+      launch_fill_cyclic(J.g, J.sol, st);
+      launch_residual(J.g, J.op, J.forc, J.sol, v[k].c->part, 1024, B.d_rr + 2 * k, st);
+    }
+    launch_unpack(J.g, J.sol, v[k].sol, false, false, false, st);
+  }
+  if (want_res) CK(cudaMemcpyAsync(B.h_rr, B.d_rr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  for (int k = 0; k < count; ++k)
+    if (R.h_ctl[k].error) return fail(PYOMGPU_TIMEOUT, "reduction wait exceeded %.3f s", o->timeout_s);
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, o->e0, o->e1));
+  if (ms_out) *ms_out = ms;
+  int worst = PYOMGPU_OK;
+  for (int k = 0; k < count; ++k) {
+    const CGResult& r = R.h_out[k];
+    worst = std::max(worst, r.status);
+    if (!infos) continue;
+    pyomgpu_solve_info& I = infos[k];
+    I.iterations = r.iterations;
+    I.converged = r.converged;
+    I.status = r.status;
+    I.outer_iterations = 1;
+    I.estimated_error = r.est;
+    I.device_ms = ms;
+    I.kernel_launches = (int)launch_jobs.size();
     if (want_res) {
       const double rr = B.h_rr[2 * k], bb = B.h_rr[2 * k + 1];
       I.rel_residual = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
@@ -967,6 +1295,12 @@ int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* c, int32_t kernel) {
   return PYOMGPU_OK;
 }
 
+int32_t pyomgpu_set_batch_kernel(pyomgpu_ctx* c, int32_t kernel) {
+  if (!c || kernel < 0 || kernel > 2) return fail(PYOMGPU_EINVAL, "set_batch_kernel: bad arguments");
+  c->batch_kernel = kernel;
+  return PYOMGPU_OK;
+}
+
 int32_t pyomgpu_resident_layout(pyomgpu_ctx* c, int32_t* npx, int32_t* npy, int32_t* points_per_thread) {
   if (!c) return fail(PYOMGPU_EINVAL, "null context");
   if (int rc = res_plan(c)) return rc;
@@ -974,6 +1308,16 @@ int32_t pyomgpu_resident_layout(pyomgpu_ctx* c, int32_t* npx, int32_t* npy, int3
   if (npx) *npx = c->resd.npx;
   if (npy) *npy = c->resd.npy;
   if (points_per_thread) *points_per_thread = c->resd.p;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_resident_layout32(pyomgpu_ctx* c, int32_t* npx, int32_t* npy, int32_t* points_per_thread) {
+  if (!c) return fail(PYOMGPU_EINVAL, "null context");
+  if (int rc = res_plan32(c)) return rc;
+  if (!c->resd.ok32) return fail(PYOMGPU_EINVAL, "the grid does not fit the FP32 resident kernel");
+  if (npx) *npx = c->resd.npx32;
+  if (npy) *npy = c->resd.npy32;
+  if (points_per_thread) *points_per_thread = c->resd.p32;
   return PYOMGPU_OK;
 }
 
@@ -1276,12 +1620,21 @@ int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t co
     tmp.resize(count);
     info = tmp.data();
   }
-  int rc = run_batch(o, v, eps, max_it, rtol, rtol > 0.0, info, nullptr, st);
-  if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  bool resident = false;
+  int rc = PYOMGPU_OK;
+  if (o->batch_kernel != 1) {
+    rc = run_res_multi(o, v, eps, max_it, rtol, rtol > 0.0, info, nullptr, st, &resident);
+    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    if (!resident && o->batch_kernel == 2) return fail(PYOMGPU_EINVAL, "a batch grid does not fit on chip");
+  }
+  if (!resident) {
+    rc = run_batch(o, v, eps, max_it, rtol, rtol > 0.0, info, nullptr, st);
+    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+  }
   for (int k = 0; k < count; ++k) {
     if (s_host[k]) CK(cudaMemcpyAsync(sol[k], v[k].sol, ctx[k]->n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    // the whole call: the work-queue kernel, pack + unpack per solve (+ halo fill and 2-pass residual)
-    info[k].kernel_launches = 1 + count * (rtol > 0.0 ? 5 : 2);
+    // the whole call: the solve launches, pack + unpack per solve (+ halo fill and 2-pass residual)
+    info[k].kernel_launches += count * (rtol > 0.0 ? 5 : 2);
   }
   CK(cudaStreamSynchronize(st));
   return rc;
@@ -1346,7 +1699,11 @@ int32_t pyomgpu_solve_rtol(pyomgpu_ctx* c, const double* forc, double* sol, doub
     I->kernel_launches = 6;  // pack, cg_ref, fill_cyclic, residual x2, unpack
   } else {
     I->kernel_launches = 5;  // pack, final fill_cyclic + residual x2, unpack (+6 per refinement below)
-    // FP32 PCG (FP64 products) for the correction, FP64 true residual outside
+    // FP32 PCG (FP64 products) for the correction, FP64 true residual outside:
+    // on the FP32 resident kernel where the grid fits on chip, else the
+    // pipelined tile kernel
+    if (int prc = res_plan32(c)) return prc;
+    const bool use_res32 = c->cg_kernel != 1 && c->resd.ok32;
     const double inner_rtol = 1e-6;
     const int max_outer = 12;
     rc = PYOMGPU_MAXITER;
@@ -1371,8 +1728,10 @@ int32_t pyomgpu_solve_rtol(pyomgpu_ctx* c, const double* forc, double* sol, doub
       CK(cudaMemsetAsync(F.x32, 0, c->g.size() * sizeof(float), st));
       PipeResult R{};
       float ms = 0.f;
-      int irc = run_pipe<float>(c, F.op32, F.b32, F.x32, F.r32, F.q32, F.w32, inner_rtol,
-                                std::max(1, max_it - I->iterations), &R, &ms, st);
+      const int left = std::max(1, max_it - I->iterations);
+      int irc = use_res32 ? run_cg_res32(c, F.op32, F.b32, F.x32, inner_rtol, left, &R, &ms, st)
+                          : run_pipe<float>(c, F.op32, F.b32, F.x32, F.r32, F.q32, F.w32, inner_rtol, left, &R, &ms,
+                                            st);
       if (irc) return irc;
       I->iterations += R.iterations;
       I->outer_iterations += 1;

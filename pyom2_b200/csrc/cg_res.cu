@@ -54,11 +54,6 @@ __device__ __forceinline__ double ld_relaxed_f64(const double* p) {
   asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ double ld_acquire_f64(const double* p) {
-  double v;
-  asm volatile("ld.acquire.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-  return v;
-}
 // Plain store, cached in L2 only (ordered before a later st.release of the
 // same thread, or of thread 0 after a block barrier).
 __device__ __forceinline__ void st_weak_f64(double* p, double v) { __stcg(p, v); }
@@ -79,17 +74,14 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 // current value; a stale word carries an older tag.  No ordering between words
 // is needed, hence no release, acquire or emptying.  The tag is the solve's
 // generation (12 bits) and the epoch (20 bits; a stale word is at most two epochs
-// old, so the wrap-around cannot confuse them).
+// old, so the wrap-around cannot confuse them).  Slots and records are filled
+// with all-ones words before every solve, a tag no solve uses (generations stop
+// at 4094), so no word left by an earlier solve or kernel can pass as current.
 __device__ __forceinline__ unsigned res_tag(const CGResParams& P, unsigned ep) {
   return (P.tag_gen << 20) | (ep & 0xFFFFFu);
 }
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
 }
 __device__ __forceinline__ unsigned long long tag_lo(unsigned tag, double v) {
   return ((unsigned long long)tag << 32) | (unsigned)__double2loint(v);
@@ -127,34 +119,48 @@ __device__ __forceinline__ void publish_cyclic(double* a, const Geo& g, int i, i
   }
 }
 
-// Writes (q, s) as the tagged record of interior (i,j) -- 4 words at 4 * position:
-// q low, q high, s low, s high -- and of the halo positions setcyclic_xy fills from it.
-__device__ __forceinline__ void publish_cyclic_tagged(unsigned long long* a, const Geo& g, int i, int j, double q,
-                                                      double s, unsigned tag) {
-  const unsigned long long w0 = tag_lo(tag, q), w1 = tag_hi(tag, q), w2 = tag_lo(tag, s), w3 = tag_hi(tag, s);
-  auto put = [&](size_t pos) {
-    st_relaxed_u64(a + 4 * pos, w0);
-    st_relaxed_u64(a + 4 * pos + 1, w1);
-    st_relaxed_u64(a + 4 * pos + 2, w2);
-    st_relaxed_u64(a + 4 * pos + 3, w3);
-  };
-  put(g.at(i, j));
-  int xc, yc;
-  cyclic_copies(g, i, j, xc, yc);
-  if (xc != 0x7fffffff) put(g.at(xc, j));
-  if (yc != 0x7fffffff) {
-    put(g.at(i, yc));
-    if (xc != 0x7fffffff) put(g.at(xc, yc));
-  }
+// 32-byte relaxed accesses (four tagged words; each word is validated on its own,
+// so the access need not be single-copy atomic as a whole).  The address is
+// 32-byte aligned.
+__device__ __forceinline__ void st_relaxed_v4_u64(unsigned long long* p, unsigned long long w0, unsigned long long w1,
+                                                  unsigned long long w2, unsigned long long w3) {
+  asm volatile("st.relaxed.gpu.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(w0), "l"(w1), "l"(w2), "l"(w3)
+               : "memory");
+}
+__device__ __forceinline__ void ld_relaxed_v4_u64(const unsigned long long* p, unsigned long long& w0,
+                                                  unsigned long long& w1, unsigned long long& w2,
+                                                  unsigned long long& w3) {
+  asm volatile("ld.relaxed.gpu.global.v4.u64 {%0, %1, %2, %3}, [%4];"
+               : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3)
+               : "l"(p)
+               : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed_v2_u64(unsigned long long* p, unsigned long long w0, unsigned long long w1) {
+  asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(w0), "l"(w1) : "memory");
+}
+__device__ __forceinline__ void ld_relaxed_v2_u64(const unsigned long long* p, unsigned long long& w0,
+                                                  unsigned long long& w1) {
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(p) : "memory");
+}
+
+// FP32 fields: (q, s) as the tagged record at padded position pos -- 2 words
+// at 2 * pos, (tag << 32) | the value's bits -- in one 16-byte store.
+__device__ __forceinline__ void put_record_tagged(unsigned long long* a, long long pos, float q, float s,
+                                                  unsigned tag) {
+  st_relaxed_v2_u64(a + 2 * pos, ((unsigned long long)tag << 32) | __float_as_uint(q),
+                    ((unsigned long long)tag << 32) | __float_as_uint(s));
+}
+
+// Writes (q, s) as the tagged record at padded position pos -- 4 words at
+// 4 * pos: q low, q high, s low, s high -- in one 32-byte store.
+__device__ __forceinline__ void put_record_tagged(unsigned long long* a, long long pos, double q, double s,
+                                                  unsigned tag) {
+  st_relaxed_v4_u64(a + 4 * pos, tag_lo(tag, q), tag_hi(tag, q), tag_lo(tag, s), tag_hi(tag, s));
 }
 
 __device__ __forceinline__ void st_release_cta_u32(unsigned* p, unsigned v) {
   asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_acquire_cta_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)) : "memory");
-  return v;
 }
 __device__ __forceinline__ unsigned ld_relaxed_cta_u32(const unsigned* p) {
   unsigned v;
@@ -234,6 +240,34 @@ __device__ __forceinline__ void col_put(uint32_t* v, int k, double d) {
   v[2 * k] = (uint32_t)__double2loint(d);
   v[2 * k + 1] = (uint32_t)__double2hiint(d);
 }
+// FP32 fields: one column per value
+__device__ __forceinline__ void col_put(uint32_t* v, int k, float f) { v[k] = __float_as_uint(f); }
+template <typename T>
+__device__ __forceinline__ T colT_get(const uint32_t* v, int k) {
+  if constexpr (sizeof(T) == 8)
+    return __hiloint2double((int)v[2 * k + 1], (int)v[2 * k]);
+  else
+    return __uint_as_float(v[k]);
+}
+
+// The operator and vectors of a solve in the field type T (FP64, or the FP32
+// copies of the mixed-precision correction solve).
+template <typename T>
+__device__ __forceinline__ OpDev<T> res_op(const CGResParams& P) {
+  if constexpr (sizeof(T) == 8) return P.op; else return P.op32;
+}
+template <typename T>
+__device__ __forceinline__ const T* res_forc(const CGResParams& P) {
+  if constexpr (sizeof(T) == 8) return P.forc; else return P.forc32;
+}
+template <typename T>
+__device__ __forceinline__ T* res_solv(const CGResParams& P) {
+  if constexpr (sizeof(T) == 8) return P.sol; else return P.sol32;
+}
+template <typename T>
+__device__ __forceinline__ T* res_resv(const CGResParams& P) {
+  if constexpr (sizeof(T) == 8) return P.res; else return P.res32;
+}
 
 // ------------------------------------------------------------ control flow
 // Scalars of the solve in shared memory, advanced by thread 0 only (the
@@ -269,7 +303,7 @@ __device__ void ctl_begin(ResCtl& C, const CGResParams& P) {
 // v = (Z res, res), sum f^2 and sum res^2 over the unknowns, max|Z res|
 __device__ void ctl_init(ResCtl& C, const CGResParams& P, const double* v) {
   C.beta = v[0];
-  C.bb = v[1];
+  C.bb = v[1] > 0.0 ? v[1] : v[2];  // the rtol stop relative to ||res_0|| for a zero forcing
   C.rtol2bb = P.rtol * P.rtol * C.bb;
   C.betam1 = 1.0;
   C.betamin = C.step1 = C.est = C.bq = C.alpha = 0.0;
@@ -368,40 +402,45 @@ __device__ void ctl1_iter(ResCtl& C, const CGResParams& P, const double* v) {
 }
 
 // ------------------------------------------------- reduction and exchange
-struct Halo {
+template <typename T>
+struct HaloT {
   int sidx;       // shared-memory index (-1: none)
   long long gidx; // padded position whose exchange record is received
-  double q, s;    // received Z*res and direction
+  T q, s;         // received Z*res and direction
 };
+using Halo = HaloT<double>;
 
-// Loads this thread's halo values (after a completed reduction).
-__device__ __forceinline__ void worker_halo_load(const CGResParams& P, Halo (&hl)[2]) {
-#pragma unroll
-  for (int e = 0; e < 2; e++)
-    if (hl[e].sidx >= 0) {
-      hl[e].q = __ldcg(P.hx + 4 * hl[e].gidx);
-      hl[e].s = __ldcg(P.hx + 4 * hl[e].gidx + 1);
-    }
-}
 
 // Loads this thread's halo values from tagged records, polling (bounded) a
 // record until both of its values carry `tag`.  False on time-out.
-__device__ __forceinline__ bool worker_halo_load_tagged(const CGResParams& P, Halo (&hl)[2], unsigned tag) {
+template <typename T>
+__device__ __forceinline__ bool worker_halo_load_tagged(const CGResParams& P, HaloT<T> (&hl)[2], unsigned tag) {
   const unsigned long long* hx = reinterpret_cast<const unsigned long long*>(P.hx);
   const unsigned long long t0 = globaltimer_ns();
-  // one record after the other (a worker rarely has two): four words live at a time
+  // one record after the other (a worker rarely has two)
 #pragma unroll 1
   for (int e = 0; e < 2; e++) {
     if (hl[e].sidx < 0) continue;
-    const unsigned long long* r = hx + 4 * hl[e].gidx;
     for (unsigned spin = 1;; spin++) {
-      const unsigned long long w0 = ld_relaxed_u64(r), w1 = ld_relaxed_u64(r + 1), w2 = ld_relaxed_u64(r + 2),
-                               w3 = ld_relaxed_u64(r + 3);
-      if (tag_ok(w0, tag) && tag_ok(w1, tag) && tag_ok(w2, tag) && tag_ok(w3, tag)) {
-        hl[e].q = untag(w0, w1);
-        hl[e].s = untag(w2, w3);
-        break;
+      bool ok;
+      if constexpr (sizeof(T) == 8) {
+        unsigned long long w0, w1, w2, w3;
+        ld_relaxed_v4_u64(hx + 4 * hl[e].gidx, w0, w1, w2, w3);
+        ok = tag_ok(w0, tag) && tag_ok(w1, tag) && tag_ok(w2, tag) && tag_ok(w3, tag);
+        if (ok) {
+          hl[e].q = untag(w0, w1);
+          hl[e].s = untag(w2, w3);
+        }
+      } else {
+        unsigned long long w0, w1;
+        ld_relaxed_v2_u64(hx + 2 * hl[e].gidx, w0, w1);
+        ok = tag_ok(w0, tag) && tag_ok(w1, tag);
+        if (ok) {
+          hl[e].q = __uint_as_float((unsigned)w0);
+          hl[e].s = __uint_as_float((unsigned)w1);
+        }
       }
+      if (ok) break;
       if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
         atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
         return false;
@@ -415,7 +454,8 @@ __device__ __forceinline__ bool worker_halo_load_tagged(const CGResParams& P, Ha
 // entries [0,ph) west column, [ph,2ph) east column, [2ph,2ph+pw) south row,
 // [2ph+pw,2ph+2pw) north row (a corner point in two entries); quantity k of
 // entry e at k*nent+e.  One quantity of one point:
-__device__ __forceinline__ void stage_one(double* spub, int pw, int ph, int lx, int ly, double v) {
+template <typename T>
+__device__ __forceinline__ void stage_one(T* spub, int pw, int ph, int lx, int ly, T v) {
   if (lx == 0) spub[ly] = v;
   if (lx == pw - 1) spub[ph + ly] = v;
   if (ly == 0) spub[2 * ph + lx] = v;
@@ -458,8 +498,13 @@ __device__ __forceinline__ void copy_out(const CGResParams& P, double* hx, const
   }
 }
 
-// copy_out<2> for tagged records: (Z res, direction) of each staged boundary entry.
-__device__ __forceinline__ void copy_out_tagged(const CGResParams& P, const double* spub, int ilo, int ihi, int jlo,
+// copy_out<2> for tagged records: (Z res, direction) of each staged boundary
+// entry, written once, at the position the block across that edge polls: the
+// point itself when the neighbour is an interior piece, its setcyclic_xy image
+// in the domain halo (setcyclic_x: a(nx+1) = a(1), a(0) = a(nx); the same in y)
+// when the edge is a cyclic domain edge; nothing at a closed domain edge.
+template <typename T>
+__device__ __forceinline__ void copy_out_tagged(const CGResParams& P, const T* spub, int ilo, int ihi, int jlo,
                                                 int jhi, int wt, unsigned tag) {
   const Geo& g = P.g;
   unsigned long long* hx = reinterpret_cast<unsigned long long*>(P.hx);
@@ -467,25 +512,41 @@ __device__ __forceinline__ void copy_out_tagged(const CGResParams& P, const doub
 #pragma unroll 1
   for (int e = wt; e < nent; e += kResWorkers) {
     int i, j;
-    bool need;
-    if (e < ph) {
+    bool own, img;
+    if (e < ph) {  // west column
       i = ilo;
       j = jlo + e;
-      need = ilo > 1 || g.cyclic_x;
-    } else if (e < 2 * ph) {
+      own = ilo > 1;
+      img = !own && g.cyclic_x;
+    } else if (e < 2 * ph) {  // east column
       i = ihi;
       j = jlo + e - ph;
-      need = ihi < g.nx || g.cyclic_x;
-    } else if (e < 2 * ph + pw) {
+      own = ihi < g.nx;
+      img = !own && g.cyclic_x;
+    } else if (e < 2 * ph + pw) {  // south row
       i = ilo + e - 2 * ph;
       j = jlo;
-      need = jlo > 1 || g.cyclic_y;
-    } else {
+      own = jlo > 1;
+      img = !own && g.cyclic_y;
+    } else {  // north row
       i = ilo + e - 2 * ph - pw;
       j = jhi;
-      need = jhi < g.ny || g.cyclic_y;
+      own = jhi < g.ny;
+      img = !own && g.cyclic_y;
     }
-    if (need) publish_cyclic_tagged(hx, g, i, j, spub[e], spub[nent + e], tag);
+    if (!own && !img) continue;
+    int ti = i, tj = j;
+    if (img) {
+      if (e < ph)
+        ti = g.nx + 1;
+      else if (e < 2 * ph)
+        ti = 0;
+      else if (e < 2 * ph + pw)
+        tj = g.ny + 1;
+      else
+        tj = 0;
+    }
+    put_record_tagged(hx, g.at(ti, tj), spub[e], spub[nent + e], tag);
   }
 }
 
@@ -511,7 +572,7 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // every block obtains the same bits, and lane 0 advances the control state.
 // False on time-out.
 template <int NV, int kMaxSlot, int kStep, bool TAG = false>
-__device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int npoll, ResCtl& C,
+__device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int bid, int npoll, ResCtl& C,
                                                  const double (*wred)[kResSlotWords], unsigned* hflag = nullptr,
                                                  unsigned long long* tr = nullptr) {
   const int lane = threadIdx.x;
@@ -533,7 +594,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
 #pragma unroll
     for (int k = 0; k < NV; k++)
       if ((lane >> 1) == k) mv = t[k];
-    if (lane < 2 * NV) st_relaxed_u64(tslot(ep, blockIdx.x) + lane, (lane & 1) ? tag_hi(tag, mv) : tag_lo(tag, mv));
+    if (lane < 2 * NV) st_relaxed_u64(tslot(ep, bid) + lane, (lane & 1) ? tag_hi(tag, mv) : tag_lo(tag, mv));
     if (tr != nullptr && lane == 0) tr[0] = globaltimer_ns();
   } else {
     double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
@@ -544,7 +605,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
     }
     // one word per lane (a lone lane's stores go out one after another); the
     // last word, released after a warp barrier, makes the others visible
-    double* mine = res_slot(P, ep, blockIdx.x);
+    double* mine = res_slot(P, ep, bid);
     double mv = 0.0;
 #pragma unroll
     for (int k = 0; k < NV; k++)
@@ -575,10 +636,15 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
         const unsigned long long* sl = tslot(ep, lane + 32 * m);
         bool all = true;
 #pragma unroll
-        for (int k = 0; k < NV; k++) {
-          const unsigned long long lo = ld_relaxed_u64(sl + 2 * k), hi = ld_relaxed_u64(sl + 2 * k + 1);
-          all = all && tag_ok(lo, tag) && tag_ok(hi, tag);
-          got[m][k] = untag(lo, hi);  // kept only once every word of the slot is current
+        for (int k = 0; k < NV; k += 2) {  // two values (four words, 32 bytes) per load
+          unsigned long long w0, w1, w2, w3;
+          ld_relaxed_v4_u64(sl + 2 * k, w0, w1, w2, w3);
+          all = all && tag_ok(w0, tag) && tag_ok(w1, tag);
+          got[m][k] = untag(w0, w1);  // kept only once every word of the slot is current
+          if (k + 1 < NV) {
+            all = all && tag_ok(w2, tag) && tag_ok(w3, tag);
+            got[m][k + 1] = untag(w2, w3);
+          }
         }
         if (all) have |= 1u << m;
       }
@@ -633,7 +699,7 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
     // buffer (= the one of epoch ep+2) is free; the next publication's release
     // orders these stores before it
     __syncwarp();
-    if (lane < kResSlotWords) st_weak_f64(res_slot(P, ep + 2, blockIdx.x) + lane, empty_word());
+    if (lane < kResSlotWords) st_weak_f64(res_slot(P, ep + 2, bid) + lane, empty_word());
   }
   double out[NV];
 #pragma unroll
@@ -664,34 +730,6 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
   return ok;
 }
 
-// Waits (bounded) until the controller has acquired every slot of the
-// reduction carrying the halo records (hflag reaches target), then loads them.
-// False on time-out.
-__device__ __forceinline__ bool worker_halo_early(const CGResParams& P, const unsigned* hflag, unsigned target,
-                                                  Halo (&hl)[2]) {
-  const unsigned long long t0 = globaltimer_ns();
-  for (unsigned spin = 1; ld_acquire_cta_u32(hflag) < target; spin++)
-    if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
-      atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
-      return false;
-    }
-  worker_halo_load(P, hl);
-  return true;
-}
-
-// worker_halo_early for tagged records: waits (bounded) for the controller to
-// acquire every slot of the halo-carrying reduction `target`, then loads the
-// halo, polling each record until it carries that reduction's tag.
-__device__ __forceinline__ bool worker_halo_early_tagged(const CGResParams& P, const unsigned* hflag,
-                                                         unsigned target, Halo (&hl)[2]) {
-  const unsigned long long t0 = globaltimer_ns();
-  for (unsigned spin = 1; ld_acquire_cta_u32(hflag) < target; spin++)
-    if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
-      atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
-      return false;
-    }
-  return worker_halo_load_tagged(P, hl, res_tag(P, 2u * (target - 1u)));
-}
 
 __device__ __forceinline__ void workers_sync() {
   asm volatile("bar.sync 1, %0;" ::"r"(kResWorkers) : "memory");
@@ -705,49 +743,47 @@ __device__ __forceinline__ void workers_sync() {
 // memory) and S2 (the controller's decision is in shared memory, or a wait
 // timed out).  Work that overlaps the wait of the other blocks (the solution
 // update) runs between S1 and S2.
-template <int P, bool TRACE>
-__global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_constant__ CGResParams Pm) {
-  constexpr int CH = P == 8 ? 8 : 4;  // points per TMEM chunk (tcgen05 .x16 / .x8; .x16 at P = 16 spills)
-  constexpr int NC = P / CH;  // chunks per field
-  constexpr int CW = 2 * CH;  // TMEM columns per chunk
+//
+// One solve by the blocks 0 .. npx*npy-1 of a group (bid: this block's index in
+// it); the caller has allocated the block's 512 TMEM columns (address in
+// *s_tmem) and provides the dynamic shared memory sm.  Every block of the
+// group calls it for the same solve; a block returns once its share is done
+// (all threads together, after a block barrier).
+template <typename T, int P, bool TRACE>
+__device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, double* sm, const uint32_t* s_tmem_p,
+                                          ResCtl& C, double (*wred)[kResSlotWords]) {
+  // points per TMEM chunk (FP64: tcgen05 .x16 / .x8, .x16 at P = 16 spills; FP32: .x8)
+  constexpr int CH = sizeof(T) == 4 ? 8 : (P == 8 ? 8 : 4);
+  constexpr int NC = P / CH;                     // chunks per field
+  constexpr int CW = (int)(sizeof(T) / 4) * CH;  // TMEM columns per chunk
   static_assert(P % CH == 0 && NC * CW <= 32, "a field takes at most 32 TMEM columns per thread");
-  extern __shared__ __align__(16) double sm[];
-  __shared__ uint32_t s_tmem;
-  __shared__ ResCtl C;
-  __shared__ double wred[kResThreads / 32][kResSlotWords];
-  __shared__ unsigned s_hflag;  // reductions whose halo records the workers may load
   const Geo g = Pm.g;
-  const OpDev<double> op = Pm.op;
+  const OpDev<T> op = res_op<T>(Pm);
   const int warp = threadIdx.x >> 5;
-  if (warp == 0) {
-    tc::tmem_alloc(&s_tmem, 512);
-    tc::tmem_relinquish();
-  }
-  if (threadIdx.x == 0) s_hflag = 0u;
   // traced instantiation: this block's timestamps of loop trip t (nullptr outside the window)
   auto trace_row = [&](unsigned t) -> unsigned long long* {
     if (!TRACE) return nullptr;
     const int k = (int)t - Pm.trace_it0;
     if (k < 0 || k >= Pm.trace_nit) return nullptr;
-    return Pm.trace + ((size_t)blockIdx.x * Pm.trace_nit + k) * kResTracePhases;
+    return Pm.trace + ((size_t)bid * Pm.trace_nit + k) * kResTracePhases;
   };
 
-  const int nb = gridDim.x;
-  const int px = blockIdx.x % Pm.npx, py = blockIdx.x / Pm.npx;
+  const int nb = Pm.npx * Pm.npy;
+  const int px = bid % Pm.npx, py = bid / Pm.npx;
   const int ilo = 1 + (int)(((long long)px * g.nx) / Pm.npx);
   const int ihi = (int)(((long long)(px + 1) * g.nx) / Pm.npx);
   const int jlo = 1 + (int)(((long long)py * g.ny) / Pm.npy);
   const int jhi = (int)(((long long)(py + 1) * g.ny) / Pm.npy);
   const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, sp = pw + 2;
   const int pw_ = pw, ph_ = ph, jlo_ = jlo;
-  double* ss = sm;                    // (pw+2) x (ph+2): direction, halo included
-  double* sfx = ss + sp * (ph + 2);   // (pw+1) x ph: FX(ilo+lx, j), lx = 0..pw
-  double* sfy = sfx + (pw + 1) * ph;  // pw x (ph+1): FY(i, jlo+ly), ly = 0..ph
-  double* sbx = sfy + pw * (ph + 1);  // ph: bx(jlo+ly), then ph: by(jlo+ly)
-  double* spub = sbx + 2 * ph;        // 2 x 2(pw+ph): staged boundary Z*res, direction
+  T* ss = reinterpret_cast<T*>(sm);  // (pw+2) x (ph+2): direction, halo included
+  T* sfx = ss + sp * (ph + 2);        // (pw+1) x ph: FX(ilo+lx, j), lx = 0..pw
+  T* sfy = sfx + (pw + 1) * ph;       // pw x (ph+1): FY(i, jlo+ly), ly = 0..ph
+  T* sbx = sfy + pw * (ph + 1);       // ph: bx(jlo+ly), then ph: by(jlo+ly)
+  T* spub = sbx + 2 * ph;             // 2 x 2(pw+ph): staged boundary Z*res, direction
   const int nent = 2 * (pw + ph);
 
-  for (int e = threadIdx.x; e < sp * (ph + 2); e += kResThreads) ss[e] = 0.0;
+  for (int e = threadIdx.x; e < sp * (ph + 2); e += kResThreads) ss[e] = (T)0;
   for (int e = threadIdx.x; e < (pw + 1) * ph; e += kResThreads)
     sfx[e] = op.FX[g.at(ilo + e % (pw + 1), jlo + e / (pw + 1))];
   for (int e = threadIdx.x; e < pw * (ph + 1); e += kResThreads) sfy[e] = op.FY[g.at(ilo + e % pw, jlo + e / pw)];
@@ -764,14 +800,14 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     unsigned ep = 0;
     bool stopped_after_update = false;  // the stop decided before sweep B (C stays as the workers read it)
     __syncthreads();  // S1
-    bool ok = controller_epoch<4, 3, kStepInit, true>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred, &s_hflag);
+    bool ok = controller_epoch<4, 3, kStepInit, true>(Pm, ep, bid, nb + (Pm.stall_extra ? 1 : 0), C, wred);
     if (!__syncthreads_and(ok)) goto out;  // S2
     if (C.act == kRun) {
       for (unsigned trip = 0;; trip++) {
         unsigned long long* tr = threadIdx.x == 0 ? trace_row(trip) : nullptr;
         __syncthreads();  // S1: partials of sweep A
         if (TRACE && tr) tr[10] = globaltimer_ns();
-        ok = controller_epoch<2, 1, kStepA, true>(Pm, ++ep, nb, C, wred, nullptr, TRACE && tr ? tr + 11 : nullptr);
+        ok = controller_epoch<2, 1, kStepA, true>(Pm, ++ep, bid, nb, C, wred, nullptr, TRACE && tr ? tr + 11 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
         if (C.stop_after) {  // the workers finish sweep B and stop
@@ -780,13 +816,13 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         }
         __syncthreads();  // S1: partials of sweep B
         if (TRACE && tr) tr[14] = globaltimer_ns();
-        ok = controller_epoch<2, -1, kStepB, true>(Pm, ++ep, nb, C, wred, &s_hflag,
+        ok = controller_epoch<2, -1, kStepB, true>(Pm, ++ep, bid, nb, C, wred, nullptr,
                                                    TRACE && tr ? tr + 15 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
       }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bid == 0 && threadIdx.x == 0) {
       const int converged = stopped_after_update || C.act == kDoneOk;
       Pm.out->iterations = C.n;
       Pm.out->converged = converged;
@@ -802,14 +838,14 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     const int nrow_ = (lx_ < pw && ly0_ < ph) ? min(P, ph - ly0_) : 0;
     const int i_ = ilo + lx_;
     int lx = lx_, ly0 = ly0_, nrow = nrow_, i = i_;
-    const double axi = nrow_ > 0 ? op.ax[i_ + 1] : 0.0;
+    const T axi = nrow_ > 0 ? op.ax[i_ + 1] : (T)0;
     // TMEM of this thread: lane 32*(warp%4)+lane, 32 columns per field from 128*(warp/4)
-    const uint32_t tm = s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * (warp >> 2));
+    const uint32_t tm = *s_tmem_p + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * (warp >> 2));
     const uint32_t t_res = tm, t_sol = tm + 32, t_z = tm + 64;
 
     // halo positions received (west, east, south, north edges that have a
     // neighbour; a non-cyclic domain edge keeps the zero direction)
-    Halo hl[2];
+    HaloT<T> hl[2];
     {
       const int nW = (ilo > 1 || g.cyclic_x) ? ph : 0, nE = (ihi < g.nx || g.cyclic_x) ? ph : 0;
       const int nS = (jlo > 1 || g.cyclic_y) ? pw : 0, nN = (jhi < g.ny || g.cyclic_y) ? pw : 0;
@@ -818,7 +854,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         const int h = wt + e * kResWorkers;
         hl[e].sidx = -1;
         hl[e].gidx = 0;
-        hl[e].q = hl[e].s = 0.0;
+        hl[e].q = hl[e].s = (T)0;
         if (h >= nW + nE + nS + nN) continue;
         int hx, hy;
         if (h < nW) {
@@ -839,7 +875,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
       }
     }
 
-    double s[P], q[P];  // direction; q: Z*res before sweep A, As after it
+    T s[P], q[P];  // direction; q: Z*res before sweep A, As after it
     unsigned hready = 0;  // halo-carrying reductions completed
 
     // ---------------------------------------------------------------- init
@@ -852,25 +888,25 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
 #pragma unroll
         for (int k = 0; k < CH; k++) {
           const int u = c * CH + k;
-          double rv = 0.0, w = 0.0, x = 0.0;
-          s[u] = 0.0;
-          q[u] = 0.0;
-          if (u < nrow) {
+          T rv = 0, w = 0, x = 0;
+          s[u] = 0;
+          q[u] = 0;
+          if (u < nrow) {  // partial sums in FP64 for either field type
             const int ly = ly0 + u, j = jlo + ly;
-            const double f = Pm.forc[fidx(g.nx, i, j)];
-            rv = f - apply_point(op, g, Pm.sol, i, j);
+            const T f = res_forc<T>(Pm)[sizeof(T) == 8 ? fidx(g.nx, i, j) : g.at(i, j)];
+            rv = f - apply_point(op, g, (const T*)res_solv<T>(Pm), i, j);
             w = op.W[g.at(i, j)];
-            x = Pm.sol[g.at(i, j)];
-            const double zr = w * rv;
-            v[0] += zr * rv;
-            if (w != 0.0) {
-              v[1] += f * f;
-              v[2] += rv * rv;
+            x = res_solv<T>(Pm)[g.at(i, j)];
+            const T zr = w * rv;
+            v[0] += (double)zr * (double)rv;
+            if (w != (T)0) {
+              v[1] += (double)f * (double)f;
+              v[2] += (double)rv * (double)rv;
             }
-            v[3] = fmax(v[3], fabs(zr));
+            v[3] = fmax(v[3], fabs((double)zr));
             q[u] = zr;
             stage_one(spub, pw, ph, lx, ly, zr);
-            stage_one(spub + nent, pw, ph, lx, ly, 0.0);
+            stage_one(spub + nent, pw, ph, lx, ly, (T)0);
           }
           col_put(br, k, rv);
           col_put(bz, k, w);
@@ -886,7 +922,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
     workers_sync();
     copy_out_tagged(Pm, spub, ilo, ihi, jlo, jhi, wt, res_tag(Pm, 2u * hready));
     __syncthreads();  // S1
-    if (!__syncthreads_and(worker_halo_early_tagged(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
+    // the neighbours' records of this exchange, polled until they carry its tag
+    if (!__syncthreads_and(worker_halo_load_tagged(Pm, hl, res_tag(Pm, 2u * hready++)))) goto out;  // S2
     if (C.act != kRun) goto done;
 
     for (unsigned trip = 0;; trip++) {
@@ -898,7 +935,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
       nrow = opaque(nrow_);
       {
         const int sp = opaque(pw + 2);
-        const double bq = C.bq;
+        const T bq = (T)C.bq;
 #pragma unroll
         for (int u = 0; u < P; u++)
           if (u < nrow) {
@@ -918,22 +955,22 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         const int pw = opaque(pw_), sp = pw + 2, ph = opaque(ph_);
         double v[2] = {0.0, 0.0};  // (s, As), max|s|
         if (nrow > 0) {
-          double fys = sfy[ly0 * pw + lx];
+          T fys = sfy[ly0 * pw + lx];
 #pragma unroll
           for (int u = 0; u < P; u++)
             if (u < nrow) {
               const int ly = ly0 + u;
               const int k = (ly + 1) * sp + lx + 1;
-              const double sc = s[u];
-              const double se = ss[k + 1], sw = ss[k - 1];
-              const double sn = (u + 1 < P && u + 1 < nrow) ? s[u + 1 < P ? u + 1 : u] : ss[k + sp];
-              const double so = (u > 0) ? s[u > 0 ? u - 1 : 0] : ss[k - sp];
-              const double fxw = sfx[ly * (pw + 1) + lx], fxe = sfx[ly * (pw + 1) + lx + 1];
-              const double fyn = sfy[(ly + 1) * pw + lx];
-              const double a = axi * sbx[ly] * (fxe * (se - sc) + fxw * (sw - sc)) +
-                               sbx[ph + ly] * (fyn * (sn - sc) + fys * (so - sc));
-              v[0] += sc * a;
-              v[1] = fmax(v[1], fabs(sc));
+              const T sc = s[u];
+              const T se = ss[k + 1], sw = ss[k - 1];
+              const T sn = (u + 1 < P && u + 1 < nrow) ? s[u + 1 < P ? u + 1 : u] : ss[k + sp];
+              const T so = (u > 0) ? s[u > 0 ? u - 1 : 0] : ss[k - sp];
+              const T fxw = sfx[ly * (pw + 1) + lx], fxe = sfx[ly * (pw + 1) + lx + 1];
+              const T fyn = sfy[(ly + 1) * pw + lx];
+              const T a = axi * sbx[ly] * (fxe * (se - sc) + fxw * (sw - sc)) +
+                          sbx[ph + ly] * (fyn * (sn - sc) + fys * (so - sc));
+              v[0] += (double)sc * (double)a;
+              v[1] = fmax(v[1], fabs((double)sc));
               q[u] = a;
               fys = fyn;
             }
@@ -953,7 +990,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
       i = opaque(i_);
       {
         const int pw = opaque(pw_), ph = opaque(ph_), jlo = opaque(jlo_);
-        const double alpha = C.alpha;
+        const T alpha = (T)C.alpha;
         const bool stop_after = C.stop_after != 0;
         double v[2] = {0.0, 0.0};  // (Z res, res), sum res^2 over the unknowns
 #pragma unroll
@@ -966,11 +1003,11 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
           for (int k = 0; k < CH; k++) {
             const int u = c * CH + k;
             if (u < nrow) {
-              const double w = col_get(bz, k);
-              const double rv = col_get(br, k) - alpha * q[u];
-              const double zr = w * rv;
-              v[0] += zr * rv;
-              if (w != 0.0) v[1] += rv * rv;
+              const T w = colT_get<T>(bz, k);
+              const T rv = colT_get<T>(br, k) - alpha * q[u];
+              const T zr = w * rv;
+              v[0] += (double)zr * (double)rv;
+              if (w != (T)0) v[1] += (double)rv * (double)rv;
               q[u] = zr;
               col_put(br, k, rv);
             }
@@ -1002,7 +1039,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
 #pragma unroll
           for (int k = 0; k < CH; k++) {
             const int u = c * CH + k;
-            if (u < nrow) col_put(bx, k, col_get(bx, k) + alpha * s[u]);
+            if (u < nrow) col_put(bx, k, colT_get<T>(bx, k) + alpha * s[u]);
           }
           tm_st<CW>(t_sol + c * CW, bx);
         }
@@ -1010,7 +1047,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         if (TRACE && tr) tr[8] = globaltimer_ns();
         if (stop_after) goto done;
       }
-      if (!__syncthreads_and(worker_halo_early_tagged(Pm, &s_hflag, ++hready, hl))) goto out;  // S2
+      // the halo of the next direction, while the controller completes reduction B
+      if (!__syncthreads_and(worker_halo_load_tagged(Pm, hl, res_tag(Pm, 2u * hready++)))) goto out;  // S2
       if (TRACE && tr) tr[9] = globaltimer_ns();
       if (C.act != kRun) goto done;
     }
@@ -1028,8 +1066,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
         const int u = c * CH + k;
         if (u < nrow) {
           const int j = jlo + ly0 + u;
-          store_cyclic(Pm.res, g, i, j, col_get(br, k));
-          Pm.sol[g.at(i, j)] = col_get(bx, k);
+          store_cyclic(res_resv<T>(Pm), g, i, j, colT_get<T>(br, k));
+          res_solv<T>(Pm)[g.at(i, j)] = colT_get<T>(bx, k);
         }
       }
     }
@@ -1037,7 +1075,68 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_con
 out:
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(s_tmem, 512);
+  tc::fence_after_sync();
+}
+
+// Block layout: warp 0 is the controller, warps 1-15 the workers (res_solve).
+template <int P, bool TRACE>
+__global__ void __launch_bounds__(kResThreads, 1) cg_res_kernel(const __grid_constant__ CGResParams Pm) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint32_t s_tmem;
+  __shared__ ResCtl C;
+  __shared__ double wred[kResThreads / 32][kResSlotWords];
+  if ((threadIdx.x >> 5) == 0) {
+    tc::tmem_alloc(&s_tmem, 512);
+    tc::tmem_relinquish();
+  }
+  res_solve<double, P, TRACE>(Pm, (int)blockIdx.x, sm, &s_tmem, C, wred);
+  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_tmem, 512);
+}
+
+// The same solve with FP32 fields (shared memory, TMEM, registers, exchange
+// records) and FP64 partial sums and control: the correction solve of the
+// mixed-precision path, on grids twice the size of the FP64 kernel's.
+template <int P>
+__global__ void __launch_bounds__(kResThreads, 1) cg_res32_kernel(const __grid_constant__ CGResParams Pm) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint32_t s_tmem;
+  __shared__ ResCtl C;
+  __shared__ double wred[kResThreads / 32][kResSlotWords];
+  if ((threadIdx.x >> 5) == 0) {
+    tc::tmem_alloc(&s_tmem, 512);
+    tc::tmem_relinquish();
+  }
+  res_solve<float, P, false>(Pm, (int)blockIdx.x, sm, &s_tmem, C, wred);
+  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_tmem, 512);
+}
+
+// Many solves in one launch: the blocks form groups (group k: blocks
+// group_base[k] .. group_base[k+1]-1), and each group runs the solves
+// job_first[k] .. job_first[k+1]-1 one after another, every block of the
+// group in the same order.  A solve has its own operator, vectors, reduction
+// slots, exchange records, error flag and result, so the groups never wait on
+// one another and a block may start its group's next solve while others still
+// finish the last one.
+template <int P>
+__global__ void __launch_bounds__(kResThreads, 1) cg_res_multi_kernel(const __grid_constant__ ResMultiParams M) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ uint32_t s_tmem;
+  __shared__ ResCtl C;
+  __shared__ double wred[kResThreads / 32][kResSlotWords];
+  if ((threadIdx.x >> 5) == 0) {
+    tc::tmem_alloc(&s_tmem, 512);
+    tc::tmem_relinquish();
+  }
+  int grp = 0;
+  while (grp + 1 < M.ngroup && M.group_base[grp + 1] <= (int)blockIdx.x) grp++;
+  const int bid = (int)blockIdx.x - M.group_base[grp];
+  for (int j = M.job_first[grp]; j < M.job_first[grp + 1]; j++) {
+    const CGResParams& Pm = M.jobs[j];
+    if (bid < Pm.npx * Pm.npy) res_solve<double, P, false>(Pm, bid, sm, &s_tmem, C, wred);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_tmem, 512);
 }
 
 template __global__ void cg_res_kernel<4, false>(const __grid_constant__ CGResParams);
@@ -1046,6 +1145,9 @@ template __global__ void cg_res_kernel<16, false>(const __grid_constant__ CGResP
 template __global__ void cg_res_kernel<4, true>(const __grid_constant__ CGResParams);
 template __global__ void cg_res_kernel<8, true>(const __grid_constant__ CGResParams);
 template __global__ void cg_res_kernel<16, true>(const __grid_constant__ CGResParams);
+template __global__ void cg_res_multi_kernel<16>(const __grid_constant__ ResMultiParams);
+template __global__ void cg_res32_kernel<16>(const __grid_constant__ CGResParams);
+template __global__ void cg_res32_kernel<32>(const __grid_constant__ CGResParams);
 
 // Single-reduction variant (one cross-block reduction per iteration) of the
 // same Jacobi-PCG, in the style of Chronopoulos and Gear but with the exact
@@ -1116,20 +1218,20 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res1_kernel(const __grid_co
     // ============================================================ controller
     unsigned ep = 0;
     __syncthreads();  // S1: init partials
-    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, nb + (Pm.stall_extra ? 1 : 0), C, wred);
+    bool ok = controller_epoch<4, 3, kStepInit>(Pm, ep, (int)blockIdx.x, nb + (Pm.stall_extra ? 1 : 0), C, wred);
     if (!__syncthreads_and(ok)) goto out;  // S2
     if (C.act == kRun) {
       __syncthreads();  // S1: delta of the first direction
-      ok = controller_epoch<2, -1, kStepInitD>(Pm, ++ep, nb, C, wred);
+      ok = controller_epoch<2, -1, kStepInitD>(Pm, ++ep, (int)blockIdx.x, nb, C, wred);
       if (!__syncthreads_and(ok)) goto out;  // S2
       while (C.act == kRun) {
         __syncthreads();  // S1: partials of one sweep
-        ok = controller_epoch<7, 6, kStepIter>(Pm, ++ep, nb, C, wred);
+        ok = controller_epoch<7, 6, kStepIter>(Pm, ++ep, (int)blockIdx.x, nb, C, wred);
         if (!__syncthreads_and(ok)) goto out;  // S2
       }
       if (C.act == kNeedMaxp) {
         __syncthreads();  // S1: max|p| of the new direction
-        ok = controller_epoch<2, 0, kStepMaxp>(Pm, ++ep, nb, C, wred);
+        ok = controller_epoch<2, 0, kStepMaxp>(Pm, ++ep, (int)blockIdx.x, nb, C, wred);
         if (!__syncthreads_and(ok)) goto out;  // S2
       }
     }
@@ -1443,6 +1545,11 @@ out:
 template __global__ void cg_res1_kernel<4>(const __grid_constant__ CGResParams);
 template __global__ void cg_res1_kernel<8>(const __grid_constant__ CGResParams);
 template __global__ void cg_res1_kernel<16>(const __grid_constant__ CGResParams);
+
+const void* cg_res_multi_kernel_ptr() { return (const void*)cg_res_multi_kernel<16>; }
+const void* cg_res32_kernel_ptr(int p) {
+  return p == 16 ? (const void*)cg_res32_kernel<16> : p == 32 ? (const void*)cg_res32_kernel<32> : nullptr;
+}
 
 const void* cg_res_kernel_ptr(int p, bool single) {
   switch (p) {

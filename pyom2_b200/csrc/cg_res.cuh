@@ -48,6 +48,24 @@ struct CGResParams {
   // trace_it0) * kResTracePhases + phase]
   unsigned long long* trace;
   int trace_it0, trace_nit;
+  // FP32 fields (cg_res32_kernel): operator copy, right-hand side, solution and
+  // residual, all in the padded layout; the exchange records then hold two
+  // tagged words per position
+  OpDev<float> op32;
+  const float* forc32;
+  float* sol32;
+  float* res32;
+};
+
+// Many resident solves in one launch (cg_res_multi_kernel): groups of blocks,
+// each running a list of solves one after another.  Every job has its own
+// CGResParams with npx * npy at most its group's size, its own slots, exchange
+// records (tagged), error flag and result.
+struct ResMultiParams {
+  const CGResParams* jobs;  // device array, grouped: jobs of group k are job_first[k] .. job_first[k+1]-1
+  const int* group_base;    // ngroup + 1 block offsets
+  const int* job_first;     // ngroup + 1 job offsets
+  int ngroup;
 };
 
 // Phases of the trace (worker warp 1 lane 0 unless noted "ctl": warp 0 lane 0):
@@ -76,6 +94,16 @@ __host__ __device__ constexpr int res_threads(int w, int h, int p) { return w * 
 // (the reference's recurrences) or one (single = true: A p by recurrence and
 // (p, Ap) by its exact expansion in products of the sweep before).
 const void* cg_res_kernel_ptr(int p, bool single);
+// The two-reduction kernel with FP32 fields at p = 16 or 32 points per thread.
+const void* cg_res32_kernel_ptr(int p);
+// Dynamic shared memory of a w x h piece of the FP32 kernel: the stencil
+// operand with its halo, FX, FY, bx, by and the staged boundary values.
+__host__ __device__ constexpr size_t res32_smem_bytes(int w, int h) {
+  return 4 * (((size_t)(w + 2) * (h + 2) + (size_t)(w + 1) * h + (size_t)w * (h + 1) + 2 * (size_t)h +
+               4 * (size_t)(w + h) + 3) / 4 * 4);
+}
+// The multi-solve launch of the two-reduction kernel at 16 points per thread.
+const void* cg_res_multi_kernel_ptr();
 // The traced instantiation of the two-reduction kernel (same arithmetic).
 const void* cg_res_trace_kernel_ptr(int p);
 

@@ -18,6 +18,7 @@
 
 using pyomgpu::BatchProblem;
 using pyomgpu::BatchState;
+using pyomgpu::CGResParams;
 using pyomgpu::CGResult;
 using pyomgpu::Geo;
 using pyomgpu::IslandDev;
@@ -102,6 +103,12 @@ struct pyomgpu_ctx {
     size_t smem = 0;
     double *hx = nullptr, *slots = nullptr;
     unsigned tag_gen = 0;  // generation of the next solve's epoch tags (0 .. 4094)
+    // FP32 instance (cg_res32_kernel, the mixed-precision correction solves)
+    bool planned32 = false, ok32 = false;
+    int npx32 = 0, npy32 = 0, wmax32 = 0, hmax32 = 0, p32 = 0;
+    size_t smem32 = 0;
+    double *hx32 = nullptr, *slots32 = nullptr;
+    float* res32 = nullptr;
     // phase trace of the next resident solve (pyomgpu_resident_trace): device
     // buffer of trace_cap words, loop trips trace_it0 .. trace_it0 + trace_nit - 1
     unsigned long long* trace = nullptr;
@@ -130,6 +137,22 @@ struct pyomgpu_ctx {
     unsigned long long* sync = nullptr;  // SyncCtl, gen, any_active
   } batch;
 
+  // many resident solves in one launch (cg_res_multi_kernel), owned by the
+  // context that runs the batch: job table, group offsets, results, error flags
+  struct ResMulti {
+    int cap = 0;  // jobs
+    CGResParams* d_jobs = nullptr;
+    CGResParams* h_jobs = nullptr;  // pinned
+    int* d_idx = nullptr;           // group_base (cap + 1) then job_first (cap + 1)
+    int* h_idx = nullptr;           // pinned
+    CGResult* d_out = nullptr;
+    CGResult* h_out = nullptr;      // pinned
+    SyncCtl* d_ctl = nullptr;
+    SyncCtl* h_ctl = nullptr;       // pinned
+    size_t smem_cap = 0;            // dynamic shared memory reserved for the kernel (0: not yet)
+  } rmulti;
+  int batch_kernel = 0;  // 0 automatic, 1 work-queue kernel, 2 resident groups
+
   ~pyomgpu_ctx() {
     for (void* p : fast.owned)
       if (p) cudaFree(p);
@@ -141,7 +164,12 @@ struct pyomgpu_ctx {
     if (batch.h_state) cudaFreeHost(batch.h_state);
     if (batch.h_rr) cudaFreeHost(batch.h_rr);
     if (batch.h_group) cudaFreeHost(batch.h_group);
-    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace, (void*)batch.d_group})
+    for (void* p : {(void*)rmulti.d_jobs, (void*)rmulti.d_idx, (void*)rmulti.d_out, (void*)rmulti.d_ctl})
+      if (p) cudaFree(p);
+    for (void* p : {(void*)rmulti.h_jobs, (void*)rmulti.h_idx, (void*)rmulti.h_out, (void*)rmulti.h_ctl})
+      if (p) cudaFreeHost(p);
+    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace, (void*)batch.d_group, (void*)resd.hx32,
+                    (void*)resd.slots32, (void*)resd.res32})
       if (p) cudaFree(p);
     void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
                     sf.by, sp.FX, sp.FY, sp.W, sp.ax, sp.bx, sp.by, bnd_i, bnd_j, psin, lu, line_forc, line_psi0, ipiv,

@@ -166,11 +166,13 @@ class ExternalMode:
         single = getattr(self, "_cg_kernel", "auto") == "resident1"
         return f"cg_res{'1' if single else ''}_kernel<{lay[2]}>"
 
-    def resident_layout(self):
+    def resident_layout(self, fp32: bool = False):
         """(pieces in x, pieces in y, points per thread) of the resident
-        kernel on this grid, or None when the grid does not fit."""
+        kernel on this grid (``fp32``: of the FP32 one that runs the
+        mixed-precision correction solves), or None when the grid does not fit."""
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
-        rc = self._L.pyomgpu_resident_layout(self._ctx, C.byref(a), C.byref(b), C.byref(c))
+        fn = self._L.pyomgpu_resident_layout32 if fp32 else self._L.pyomgpu_resident_layout
+        rc = fn(self._ctx, C.byref(a), C.byref(b), C.byref(c))
         if rc == _abi.EINVAL:
             return None
         _abi.check(rc)
@@ -455,17 +457,27 @@ def congrad_surf_press(M, forc):
     return it
 
 
-def congrad_streamfunction_batch(contexts, forcs, sols, eps=1e-12, max_it=1000000, rtol=0.0):
+_BATCH_KERNELS = {"auto": 0, "queue": 1, "resident": 2}
+
+
+def congrad_streamfunction_batch(contexts, forcs, sols, eps=1e-12, max_it=1000000, rtol=0.0, kernel=None):
     """Many congrad_streamfunction solves (solve_streamfct.f90:153-327) in one
-    work-queue launch: solve k on ``contexts[k]`` (an :class:`ExternalMode`;
-    repeats allowed) with ``forcs[k]`` (None = zero forcing) and ``sols[k]``
-    updated in place.  The reference runs such solves one after another
+    call: solve k on ``contexts[k]`` (an :class:`ExternalMode`; repeats
+    allowed) with ``forcs[k]`` (None = zero forcing) and ``sols[k]`` updated
+    in place.  The reference runs such solves one after another
     (streamfct_init.f90:272-287).  ``rtol`` > 0 adds the relative-residual
-    stop.  Returns one info dict per solve."""
+    stop.  ``kernel`` ("auto", "queue" = the work-queue kernel, "resident" =
+    groups of SMs running on-chip solves side by side) is stored on
+    ``contexts[0]`` for this and later calls; None keeps its setting.
+    Returns one info dict per solve."""
     L = _abi.load()
     n = len(contexts)
     if n < 1 or len(forcs) != n or len(sols) != n:
         raise PyOMGPUError(_abi.EINVAL, "contexts, forcs and sols must have the same non-zero length")
+    if kernel is not None:
+        if kernel not in _BATCH_KERNELS:
+            raise ValueError(f"kernel must be one of {sorted(_BATCH_KERNELS)}")
+        _abi.check(L.pyomgpu_set_batch_kernel(contexts[0]._ctx, _BATCH_KERNELS[kernel]))
     VP = C.c_void_p * n
     ctx = VP(*[em._ctx for em in contexts])
     fp = VP(*[None if f is None else _ptr(f, em.shape).value for em, f in zip(contexts, forcs)])

@@ -1,6 +1,8 @@
-"""GPU parity of the work-queue batch (pyomgpu_congrad_streamfunction_batch):
-many congrad_streamfunction solves in one launch, each checked against a
-separate oracle solve on the same inputs (solve_streamfct.f90:153-327).
+"""GPU parity of the batch (pyomgpu_congrad_streamfunction_batch): many
+congrad_streamfunction solves in one call, each checked against a separate
+oracle solve on the same inputs (solve_streamfct.f90:153-327), on both
+engines: the work-queue kernel ("queue") and groups of SMs running resident
+solves side by side ("resident").
 
 Tolerances as in test_gpu_parity: solutions to 1e-10 relative, iteration
 counts within one (dot products are summed in another order).
@@ -72,10 +74,14 @@ def entries(batch_set, seed=3):
     return ents
 
 
-def test_batch_matches_separate_oracle_solves(batch_set):
+ENGINES = ["queue", "resident"]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_batch_matches_separate_oracle_solves(batch_set, engine):
     ents = entries(batch_set)
     sols = [s0.copy(order="F") for *_, s0 in ents]
-    infos = external.congrad_streamfunction_batch([e[2] for e in ents], [e[3] for e in ents], sols)
+    infos = external.congrad_streamfunction_batch([e[2] for e in ents], [e[3] for e in ents], sols, kernel=engine)
     for (W, O, E, f, s0), sg, info in zip(ents, sols, infos):
         cf = O.make_coeff_streamfunction()
         so = s0.copy(order="F")
@@ -85,11 +91,12 @@ def test_batch_matches_separate_oracle_solves(batch_set):
         assert rel(sg, so) < RTOL_SOL, W.name
 
 
-def test_batch_equals_single_call_statistics(batch_set):
+@pytest.mark.parametrize("engine", ENGINES)
+def test_batch_equals_single_call_statistics(batch_set, engine):
     """The batch gives each solve the iteration count of a separate GPU call."""
     ents = entries(batch_set, seed=4)
     sols = [s0.copy(order="F") for *_, s0 in ents]
-    infos = external.congrad_streamfunction_batch([e[2] for e in ents], [e[3] for e in ents], sols)
+    infos = external.congrad_streamfunction_batch([e[2] for e in ents], [e[3] for e in ents], sols, kernel=engine)
     for (W, O, E, f, s0), sb, ib in zip(ents, sols, infos):
         s1 = s0.copy(order="F")
         it, conv, i1 = E.congrad_streamfunction(f, s1)
@@ -97,12 +104,13 @@ def test_batch_equals_single_call_statistics(batch_set):
         assert rel(sb, s1) < RTOL_SOL
 
 
-def test_batch_rtol_and_torch(batch_set):
+@pytest.mark.parametrize("engine", ENGINES)
+def test_batch_rtol_and_torch(batch_set, engine):
     import torch
     ents = entries(batch_set, seed=5)
     sols = [np.zeros(W.M.shape2d, order="F") for W, *_ in ents]
     infos = external.congrad_streamfunction_batch([e[2] for e in ents], [e[3] for e in ents], sols, eps=0.0,
-                                                  rtol=1e-10)
+                                                  rtol=1e-10, kernel=engine)
     for (W, O, E, f, _), s, info in zip(ents, sols, infos):
         assert info["status"] == 0 and info["rel_residual"] <= 1e-10, (W.name, info)
         cf = O.make_coeff_streamfunction()
@@ -116,9 +124,11 @@ def test_batch_rtol_and_torch(batch_set):
     torch.cuda.synchronize()
 
 
-def test_batch_statuses_are_per_solve(batch_set):
+@pytest.mark.parametrize("engine", ENGINES)
+def test_batch_statuses_are_per_solve(batch_set, engine):
     """A NaN forcing stops its own solve with status NaN; the others converge."""
     ents = entries(batch_set, seed=6)[:4]
+    _abi.check(_abi.load().pyomgpu_set_batch_kernel(ents[0][2]._ctx, external._BATCH_KERNELS[engine]))
     bad = ents[1][3].copy(order="F")
     bad[10, 10] = np.nan
     forcs = [e[3] for e in ents]
@@ -142,10 +152,12 @@ def test_batch_statuses_are_per_solve(batch_set):
     assert all(i["status"] == _abi.MAXITER and i["iterations"] == 6 for i in infos)
 
 
-def test_batch_timeout_then_usable(batch_set):
-    """The stall hook makes the first barrier await one block more than the
-    launch has, so no block ever reduces and every wait runs into its time
-    limit: the launch ends with PYOMGPU_TIMEOUT and the context stays usable."""
+@pytest.mark.parametrize("engine", ENGINES)
+def test_batch_timeout_then_usable(batch_set, engine):
+    """The stall hook makes the first barrier (queue) or the first reduction
+    of every solve (resident) await one block more than there are, so every
+    wait runs into its time limit: the call ends with PYOMGPU_TIMEOUT and the
+    context stays usable."""
     W, O, E = batch_set[1]
     E.set_sync_timeout(1e-3)
     E.inject_barrier_stall(True)
@@ -153,12 +165,12 @@ def test_batch_timeout_then_usable(batch_set):
     sols = [np.zeros(W.M.shape2d, order="F") for _ in f]
     try:
         with pytest.raises(_abi.PyOMGPUError) as e:
-            external.congrad_streamfunction_batch([E] * 8, f, sols)
+            external.congrad_streamfunction_batch([E] * 8, f, sols, kernel=engine)
         assert e.value.code == _abi.TIMEOUT
     finally:
         E.set_sync_timeout(2.0)
     sols = [np.zeros(W.M.shape2d, order="F") for _ in f]
-    infos = external.congrad_streamfunction_batch([E] * 8, f, sols)
+    infos = external.congrad_streamfunction_batch([E] * 8, f, sols, kernel=engine)
     assert all(i["converged"] for i in infos)
     for s in sols[1:]:
         assert np.array_equal(s, sols[0])

@@ -87,6 +87,47 @@ def test_solve_rtol_resident(oracle_lib, name):
     assert O.rel_residual(cf, Z, W.forc, sol) <= 1.5e-10
 
 
+@pytest.mark.parametrize("name", ["c0", "cyclic200", "basin130", "channel96"])
+def test_mixed_precision_on_the_fp32_resident_kernel(oracle_lib, name):
+    """solve_rtol with FP32 correction solves, which run on the FP32 resident
+    kernel where the grid fits (FP32 fields, FP64 partial sums): the FP64
+    true residual reaches rtol, the oracle's residual of the solution agrees,
+    and the solution equals the one of the pipelined tile kernel's
+    corrections (set_cg_kernel "tiled") to 1e-9 relative."""
+    W, O, E = setup(name, oracle_lib, "auto")
+    assert E.resident_layout(fp32=True) is not None
+    sol = np.zeros(W.M.shape2d, order="F")
+    info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=_abi.PREC_F32)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
+    cf = O.make_coeff_streamfunction()
+    assert O.rel_residual(cf, O.make_inv_sfc(cf), W.forc, sol) <= 1.5e-10
+    E.set_cg_kernel("tiled")
+    s2 = np.zeros(W.M.shape2d, order="F")
+    i2 = E.solve_rtol(W.forc, s2, rtol=1e-10, precision=_abi.PREC_F32)
+    E.set_cg_kernel("auto")
+    assert i2["status"] == 0
+    assert rel(sol, s2) < 1e-9
+
+
+def test_fp32_resident_fits_twice_the_grid():
+    """2048 x 1024 does not fit the FP64 resident kernel but fits the FP32
+    one at 32 points per thread; its mixed-precision solve reaches the FP64
+    residual and agrees with the FP64 tiled solve."""
+    W = synth.config3()
+    E = ExternalMode(W.M)
+    E.streamfunction_init(maxipp=10**6, maxq=10**6, psin_rtol=1e-12, psin_weighted=True)
+    assert E.resident_layout() is None
+    npx, npy, p = E.resident_layout(fp32=True)
+    assert p == 32 and npx * npy <= 148
+    sol = np.zeros(W.M.shape2d, order="F")
+    info = E.solve_rtol(W.forc, sol, rtol=1e-10, precision=_abi.PREC_F32)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-10, info
+    s64 = np.zeros(W.M.shape2d, order="F")
+    i64 = E.solve_rtol(W.forc, s64, rtol=1e-10, precision=_abi.PREC_F64)
+    assert i64["status"] == 0
+    assert rel(sol, s64) < 1e-8
+
+
 def test_headline_grid_layout_and_kernels_agree():
     """1440 x 720 (20 islands): 37 x 4 pieces of at most 39 x 180 points, 16
     points per thread; the resident kernels (two reductions and one per
