@@ -537,6 +537,14 @@ struct BatchSpec {
 
 inline size_t align32(size_t n) { return (n + 31) / 32 * 32; }
 
+// Work-pool words of one solve of pyomgpu_congrad_streamfunction_batch, enough
+// for either engine: the work-queue kernel's padded sol, res, s0, s1, As, or
+// the resident groups' padded sol, res, 4 record words per position and the
+// reduction slots.  The staged host inputs follow the work space of all solves.
+inline size_t batch_job_words(size_t padded) {
+  return std::max(5 * align32(padded), 6 * align32(padded) + align32((size_t)4 * kResMaxSlots * kResSlotWords));
+}
+
 // Grows the owner's batch workspace for `count` solves needing `pool` doubles and `tasks` tiles.
 int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
   auto& B = o->batch;
@@ -754,9 +762,10 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
 
 // The solves of `v` on the resident kernel, several at once: the SMs are split
 // into 2^t groups of nsm / 2^t blocks (t = 0 .. 4), every solve goes to the
-// split with the smallest groups it fits in (res_cut with the fewest pieces,
-// 16 points per thread), and one launch of cg_res_multi_kernel per split runs
-// its solves, assigned to the groups longest first (estimated time: the
+// finest split it fits in (res_cut with the fewest pieces, 16 points per
+// thread) that has at least as many solves as groups, and one launch of
+// cg_res_multi_kernel per split runs its solves, assigned to the groups
+// longest first (estimated time: the
 // square root of the point count for the iterations, times the cut's
 // iteration estimate plus ~6 us of reduction latency) to the least loaded.
 // *used = false (nothing run) when a grid does not fit on chip or the
@@ -775,19 +784,32 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     R.smem_cap = cap;
   }
   const int nsm = std::min(o->nsm, kResMaxSlots - 1);
-  std::vector<int> tier((size_t)count);
+  // finest split each grid fits (fewest pieces at 16 points per thread)
+  std::vector<int> fit((size_t)count), tier((size_t)count, -1);
   for (int k = 0; k < count; ++k) {
     const pyomgpu_ctx* c = v[k].c;
     ResCut cut;
     if (!res_cut(c->nx, c->ny, nsm, R.smem_cap, 16, true, cut)) return PYOMGPU_OK;
     int t = 0;
     while (t + 1 < kResSplits && cut.npx * cut.npy <= nsm >> (t + 1)) t++;
-    tier[k] = t;
+    fit[k] = t;
   }
-  // workspace per solve: padded sol and res, 4 record words per position, the slots
+  // from the finest split down, a split takes every unassigned grid that fits it
+  // if they are at least as many as its groups (else they move to coarser
+  // splits, where fewer, larger groups keep every SM busy); split 0 takes the rest
+  for (int t = kResSplits - 1; t >= 0; --t) {
+    int n = 0;
+    for (int k = 0; k < count; ++k) n += tier[k] < 0 && fit[k] >= t;
+    if (n == 0 || (t > 0 && n < (1 << t))) continue;
+    for (int k = 0; k < count; ++k)
+      if (tier[k] < 0 && fit[k] >= t) tier[k] = t;
+  }
+  // workspace per solve (batch_job_words): padded sol and res, 4 record words per
+  // position, the slots; the caller has reserved it before staging its inputs
+  // behind it, so the pool is never reallocated here
   size_t pool = 0;
-  for (int k = 0; k < count; ++k)
-    pool += 6 * align32(v[k].c->g.size()) + align32((size_t)4 * (nsm + 1) * kResSlotWords);
+  for (int k = 0; k < count; ++k) pool += batch_job_words(v[k].c->g.size());
+  if (pool > o->batch.cap) return fail(PYOMGPU_EINVAL, "resident batch: work pool not reserved");
   if (int rc = batch_reserve(o, count, pool, 1)) return rc;
   if (int rc = rmulti_reserve(o, count)) return rc;
   *used = true;
@@ -860,10 +882,9 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
         smem = std::max(smem, cut.smem);
         CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
         // records and slots all-ones: no tag of the solve (generation 0)
-        CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + align32((size_t)4 * (nsm + 1) * kResSlotWords)) * sizeof(double),
-                           st));
+        CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
         launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
-        cur += 6 * P + align32((size_t)4 * (nsm + 1) * kResSlotWords);
+        cur += batch_job_words(c->g.size());
         order.push_back(k);
       }
       jf[gi + 1] = (int)order.size() - launch_jobs.back();
@@ -1588,7 +1609,7 @@ int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t co
   size_t work = 0, stage = 0;
   std::vector<char> f_host(count), s_host(count);
   for (int k = 0; k < count; ++k) {
-    work += 5 * align32(ctx[k]->g.size());
+    work += batch_job_words(ctx[k]->g.size());
     f_host[k] = forc && forc[k] && !is_device_ptr(forc[k]);
     s_host[k] = !is_device_ptr(sol[k]);
     stage += (f_host[k] + s_host[k]) * align32(ctx[k]->n2);
