@@ -723,15 +723,13 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   return worst;
 }
 
-// Index words of the multi-solve launches: group_base and job_first of each of
-// at most kResSplits launches (2^t groups in launch t).
+// Index words of the multi-solve launches (at most kResSplits launches, 2^t
+// groups in launch t): the group_base offsets of every launch, one queue
+// counter per launch, the error flag, then the assign tables (per launch
+// ngroup x (jobs + 1) words; at most 31 x (count + 1) in all).
 constexpr int kResSplits = 5;
-inline size_t rmulti_idx_words(int count) {
-  (void)count;
-  size_t n = 0;
-  for (int t = 0; t < kResSplits; ++t) n += 2 * ((size_t(1) << t) + 1);
-  return n;
-}
+constexpr size_t kResIdxHead = 64;  // group_base words (sum of 2^t + 1 = 36) + queues (5) + error (1), rounded
+inline size_t rmulti_idx_words(int count) { return kResIdxHead + 31 * ((size_t)count + 1); }
 
 // Grows the owner's table for `count` resident jobs.
 int rmulti_reserve(pyomgpu_ctx* o, int count) {
@@ -764,10 +762,10 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
 // into 2^t groups of nsm / 2^t blocks (t = 0 .. 4), every solve goes to the
 // finest split it fits in (res_cut with the fewest pieces, 16 points per
 // thread) that has at least as many solves as groups, and one launch of
-// cg_res_multi_kernel per split runs its solves, assigned to the groups
-// longest first (estimated time: the
-// square root of the point count for the iterations, times the cut's
-// iteration estimate plus ~6 us of reduction latency) to the least loaded.
+// cg_res_multi_kernel per split runs its solves, which its groups draw from
+// one queue longest first (estimated time: the square root of the point
+// count for the iterations, times the cut's iteration estimate plus ~6 us of
+// reduction latency), so a group that finishes early takes the next one.
 // *used = false (nothing run) when a grid does not fit on chip or the
 // resident kernel is unavailable; the caller then runs the work-queue kernel.
 int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol,
@@ -817,9 +815,10 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   CK(cudaMemsetAsync(R.d_ctl, 0, sizeof(SyncCtl) * count, st));
   // jobs in launch order: split by split, group by group
   std::vector<int> order;
-  std::vector<int> launch_jobs, launch_groups, launch_gs;  // per launch: first job, groups, blocks per group
-  std::vector<int> idx_base;                    // per launch: offset of its group_base / job_first in h_idx
-  int nidx = 0;
+  std::vector<int> launch_jobs, launch_njobs, launch_groups, launch_gs;  // per launch: first job, jobs, groups, size
+  std::vector<size_t> launch_gb, launch_assign;  // per launch: offsets of its group_base and assign table in h_idx
+  size_t nassign = kResIdxHead;
+  int ngb = 0;
   size_t smem = 0;
   double* cur = B.pool;
   for (int t = 0; t < kResSplits; ++t) {
@@ -836,71 +835,71 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
       }
     if (mine.empty()) continue;
     std::stable_sort(mine.begin(), mine.end(), [&](int a, int b) { return est[a] > est[b]; });
-    std::vector<std::vector<int>> groups((size_t)ng);
-    std::vector<double> load((size_t)ng, 0.0);
-    for (int k : mine) {
-      const int gi = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-      groups[gi].push_back(k);
-      load[gi] += est[k];
-    }
     launch_jobs.push_back((int)order.size());
+    launch_njobs.push_back((int)mine.size());
     launch_groups.push_back(ng);
     launch_gs.push_back(gs);
-    idx_base.push_back(nidx);
-    int* gb = R.h_idx + nidx;
-    int* jf = gb + ng + 1;
-    for (int gi = 0; gi <= ng; ++gi) gb[gi] = gi * gs;
-    jf[0] = (int)order.size() - launch_jobs.back();
-    for (int gi = 0; gi < ng; ++gi) {
-      for (int k : groups[gi]) {
-        const pyomgpu_ctx* c = v[k].c;
-        ResCut cut;
-        res_cut(c->nx, c->ny, gs, R.smem_cap, 16, false, cut);
-        const size_t P = align32(c->g.size());
-        CGResParams& J = R.h_jobs[order.size()];
-        J = CGResParams{};
-        J.g = c->g;
-        J.op = c->sf.dev();
-        J.forc = v[k].forc ? v[k].forc : c->zeros;
-        J.sol = cur;
-        J.res = cur + P;
-        J.hx = cur + 2 * P;
-        J.hsize = (long long)c->g.size();
-        J.slots = cur + 6 * P;
-        J.nslot = cut.npx * cut.npy + 1;
-        J.npx = cut.npx;
-        J.npy = cut.npy;
-        J.wmax = cut.w;
-        J.hmax = cut.h;
-        J.eps = eps;
-        J.rtol = rtol;
-        J.max_it = max_it;
-        J.ctl = R.d_ctl + k;
-        J.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
-        J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
-        J.out = R.d_out + k;
-        smem = std::max(smem, cut.smem);
-        CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
-        // records and slots all-ones: no tag of the solve (generation 0)
-        CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
-        launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
-        cur += batch_job_words(c->g.size());
-        order.push_back(k);
-      }
-      jf[gi + 1] = (int)order.size() - launch_jobs.back();
+    launch_gb.push_back((size_t)ngb);
+    for (int gi = 0; gi <= ng; ++gi) R.h_idx[ngb + gi] = gi * gs;
+    ngb += ng + 1;
+    launch_assign.push_back(nassign);
+    nassign += (size_t)ng * (mine.size() + 1);
+    for (int k : mine) {
+      const pyomgpu_ctx* c = v[k].c;
+      ResCut cut;
+      res_cut(c->nx, c->ny, gs, R.smem_cap, 16, false, cut);
+      const size_t P = align32(c->g.size());
+      CGResParams& J = R.h_jobs[order.size()];
+      J = CGResParams{};
+      J.g = c->g;
+      J.op = c->sf.dev();
+      J.forc = v[k].forc ? v[k].forc : c->zeros;
+      J.sol = cur;
+      J.res = cur + P;
+      J.hx = cur + 2 * P;
+      J.hsize = (long long)c->g.size();
+      J.slots = cur + 6 * P;
+      J.nslot = cut.npx * cut.npy + 1;
+      J.npx = cut.npx;
+      J.npy = cut.npy;
+      J.wmax = cut.w;
+      J.hmax = cut.h;
+      J.eps = eps;
+      J.rtol = rtol;
+      J.max_it = max_it;
+      J.ctl = R.d_ctl + k;
+      J.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
+      J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
+      J.out = R.d_out + k;
+      smem = std::max(smem, cut.smem);
+      CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
+      // records and slots all-ones: no tag of the solve (generation 0)
+      CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
+      launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
+      cur += batch_job_words(c->g.size());
+      order.push_back(k);
     }
-    nidx += 2 * (ng + 1);
   }
   o->stall_next = 0;
+  // queue counters and the error flag zero, assign tables all-ones (kResUnposted)
+  int* d_queue = R.d_idx + 36;
+  int* d_err = R.d_idx + 36 + kResSplits;
   CK(cudaMemcpyAsync(R.d_jobs, R.h_jobs, sizeof(CGResParams) * order.size(), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(R.d_idx, R.h_idx, sizeof(int) * nidx, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(R.d_idx, R.h_idx, sizeof(int) * ngb, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d_queue, 0, sizeof(int) * (kResSplits + 1), st));
+  CK(cudaMemsetAsync(R.d_idx + kResIdxHead, 0xFF, sizeof(int) * (nassign - kResIdxHead), st));
   CK(cudaEventRecord(o->e0, st));
   for (size_t L = 0; L < launch_jobs.size(); ++L) {
     ResMultiParams M{};
     M.jobs = R.d_jobs + launch_jobs[L];
-    M.group_base = R.d_idx + idx_base[L];
-    M.job_first = M.group_base + launch_groups[L] + 1;
+    M.njobs = launch_njobs[L];
     M.ngroup = launch_groups[L];
+    M.group_base = R.d_idx + launch_gb[L];
+    M.queue = reinterpret_cast<unsigned*>(d_queue + L);
+    M.assign = reinterpret_cast<unsigned*>(R.d_idx + launch_assign[L]);
+    M.error = d_err;
+    // a block waits for its group's next draw while the first block finishes a whole solve
+    M.timeout_ns = (unsigned long long)(std::max(120.0, 64.0 * o->timeout_s) * 1e9);
     void* args[] = {&M};
     const int grid = launch_groups[L] * launch_gs[L];
     CK(cudaLaunchCooperativeKernel(cg_res_multi_kernel_ptr(), dim3(grid), dim3(kResThreads), args, smem, st));
@@ -908,6 +907,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   CK(cudaEventRecord(o->e1, st));
   CK(cudaMemcpyAsync(R.h_out, R.d_out, sizeof(CGResult) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(R.h_ctl, R.d_ctl, sizeof(SyncCtl) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(R.h_idx, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   for (size_t pos = 0; pos < order.size(); ++pos) {
     const int k = order[pos];
     const CGResParams& J = R.h_jobs[pos];
@@ -920,6 +920,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   if (want_res) CK(cudaMemcpyAsync(B.h_rr, B.d_rr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   CK(cudaGetLastError());
+  if (R.h_idx[0]) return fail(PYOMGPU_TIMEOUT, "resident batch: a block waited too long for its group's next solve");
   for (int k = 0; k < count; ++k)
     if (R.h_ctl[k].error) return fail(PYOMGPU_TIMEOUT, "reduction wait exceeded %.3f s", o->timeout_s);
   float ms = 0.f;

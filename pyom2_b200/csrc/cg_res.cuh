@@ -57,15 +57,21 @@ struct CGResParams {
   float* res32;
 };
 
-// Many resident solves in one launch (cg_res_multi_kernel): groups of blocks,
-// each running a list of solves one after another.  Every job has its own
-// CGResParams with npx * npy at most its group's size, its own slots, exchange
-// records (tagged), error flag and result.
+// Many resident solves in one launch (cg_res_multi_kernel): equal groups of
+// blocks taking the solves from one queue.  Every job has its own CGResParams
+// with npx * npy at most the group size, its own slots, exchange records
+// (tagged), error flag and result.
+constexpr unsigned kResUnposted = 0xFFFFFFFFu;  // assign word not yet written (the host fills all-ones)
+constexpr unsigned kResNoJob = 0xFFFFFFFEu;     // the queue is empty: the group is done
 struct ResMultiParams {
-  const CGResParams* jobs;  // device array, grouped: jobs of group k are job_first[k] .. job_first[k+1]-1
-  const int* group_base;    // ngroup + 1 block offsets
-  const int* job_first;     // ngroup + 1 job offsets
+  const CGResParams* jobs;  // device array, longest first
+  int njobs;
   int ngroup;
+  const int* group_base;    // ngroup + 1 block offsets
+  unsigned* queue;          // next job to hand out (zero on entry)
+  unsigned* assign;         // ngroup x (njobs + 1): job of each group's s-th draw (all-ones on entry)
+  int* error;               // PYOMGPU_TIMEOUT when a block gave up waiting for its group's draw
+  unsigned long long timeout_ns;
 };
 
 // Phases of the trace (worker warp 1 lane 0 unless noted "ctl": warp 0 lane 0):
