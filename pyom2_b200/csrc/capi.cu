@@ -1070,9 +1070,23 @@ int psin_and_line_psin(pyomgpu_ctx* c, double eps, int max_it, cudaStream_t st) 
     std::vector<BatchSpec> v;
     for (int k = k0; k < k1; ++k) v.push_back(BatchSpec{c, nullptr, c->psin + (size_t)k * c->n2});
     std::vector<pyomgpu_solve_info> infos(v.size());
-    int rc = run_batch(c, v, c->psin_rtol > 0.0 ? 0.0 : eps, c->psin_rtol > 0.0 ? std::max(max_it, 1000000) : max_it,
-                       c->psin_rtol, false, infos.data(), nullptr, st, c->psin_weighted);
-    if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    const double e_k = c->psin_rtol > 0.0 ? 0.0 : eps;
+    const int m_k = c->psin_rtol > 0.0 ? std::max(max_it, 1000000) : max_it;
+    // on-chip solves side by side where the grid fits (the reference's products); the
+    // work-queue kernel otherwise and for the area-weighted products
+    bool resident = false;
+    int rc = PYOMGPU_OK;
+    if (!c->psin_weighted && c->batch_kernel != 1) {
+      size_t work = 0;
+      for (const BatchSpec& b : v) work += batch_job_words(b.c->g.size());
+      if ((rc = batch_reserve(c, (int)v.size(), work, 1))) return rc;
+      rc = run_res_multi(c, v, e_k, m_k, c->psin_rtol, false, infos.data(), nullptr, st, &resident);
+      if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    }
+    if (!resident) {
+      rc = run_batch(c, v, e_k, m_k, c->psin_rtol, false, infos.data(), nullptr, st, c->psin_weighted);
+      if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+    }
     for (int k = k0; k < k1; ++k) {
       const pyomgpu_solve_info& info = infos[k - k0];
       if (info.status == PYOMGPU_NAN) return fail(PYOMGPU_NAN, "psin solve of island %d: estimated error is NaN", k + 1);
