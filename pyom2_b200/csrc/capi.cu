@@ -574,23 +574,23 @@ int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
     if (B.h_state) cudaFreeHost(B.h_state);
     if (B.d_rr) cudaFree(B.d_rr);
     if (B.h_rr) cudaFreeHost(B.h_rr);
-    if (B.d_group) cudaFree(B.d_group);
-    if (B.h_group) cudaFreeHost(B.h_group);
+    if (B.d_act) cudaFree(B.d_act);
+    if (B.h_act) cudaFreeHost(B.h_act);
     B.d_probs = nullptr;
     B.h_probs = nullptr;
     B.d_state = nullptr;
     B.h_state = nullptr;
     B.d_rr = B.h_rr = nullptr;
-    B.d_group = B.h_group = nullptr;
+    B.d_act = B.h_act = nullptr;
     B.cap_probs = 0;
     if (int rc = dalloc(&B.d_probs, (size_t)count)) return rc;
     if (int rc = dalloc(&B.d_state, (size_t)count)) return rc;
     if (int rc = dalloc(&B.d_rr, (size_t)count * 2)) return rc;
-    if (int rc = dalloc(&B.d_group, (size_t)count + 1)) return rc;
+    if (int rc = dalloc(&B.d_act, (size_t)3 * count + 2)) return rc;
     if (cudaMallocHost((void**)&B.h_probs, sizeof(BatchProblem) * count) != cudaSuccess ||
         cudaMallocHost((void**)&B.h_state, sizeof(BatchState) * count) != cudaSuccess ||
         cudaMallocHost((void**)&B.h_rr, sizeof(double) * 2 * count) != cudaSuccess ||
-        cudaMallocHost((void**)&B.h_group, sizeof(int) * (count + 1)) != cudaSuccess)
+        cudaMallocHost((void**)&B.h_act, sizeof(int) * (2 * count + 2)) != cudaSuccess)
       return fail(PYOMGPU_ENOMEM, "cudaMallocHost");
     B.cap_probs = count;
   }
@@ -610,6 +610,20 @@ int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
 int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol, bool want_res,
               pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st, int weighted = 0) {
   const int count = (int)v.size();
+  if (count > kBatchActMax) {  // one launch per kBatchActMax solves
+    int worst = PYOMGPU_OK;
+    float total = 0.f;
+    for (int k0 = 0; k0 < count; k0 += kBatchActMax) {
+      const std::vector<BatchSpec> sub(v.begin() + k0, v.begin() + std::min(count, k0 + kBatchActMax));
+      float ms = 0.f;
+      const int rc = run_batch(o, sub, eps, max_it, rtol, want_res, infos ? infos + k0 : nullptr, &ms, st, weighted);
+      if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
+      worst = std::max(worst, rc);
+      total += ms;
+    }
+    if (ms_out) *ms_out = total;
+    return worst;
+  }
   size_t pool = 0, tasks = 0;
   for (const BatchSpec& b : v) {
     pool += 5 * align32(b.c->g.size());
@@ -620,7 +634,7 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   auto& B = o->batch;
   CK(cudaMemsetAsync(B.pool, 0, pool * sizeof(double), st));
   CK(cudaMemsetAsync(B.sync, 0, 8 * sizeof(unsigned long long), st));
-  // all problems in one group, largest first: every sweep and barrier serves every
+  // all problems in one launch, largest first: every sweep and barrier serves every
   // problem still running, so the barrier latency is shared by all of them (solving
   // L2-sized groups one after another measured slower: each group then pays the
   // latency-bound iterations of its slowest problem on its own)
@@ -628,9 +642,12 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   for (int k = 0; k < count; ++k) order[k] = k;
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return v[a].c->g.size() > v[b].c->g.size(); });
-  const int ngroup = 1;
-  B.h_group[0] = 0;
-  B.h_group[1] = count;
+  // the initial active list: every problem, tiles in order
+  int* h_actn = B.h_act;
+  int* h_actprob = B.h_act + 1;
+  int* h_actoff = B.h_act + 1 + count;
+  h_actn[0] = count;
+  h_actoff[0] = 0;
   double* cur = B.pool;
   int tile0 = 0;
   for (int pos = 0; pos < count; ++pos) {
@@ -656,22 +673,26 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
     pr.tile0 = tile0;
     tile0 += pr.ntx * pr.nty;
     B.h_probs[pos] = pr;
+    h_actprob[pos] = pos;
+    h_actoff[pos + 1] = tile0;
     launch_pack(b.c->g, b.sol, pr.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
   }
   CK(cudaMemcpyAsync(B.d_probs, B.h_probs, sizeof(BatchProblem) * count, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(B.d_group, B.h_group, sizeof(int) * (ngroup + 1), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(B.d_act, B.h_act, sizeof(int) * (2 * count + 2), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(B.d_act + 2 * count + 2, 0, sizeof(int) * count, st));  // per-problem tile counters
   CK(cudaMemsetAsync(B.d_state, 0, sizeof(BatchState) * count, st));
   BatchParams P{};
   P.probs = B.d_probs;
   P.state = B.d_state;
   P.nprob = count;
   P.ntasks = tile0;
-  P.ngroup = ngroup;
-  P.group = B.d_group;
   P.part = B.part;
+  P.act_n = B.d_act;
+  P.act_prob = B.d_act + 1;
+  P.act_off = B.d_act + 1 + count;
+  P.done = B.d_act + 2 * count + 2;
   P.ctl = reinterpret_cast<SyncCtl*>(B.sync);
   P.gen = B.sync + 2;
-  P.any_active = reinterpret_cast<int*>(B.sync + 3);
   P.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
   P.stall_extra = o->stall_next;
   o->stall_next = 0;
@@ -723,13 +744,12 @@ int run_batch(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int m
   return worst;
 }
 
-// Index words of the multi-solve launches (at most kResSplits launches, 2^t
-// groups in launch t): the group_base offsets of every launch, one queue
-// counter per launch, the error flag, then the assign tables (per launch
-// ngroup x (jobs + 1) words; at most 31 x (count + 1) in all).
-constexpr int kResSplits = 5;
-constexpr size_t kResIdxHead = 64;  // group_base words (sum of 2^t + 1 = 36) + queues (5) + error (1), rounded
-inline size_t rmulti_idx_words(int count) { return kResIdxHead + 31 * ((size_t)count + 1); }
+// Index words of a multi-solve launch on at most kResMaxSlots blocks: the
+// per-block list offsets (kResMaxSlots + 1), the error flag, the per-job join
+// counters, then the (job, piece) list entries (at most one per block per job).
+inline size_t rmulti_idx_words(int count) {
+  return (size_t)kResMaxSlots + 2 + (size_t)count + 2 * (size_t)kResMaxSlots * (size_t)count;
+}
 
 // Grows the owner's table for `count` resident jobs.
 int rmulti_reserve(pyomgpu_ctx* o, int count) {
@@ -758,14 +778,14 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
   return 0;
 }
 
-// The solves of `v` on the resident kernel, several at once: the SMs are split
-// into 2^t groups of nsm / 2^t blocks (t = 0 .. 4), every solve goes to the
-// finest split it fits in (res_cut with the fewest pieces, 16 points per
-// thread) that has at least as many solves as groups, and one launch of
-// cg_res_multi_kernel per split runs its solves, which its groups draw from
-// one queue longest first (estimated time: the square root of the point
-// count for the iterations, times the cut's iteration estimate plus ~6 us of
-// reduction latency), so a group that finishes early takes the next one.
+// The solves of `v` on the resident kernel, several at once, in one launch of
+// cg_res_multi_kernel on all SMs.  Every solve takes its densest cut (res_cut
+// with the fewest pieces at 16 points per thread: the least block-time per
+// iteration) and is placed by list scheduling on the host, largest gangs
+// first, then longest: on the pieces' count of blocks that become free
+// earliest under the estimated durations (iterations ~ the square root of the
+// point count, times the cut's iteration estimate plus ~6 us of reduction
+// latency); each block runs its entries in order of planned start.
 // *used = false (nothing run) when a grid does not fit on chip or the
 // resident kernel is unavailable; the caller then runs the work-queue kernel.
 int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol,
@@ -782,26 +802,24 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     R.smem_cap = cap;
   }
   const int nsm = std::min(o->nsm, kResMaxSlots - 1);
-  // finest split each grid fits (fewest pieces at 16 points per thread)
-  std::vector<int> fit((size_t)count), tier((size_t)count, -1);
+  std::vector<ResCut> cuts((size_t)count);
+  std::vector<double> est((size_t)count);
+  int need = 0;
   for (int k = 0; k < count; ++k) {
     const pyomgpu_ctx* c = v[k].c;
-    ResCut cut;
-    if (!res_cut(c->nx, c->ny, nsm, R.smem_cap, 16, true, cut)) return PYOMGPU_OK;
-    int t = 0;
-    while (t + 1 < kResSplits && cut.npx * cut.npy <= nsm >> (t + 1)) t++;
-    fit[k] = t;
+    if (!res_cut(c->nx, c->ny, nsm, R.smem_cap, 16, true, cuts[k])) return PYOMGPU_OK;
+    need += cuts[k].npx * cuts[k].npy;
   }
-  // from the finest split down, a split takes every unassigned grid that fits it
-  // if they are at least as many as its groups (else they move to coarser
-  // splits, where fewer, larger groups keep every SM busy); split 0 takes the rest
-  for (int t = kResSplits - 1; t >= 0; --t) {
-    int n = 0;
-    for (int k = 0; k < count; ++k) n += tier[k] < 0 && fit[k] >= t;
-    if (n == 0 || (t > 0 && n < (1 << t))) continue;
-    for (int k = 0; k < count; ++k)
-      if (tier[k] < 0 && fit[k] >= t) tier[k] = t;
-  }
+  // fewer pieces in all than SMs: every solve gets its share of the SMs (in
+  // proportion to its densest cut) and the fastest cut within it, all at once
+  if (need < nsm)
+    for (int k = 0; k < count; ++k) {
+      const pyomgpu_ctx* c = v[k].c;
+      const int share = std::max(cuts[k].npx * cuts[k].npy, (nsm * cuts[k].npx * cuts[k].npy) / need);
+      ResCut cut;
+      if (res_cut(c->nx, c->ny, share, R.smem_cap, 16, false, cut)) cuts[k] = cut;
+    }
+  for (int k = 0; k < count; ++k) est[k] = std::sqrt((double)v[k].c->nx * v[k].c->ny) * (cuts[k].cost + 6000.0);
   // workspace per solve (batch_job_words): padded sol and res, 4 record words per
   // position, the slots; the caller has reserved it before staging its inputs
   // behind it, so the pool is never reallocated here
@@ -812,105 +830,117 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   if (int rc = rmulti_reserve(o, count)) return rc;
   *used = true;
   auto& B = o->batch;
-  CK(cudaMemsetAsync(R.d_ctl, 0, sizeof(SyncCtl) * count, st));
-  // jobs in launch order: split by split, group by group
-  std::vector<int> order;
-  std::vector<int> launch_jobs, launch_njobs, launch_groups, launch_gs;  // per launch: first job, jobs, groups, size
-  std::vector<size_t> launch_gb, launch_assign;  // per launch: offsets of its group_base and assign table in h_idx
-  size_t nassign = kResIdxHead;
-  int ngb = 0;
+  // list scheduling: gangs on the blocks free earliest
+  std::vector<int> order((size_t)count);
+  for (int k = 0; k < count; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const int na = cuts[a].npx * cuts[a].npy, nb = cuts[b].npx * cuts[b].npy;
+    return na != nb ? na > nb : est[a] > est[b];
+  });
+  std::vector<double> free_at((size_t)nsm, 0.0), start((size_t)count, 0.0);
+  std::vector<std::vector<int>> gang((size_t)count);  // blocks of each job, piece order
+  std::vector<int> blk((size_t)nsm);
+  for (int k : order) {
+    const int nb = cuts[k].npx * cuts[k].npy;
+    for (int b = 0; b < nsm; ++b) blk[b] = b;
+    std::partial_sort(blk.begin(), blk.begin() + nb, blk.end(), [&](int a, int b) {
+      return free_at[a] != free_at[b] ? free_at[a] < free_at[b] : a < b;
+    });
+    double t = 0.0;
+    for (int q = 0; q < nb; ++q) t = std::max(t, free_at[blk[q]]);
+    start[k] = t;
+    gang[k].assign(blk.begin(), blk.begin() + nb);
+    std::sort(gang[k].begin(), gang[k].end());
+    for (int b : gang[k]) free_at[b] = t + est[k];
+  }
+  // per-block lists in planned-start order (ties: job order above), one total order for all
+  std::vector<int> rank((size_t)count);
+  {
+    std::vector<int> by_start = order;
+    std::stable_sort(by_start.begin(), by_start.end(), [&](int a, int b) { return start[a] < start[b]; });
+    for (int r = 0; r < count; ++r) rank[by_start[r]] = r;
+  }
+  std::vector<std::vector<std::pair<int, int>>> lists((size_t)nsm);  // (rank, piece) per block
+  for (int k = 0; k < count; ++k)
+    for (int q = 0; q < (int)gang[k].size(); ++q) lists[gang[k][q]].push_back({rank[k], q});
+  int* h_off = R.h_idx;
+  int* h_err = R.h_idx + kResMaxSlots + 1;
+  int* h_join = h_err + 1;
+  int2* h_list = reinterpret_cast<int2*>(h_join + count + (count & 1));  // 8-byte aligned
+  (void)h_err;
+  std::vector<int> job_of_rank((size_t)count);
+  for (int k = 0; k < count; ++k) job_of_rank[rank[k]] = k;
+  int nent = 0;
+  for (int b = 0; b < nsm; ++b) {
+    std::sort(lists[b].begin(), lists[b].end());
+    h_off[b] = nent;
+    for (const auto& e : lists[b]) h_list[nent++] = make_int2(e.first, e.second);
+  }
+  h_off[nsm] = nent;
+  // the job table in rank order (list entries name ranks)
   size_t smem = 0;
   double* cur = B.pool;
-  for (int t = 0; t < kResSplits; ++t) {
-    const int ng = 1 << t, gs = nsm >> t;
-    std::vector<int> mine;
-    std::vector<double> est((size_t)count, 0.0);
-    for (int k = 0; k < count; ++k)
-      if (tier[k] == t) {
-        const pyomgpu_ctx* c = v[k].c;
-        ResCut cut;
-        res_cut(c->nx, c->ny, gs, R.smem_cap, 16, false, cut);
-        est[k] = std::sqrt((double)c->nx * c->ny) * (cut.cost + 6000.0);
-        mine.push_back(k);
-      }
-    if (mine.empty()) continue;
-    std::stable_sort(mine.begin(), mine.end(), [&](int a, int b) { return est[a] > est[b]; });
-    launch_jobs.push_back((int)order.size());
-    launch_njobs.push_back((int)mine.size());
-    launch_groups.push_back(ng);
-    launch_gs.push_back(gs);
-    launch_gb.push_back((size_t)ngb);
-    for (int gi = 0; gi <= ng; ++gi) R.h_idx[ngb + gi] = gi * gs;
-    ngb += ng + 1;
-    launch_assign.push_back(nassign);
-    nassign += (size_t)ng * (mine.size() + 1);
-    for (int k : mine) {
-      const pyomgpu_ctx* c = v[k].c;
-      ResCut cut;
-      res_cut(c->nx, c->ny, gs, R.smem_cap, 16, false, cut);
-      const size_t P = align32(c->g.size());
-      CGResParams& J = R.h_jobs[order.size()];
-      J = CGResParams{};
-      J.g = c->g;
-      J.op = c->sf.dev();
-      J.forc = v[k].forc ? v[k].forc : c->zeros;
-      J.sol = cur;
-      J.res = cur + P;
-      J.hx = cur + 2 * P;
-      J.hsize = (long long)c->g.size();
-      J.slots = cur + 6 * P;
-      J.nslot = cut.npx * cut.npy + 1;
-      J.npx = cut.npx;
-      J.npy = cut.npy;
-      J.wmax = cut.w;
-      J.hmax = cut.h;
-      J.eps = eps;
-      J.rtol = rtol;
-      J.max_it = max_it;
-      J.ctl = R.d_ctl + k;
-      J.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
-      J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
-      J.out = R.d_out + k;
-      smem = std::max(smem, cut.smem);
-      CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
-      // records and slots all-ones: no tag of the solve (generation 0)
-      CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
-      launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
-      cur += batch_job_words(c->g.size());
-      order.push_back(k);
-    }
+  for (int r = 0; r < count; ++r) {
+    const int k = job_of_rank[r];
+    const pyomgpu_ctx* c = v[k].c;
+    const ResCut& cut = cuts[k];
+    const size_t P = align32(c->g.size());
+    CGResParams& J = R.h_jobs[r];
+    J = CGResParams{};
+    J.g = c->g;
+    J.op = c->sf.dev();
+    J.forc = v[k].forc ? v[k].forc : c->zeros;
+    J.sol = cur;
+    J.res = cur + P;
+    J.hx = cur + 2 * P;
+    J.hsize = (long long)c->g.size();
+    J.slots = cur + 6 * P;
+    J.nslot = cut.npx * cut.npy + 1;
+    J.npx = cut.npx;
+    J.npy = cut.npy;
+    J.wmax = cut.w;
+    J.hmax = cut.h;
+    J.eps = eps;
+    J.rtol = rtol;
+    J.max_it = max_it;
+    J.ctl = R.d_ctl + k;
+    J.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
+    J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
+    J.out = R.d_out + k;
+    smem = std::max(smem, cut.smem);
+    CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
+    // records and slots all-ones: no tag of the solve (generation 0)
+    CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
+    launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
+    cur += batch_job_words(c->g.size());
   }
   o->stall_next = 0;
-  // queue counters and the error flag zero, assign tables all-ones (kResUnposted)
-  int* d_queue = R.d_idx + 36;
-  int* d_err = R.d_idx + 36 + kResSplits;
-  CK(cudaMemcpyAsync(R.d_jobs, R.h_jobs, sizeof(CGResParams) * order.size(), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(R.d_idx, R.h_idx, sizeof(int) * ngb, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(d_queue, 0, sizeof(int) * (kResSplits + 1), st));
-  CK(cudaMemsetAsync(R.d_idx + kResIdxHead, 0xFF, sizeof(int) * (nassign - kResIdxHead), st));
+  const size_t list_words = (size_t)(reinterpret_cast<int*>(h_list + nent) - R.h_idx);
+  CK(cudaMemcpyAsync(R.d_jobs, R.h_jobs, sizeof(CGResParams) * count, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(R.d_idx + kResMaxSlots + 1, 0, sizeof(int) * (count + 1), st));  // error flag, join counters
+  // offsets, then (after the zeroed error flag and join counters) the entries
+  CK(cudaMemcpyAsync(R.d_idx, R.h_idx, sizeof(int) * (kResMaxSlots + 1), cudaMemcpyHostToDevice, st));
+  const size_t lst0 = (size_t)(reinterpret_cast<int*>(h_list) - R.h_idx);
+  CK(cudaMemcpyAsync(R.d_idx + lst0, h_list, sizeof(int) * (list_words - lst0), cudaMemcpyHostToDevice, st));
+  int* d_err = R.d_idx + kResMaxSlots + 1;
+  ResMultiParams M{};
+  M.jobs = R.d_jobs;
+  M.list_off = R.d_idx;
+  M.list = reinterpret_cast<const int2*>(R.d_idx + lst0);
+  M.join = d_err + 1;
+  M.error = d_err;
+  // a block may wait for its gang while other pieces finish their previous solves
+  M.gang_timeout_ns = (unsigned long long)(std::max(120.0, 64.0 * o->timeout_s) * 1e9);
+  void* args[] = {&M};
   CK(cudaEventRecord(o->e0, st));
-  for (size_t L = 0; L < launch_jobs.size(); ++L) {
-    ResMultiParams M{};
-    M.jobs = R.d_jobs + launch_jobs[L];
-    M.njobs = launch_njobs[L];
-    M.ngroup = launch_groups[L];
-    M.group_base = R.d_idx + launch_gb[L];
-    M.queue = reinterpret_cast<unsigned*>(d_queue + L);
-    M.assign = reinterpret_cast<unsigned*>(R.d_idx + launch_assign[L]);
-    M.error = d_err;
-    // a block waits for its group's next draw while the first block finishes a whole solve
-    M.timeout_ns = (unsigned long long)(std::max(120.0, 64.0 * o->timeout_s) * 1e9);
-    void* args[] = {&M};
-    const int grid = launch_groups[L] * launch_gs[L];
-    CK(cudaLaunchCooperativeKernel(cg_res_multi_kernel_ptr(), dim3(grid), dim3(kResThreads), args, smem, st));
-  }
+  CK(cudaLaunchCooperativeKernel(cg_res_multi_kernel_ptr(), dim3(nsm), dim3(kResThreads), args, smem, st));
   CK(cudaEventRecord(o->e1, st));
   CK(cudaMemcpyAsync(R.h_out, R.d_out, sizeof(CGResult) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(R.h_ctl, R.d_ctl, sizeof(SyncCtl) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(R.h_idx, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  for (size_t pos = 0; pos < order.size(); ++pos) {
-    const int k = order[pos];
-    const CGResParams& J = R.h_jobs[pos];
+  for (int r = 0; r < count; ++r) {
+    const int k = job_of_rank[r];
+    const CGResParams& J = R.h_jobs[r];
     if (want_res) {
       launch_fill_cyclic(J.g, J.sol, st);
       launch_residual(J.g, J.op, J.forc, J.sol, v[k].c->part, 1024, B.d_rr + 2 * k, st);
@@ -920,7 +950,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   if (want_res) CK(cudaMemcpyAsync(B.h_rr, B.d_rr, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   CK(cudaGetLastError());
-  if (R.h_idx[0]) return fail(PYOMGPU_TIMEOUT, "resident batch: a block waited too long for its group's next solve");
+  if (R.h_idx[0]) return fail(PYOMGPU_TIMEOUT, "resident batch: a gang did not assemble in time");
   for (int k = 0; k < count; ++k)
     if (R.h_ctl[k].error) return fail(PYOMGPU_TIMEOUT, "reduction wait exceeded %.3f s", o->timeout_s);
   float ms = 0.f;
@@ -938,7 +968,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     I.outer_iterations = 1;
     I.estimated_error = r.est;
     I.device_ms = ms;
-    I.kernel_launches = (int)launch_jobs.size();
+    I.kernel_launches = 1;
     if (want_res) {
       const double rr = B.h_rr[2 * k], bb = B.h_rr[2 * k + 1];
       I.rel_residual = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);

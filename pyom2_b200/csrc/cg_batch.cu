@@ -2,13 +2,15 @@
 // launch, each following congrad_streamfunction's control flow
 // (solve_streamfct.f90:153-327) with its own scalars.
 //
-// The tiles of all problems form one task list; every block walks it with a
-// static stride.  All problems advance in lockstep through three kinds of
-// sweep (init, A: direction + stencil, B: update) separated by grid barriers.
-// The last block to reach a barrier sums each problem's per-tile partials in
-// a fixed order, runs each problem's stopping logic, and releases the others
-// with a generation flag, so every problem ends with exactly the iterations
-// and status an individual solve would give.
+// The tiles of the problems still running form one task list; every block
+// walks it with a static stride.  All problems advance in lockstep through
+// three kinds of sweep (init, A: direction + stencil, B: update) separated by
+// grid barriers.  The block that finishes a problem's last tile of a sweep
+// (a per-problem arrival counter) sums that problem's per-tile partials in a
+// fixed order and runs its stopping logic, so every problem ends with exactly
+// the iterations and status an individual solve would give; the last block
+// at the barrier rebuilds the list of problems still running and releases
+// the others with a generation flag.
 #include <math.h>
 
 #include "cg_batch.cuh"
@@ -33,17 +35,6 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ int task_problem(const BatchParams& P, int task, int p0, int p1) {
-  int lo = p0, hi = p1 - 1;  // last problem of the group with tile0 <= task
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (P.probs[mid].tile0 <= task)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
 
 // The state moves through L2 only (ld.cg / st.cg): the reducing block may be
 // a different one at every barrier, and a stale L1 line must never be read.
@@ -138,12 +129,79 @@ __device__ void after_b(BatchState& st, const BatchProblem& pr, const double* v)
   start_iteration(st, pr, st.n + 1);
 }
 
-// Grid barrier whose last arrival reduces the partials of every problem that
-// took part in the sweep just finished and advances its state.  Returns false
-// on time-out.
-__device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, int kind, int p0, int p1,
-                               unsigned extra = 0) {
-  __shared__ int s_last, s_ok, s_any;
+__device__ __forceinline__ int atom_add_acqrel_i32(int* p, int v) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// Sums problem p's per-tile partials of the sweep just finished, in a fixed
+// order (lane l: tiles l, l+32, ..., four loads in flight; then a shuffle
+// tree), and advances its state.  Warp 0 of the block that finished the
+// problem's last tile; the tiles' partials are visible through the acq_rel
+// arrivals on done[p].
+__device__ void reduce_problem(const BatchParams& P, int p, int kind) {
+  const int lane = threadIdx.x & 31;
+  const BatchProblem& pr = P.probs[p];
+  const int nt = pr.ntx * pr.nty;
+  const int nv = (kind == kInit) ? 4 : 2;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int t0 = lane; t0 < nt; t0 += 128) {
+    double x[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int t = t0 + 32 * u;
+      const double* q = P.part + (size_t)(pr.tile0 + (t < nt ? t : 0)) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; k++) x[u][k] = (t < nt && k < nv) ? __ldcg(q + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (t0 + 32 * u >= nt) break;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (k >= nv) break;
+        const bool is_max = (kind == kInit && k == 3) || (kind == kSweepA && k == 1);
+        v[k] = is_max ? fmax(v[k], x[u][k]) : v[k] + x[u][k];
+      }
+    }
+  }
+  for (int k = 0; k < nv; k++) {
+    const bool is_max = (kind == kInit && k == 3) || (kind == kSweepA && k == 1);
+    v[k] = is_max ? warp_max(v[k]) : warp_sum(v[k]);
+  }
+  if (lane == 0) {
+    BatchState st = load_state(&P.state[p]);
+    if (kind == kInit)
+      after_init(st, pr, v);
+    else if (kind == kSweepA)
+      after_a(st, pr, v);
+    else
+      after_b(st, pr, v);
+    store_state(&P.state[p], st);
+    __stcg(&P.done[p], 0);  // ready for the next sweep (ordered before this block's barrier arrival)
+  }
+}
+
+// After a tile of problem p: counts it (thread 0) and, in the block that
+// finished the problem's last tile of this sweep, reduces the problem.
+__device__ __forceinline__ void tile_finished(const BatchParams& P, int p, int kind, int* s_flag) {
+  if (threadIdx.x == 0) {
+    __threadfence();  // this tile's partials before its arrival
+    const BatchProblem& pr = P.probs[p];
+    *s_flag = atom_add_acqrel_i32(&P.done[p], 1) + 1 == pr.ntx * pr.nty;
+  }
+  __syncthreads();
+  if (*s_flag && threadIdx.x < 32) reduce_problem(P, p, kind);
+}
+
+// Grid barrier after a sweep; the last block to arrive rebuilds the list of
+// problems in phase `want` (the next sweep's) and releases the others with a
+// generation flag.  Every block then copies the list into shared memory
+// (when it fits).  Returns false on time-out.
+__device__ bool barrier_rebuild(const BatchParams& P, unsigned long long& epoch, int want, unsigned extra,
+                                int* s_act_prob, int* s_act_off, int* s_actn) {
+  __shared__ int s_last, s_ok;
   __syncthreads();
   epoch += 1;
   if (threadIdx.x == 0) {
@@ -153,66 +211,36 @@ __device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, 
   }
   __syncthreads();
   if (s_last) {
-    // every partial of this sweep is visible (acquire side of the arrivals)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int any = 0;
-    for (int p = p0 + warp; p < p1; p += kBatchThreads / 32) {
-      const BatchProblem& pr = P.probs[p];
-      const int phase = __ldcg(&P.state[p].phase);
-      if (kind != kInit && phase != kind) {  // finished earlier (init reduces every problem)
-        if (lane == 0) any |= phase != 0;
-        continue;
-      }
-      const int nt = pr.ntx * pr.nty;
-      const int nv = (kind == kInit) ? 4 : 2;
-      double v[4] = {0.0, 0.0, 0.0, 0.0};
-      // lane l sums tiles l, l+32, l+64, ... in that order; four tiles' partials are
-      // loaded before they are added, so the loads overlap
-      for (int t0 = lane; t0 < nt; t0 += 128) {
-        double x[4][4];
+    // every problem's state of this sweep is visible (acquire side of the arrivals)
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      int m = 0, off = 0;
+      for (int base = 0; base < P.nprob; base += 32) {
+        const int p = base + lane;
+        const bool in = p < P.nprob && __ldcg(&P.state[p].phase) == want;
+        const int nt = in ? P.probs[p].ntx * P.probs[p].nty : 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        int sc = nt;  // inclusive scan of the tile counts
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int t = t0 + 32 * u;
-          const double* q = P.part + (size_t)(pr.tile0 + (t < nt ? t : 0)) * 4;
-#pragma unroll
-          for (int k = 0; k < 4; k++) x[u][k] = (t < nt && k < nv) ? __ldcg(q + k) : 0.0;
+        for (int d = 1; d < 32; d <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, sc, d);
+          if (lane >= d) sc += y;
         }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          if (t0 + 32 * u >= nt) break;
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            if (k >= nv) break;
-            const bool is_max = (kind == kInit && k == 3) || (kind == kSweepA && k == 1);
-            v[k] = is_max ? fmax(v[k], x[u][k]) : v[k] + x[u][k];
-          }
+        if (in) {
+          const int pos = m + __popc(bal & ((1u << lane) - 1u));
+          __stcg(&P.act_prob[pos], p);
+          __stcg(&P.act_off[pos + 1], off + sc);
         }
+        m += __popc(bal);
+        off += __shfl_sync(0xffffffffu, sc, 31);
       }
-      for (int k = 0; k < nv; k++) {
-        const bool is_max = (kind == kInit && k == 3) || (kind == kSweepA && k == 1);
-        v[k] = is_max ? warp_max(v[k]) : warp_sum(v[k]);
-      }
+      __syncwarp();  // every lane's list entries before lane 0's release
       if (lane == 0) {
-        BatchState st = load_state(&P.state[p]);
-        if (kind == kInit)
-          after_init(st, pr, v);
-        else if (kind == kSweepA)
-          after_a(st, pr, v);
-        else
-          after_b(st, pr, v);
-        store_state(&P.state[p], st);
-        any |= st.phase != 0;
+        __stcg(&P.act_off[0], 0);
+        __stcg(P.act_n, m);
+        __threadfence();
+        st_release_u64(P.gen, epoch);
       }
-    }
-    __threadfence();
-    if (threadIdx.x == 0) s_any = 0;
-    __syncthreads();
-    if (lane == 0 && any) atomicOr(&s_any, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __stcg(P.any_active, s_any);
-      __threadfence();
-      st_release_u64(P.gen, epoch);
     }
   } else if (threadIdx.x == 0) {
     const unsigned long long t0 = globaltimer_ns();
@@ -228,144 +256,202 @@ __device__ bool reduce_barrier(const BatchParams& P, unsigned long long& epoch, 
     }
   }
   __syncthreads();
-  return s_ok != 0;
+  if (!s_ok) return false;
+  if (s_last && threadIdx.x == 0) __threadfence();  // the list's stores before this block reads them back
+  __syncthreads();
+  const int m = __ldcg(P.act_n);  // at most nprob <= kBatchActMax
+  for (int k = threadIdx.x; k < m; k += kBatchThreads) {
+    s_act_prob[k] = __ldcg(&P.act_prob[k]);
+    s_act_off[k + 1] = __ldcg(&P.act_off[k + 1]);
+  }
+  if (threadIdx.x == 0) {
+    s_act_off[0] = 0;
+    *s_actn = m;
+  }
+  __syncthreads();
+  return true;
+}
+
+// Position of `task` in the active list: the k with off[k] <= task < off[k+1].
+__device__ __forceinline__ int act_find(const int* off, int m, int task) {
+  int lo = 0, hi = m - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= task)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
 
 }  // namespace
 
 __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchParams P) {
   __shared__ double b_s[kBoxN], b_FX[kBoxN], b_FY[kBoxN];
+  __shared__ int s_act_prob[kBatchActMax], s_act_off[kBatchActMax + 1];
+  __shared__ int s_actn, s_flag;
   unsigned long long epoch = 0;
-
-  for (int grp = 0; grp < P.ngroup; grp++) {
-  const int p0 = P.group[grp], p1 = P.group[grp + 1];
-  const int t_lo = P.probs[p0].tile0;
-  const int t_hi = P.probs[p1 - 1].tile0 + P.probs[p1 - 1].ntx * P.probs[p1 - 1].nty;
-  // ---- init: res = forc - A sol -------------------------------------------------
-  for (int task = t_lo + blockIdx.x; task < t_hi; task += gridDim.x) {
-    const int p = task_problem(P, task, p0, p1);
-    const BatchProblem& pr = P.probs[p];
-    const Geo g = pr.g;
-    const int lt = task - pr.tile0;
-    const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
-      const int i = i0 + e % kTX, j = j0 + e / kTX;
-      if (i > g.nx || j > g.ny) continue;
-      const size_t q = g.at(i, j);
-      const double f = pr.forc[fidx(g.nx, i, j)];
-      const double r = f - apply_point(pr.op, g, pr.sol, i, j);
-      store_cyclic(pr.res, g, i, j, r);
-      const double w = pr.op.W[q];
-      const double zr = w * r;
-      const double wd = pr.weighted ? 1.0 / (pr.op.ax[i + 1] * pr.op.by[j + 1]) : 1.0;
-      v[0] += (wd * zr) * r;
-      if (w != 0.0) {
-        v[1] += f * f;
-        v[2] += r * r;
-      }
-      v[3] = fmax(v[3], fabs(zr));
+  // the active list of the initial sweep (every problem, nprob <= kBatchActMax), written by the host
+  {
+    const int m = __ldcg(P.act_n);
+    for (int k = threadIdx.x; k <= m; k += kBatchThreads) {
+      if (k < m) s_act_prob[k] = __ldcg(&P.act_prob[k]);
+      s_act_off[k] = __ldcg(&P.act_off[k]);
     }
-    double out[4];
-    block_reduce<4, 3, kBatchThreads>(v, out);
-    if (threadIdx.x == 0)
-      for (int k = 0; k < 4; k++) P.part[(size_t)task * 4 + k] = out[k];
+    if (threadIdx.x == 0) s_actn = m;
+    __syncthreads();
   }
-  if (!reduce_barrier(P, epoch, kInit, p0, p1, grp == 0 ? P.stall_extra : 0u)) return;
+  auto list_off = [&]() -> const int* { return s_act_off; };
+  auto list_prob = [&]() -> const int* { return s_act_prob; };
 
-  for (;;) {
-    if (!__ldcg(P.any_active)) break;
-    // ---- sweep A: s_new = Z res + bq s_old on tile + halo, As = A s_new ---------------
-    for (int task = t_lo + blockIdx.x; task < t_hi; task += gridDim.x) {
-      const int p = task_problem(P, task, p0, p1);
-      if (__ldcg(&P.state[p].phase) != 1) continue;
+  // ---- init: res = forc - A sol -------------------------------------------------
+  {
+    const int m = s_actn;
+    const int* off = list_off();
+    const int* prb = list_prob();
+    const int ntot = off[m];
+    for (int task = blockIdx.x; task < ntot; task += gridDim.x) {
+      const int k = act_find(off, m, task);
+      const int p = prb[k];
       const BatchProblem& pr = P.probs[p];
       const Geo g = pr.g;
-      const OpDev<double> op = pr.op;
-      const int n = __ldcg(&P.state[p].n);
-      const double bq = __ldcg(&P.state[p].bq);
-      const double* __restrict__ so = pr.s[(n + 1) & 1];
-      double* __restrict__ sn = pr.s[n & 1];
-      const int lt = task - pr.tile0;
+      const int lt = task - off[k];
       const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
-      __syncthreads();  // shared boxes of the previous task are free
-      // four box points per thread in flight (the loads do not depend on the shared stores)
-#pragma unroll 4
-      for (int e = threadIdx.x; e < kBoxN; e += kBatchThreads) {
-        const int i = i0 - 1 + e % kBX, j = j0 - 1 + e / kBX;
-        double r = 0.0, w = 0.0, s = 0.0, fx = 0.0, fy = 0.0;
-        if (i <= g.nx + kOnx && j <= g.ny + kOnx) {
-          const size_t q = g.at(i, j);
-          r = pr.res[q];
-          w = op.W[q];
-          s = so[q];
-          fx = op.FX[q];
-          fy = op.FY[q];
-        }
-        b_s[e] = w * r + bq * s;
-        b_FX[e] = fx;
-        b_FY[e] = fy;
-      }
-      __syncthreads();
-      double v[2] = {0.0, 0.0};
-      for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
-        const int c = e % kTX, rr = e / kTX;
-        const int i = i0 + c, j = j0 + rr;
-        if (i > g.nx || j > g.ny) continue;
-        const int k = (rr + 1) * kBX + c + 1;
-        const double sc = b_s[k];
-        const double a = op.ax[i + 1] * op.bx[j + 1] * (b_FX[k + 1] * (b_s[k + 1] - sc) + b_FX[k] * (b_s[k - 1] - sc)) +
-                         op.by[j + 1] * (b_FY[k + kBX] * (b_s[k + kBX] - sc) + b_FY[k] * (b_s[k - kBX] - sc));
-        store_cyclic(sn, g, i, j, sc);
-        pr.As[g.at(i, j)] = a;
-        const double wd = pr.weighted ? 1.0 / (op.ax[i + 1] * op.by[j + 1]) : 1.0;
-        v[0] += (wd * sc) * a;
-        v[1] = fmax(v[1], fabs(sc));
-      }
-      double out[2];
-      block_reduce<2, 1, kBatchThreads>(v, out);
-      if (threadIdx.x == 0) {
-        P.part[(size_t)task * 4] = out[0];
-        P.part[(size_t)task * 4 + 1] = out[1];
-      }
-    }
-    if (!reduce_barrier(P, epoch, kSweepA, p0, p1)) return;
-    if (!__ldcg(P.any_active)) break;
-    // ---- sweep B: sol += alpha s, res -= alpha As ------------------------------------------
-    for (int task = t_lo + blockIdx.x; task < t_hi; task += gridDim.x) {
-      const int p = task_problem(P, task, p0, p1);
-      if (__ldcg(&P.state[p].phase) != 2) continue;
-      const BatchProblem& pr = P.probs[p];
-      const Geo g = pr.g;
-      const int n = __ldcg(&P.state[p].n);
-      const double alpha = __ldcg(&P.state[p].alpha);
-      const double* __restrict__ sn = pr.s[n & 1];
-      const int lt = task - pr.tile0;
-      const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
-      double v[2] = {0.0, 0.0};
-#pragma unroll 4
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
       for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
         const int i = i0 + e % kTX, j = j0 + e / kTX;
         if (i > g.nx || j > g.ny) continue;
         const size_t q = g.at(i, j);
-        const double w = pr.op.W[q];
-        const double r = pr.res[q] - alpha * pr.As[q];
-        pr.sol[q] = pr.sol[q] + alpha * sn[q];
+        const double f = pr.forc[fidx(g.nx, i, j)];
+        const double r = f - apply_point(pr.op, g, pr.sol, i, j);
         store_cyclic(pr.res, g, i, j, r);
+        const double w = pr.op.W[q];
+        const double zr = w * r;
         const double wd = pr.weighted ? 1.0 / (pr.op.ax[i + 1] * pr.op.by[j + 1]) : 1.0;
-        v[0] += (wd * w * r) * r;
-        if (w != 0.0) v[1] += r * r;
+        v[0] += (wd * zr) * r;
+        if (w != 0.0) {
+          v[1] += f * f;
+          v[2] += r * r;
+        }
+        v[3] = fmax(v[3], fabs(zr));
       }
-      double out[2];
-      block_reduce<2, -1, kBatchThreads>(v, out);
-      if (threadIdx.x == 0) {
-        P.part[(size_t)task * 4] = out[0];
-        P.part[(size_t)task * 4 + 1] = out[1];
+      double out[4];
+      block_reduce<4, 3, kBatchThreads>(v, out);
+      if (threadIdx.x == 0)
+        for (int c = 0; c < 4; c++) P.part[(size_t)(pr.tile0 + lt) * 4 + c] = out[c];
+      tile_finished(P, p, kInit, &s_flag);
+    }
+  }
+  if (!barrier_rebuild(P, epoch, 1, P.stall_extra, s_act_prob, s_act_off, &s_actn)) return;
+
+  for (;;) {
+    if (s_actn == 0) break;
+    // ---- sweep A: s_new = Z res + bq s_old on tile + halo, As = A s_new ---------------
+    {
+      const int m = s_actn;
+      const int* off = list_off();
+      const int* prb = list_prob();
+      const int ntot = off[m];
+      for (int task = blockIdx.x; task < ntot; task += gridDim.x) {
+        const int k = act_find(off, m, task);
+        const int p = prb[k];
+        const BatchProblem& pr = P.probs[p];
+        const Geo g = pr.g;
+        const OpDev<double> op = pr.op;
+        const int n = __ldcg(&P.state[p].n);
+        const double bq = __ldcg(&P.state[p].bq);
+        const double* __restrict__ so = pr.s[(n + 1) & 1];
+        double* __restrict__ sn = pr.s[n & 1];
+        const int lt = task - off[k];
+        const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
+        __syncthreads();  // shared boxes of the previous task are free
+        // four box points per thread in flight (the loads do not depend on the shared stores)
+#pragma unroll 4
+        for (int e = threadIdx.x; e < kBoxN; e += kBatchThreads) {
+          const int i = i0 - 1 + e % kBX, j = j0 - 1 + e / kBX;
+          double r = 0.0, w = 0.0, s = 0.0, fx = 0.0, fy = 0.0;
+          if (i <= g.nx + kOnx && j <= g.ny + kOnx) {
+            const size_t q = g.at(i, j);
+            r = pr.res[q];
+            w = op.W[q];
+            s = so[q];
+            fx = op.FX[q];
+            fy = op.FY[q];
+          }
+          b_s[e] = w * r + bq * s;
+          b_FX[e] = fx;
+          b_FY[e] = fy;
+        }
+        __syncthreads();
+        double v[2] = {0.0, 0.0};
+        for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
+          const int c = e % kTX, rr = e / kTX;
+          const int i = i0 + c, j = j0 + rr;
+          if (i > g.nx || j > g.ny) continue;
+          const int kk = (rr + 1) * kBX + c + 1;
+          const double sc = b_s[kk];
+          const double a =
+              op.ax[i + 1] * op.bx[j + 1] * (b_FX[kk + 1] * (b_s[kk + 1] - sc) + b_FX[kk] * (b_s[kk - 1] - sc)) +
+              op.by[j + 1] * (b_FY[kk + kBX] * (b_s[kk + kBX] - sc) + b_FY[kk] * (b_s[kk - kBX] - sc));
+          store_cyclic(sn, g, i, j, sc);
+          pr.As[g.at(i, j)] = a;
+          const double wd = pr.weighted ? 1.0 / (op.ax[i + 1] * op.by[j + 1]) : 1.0;
+          v[0] += (wd * sc) * a;
+          v[1] = fmax(v[1], fabs(sc));
+        }
+        double out[2];
+        block_reduce<2, 1, kBatchThreads>(v, out);
+        if (threadIdx.x == 0) {
+          P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
+          P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
+        }
+        tile_finished(P, p, kSweepA, &s_flag);
       }
     }
-    if (!reduce_barrier(P, epoch, kSweepB, p0, p1)) return;
+    if (!barrier_rebuild(P, epoch, 2, 0u, s_act_prob, s_act_off, &s_actn)) return;
+    if (s_actn == 0) break;
+    // ---- sweep B: sol += alpha s, res -= alpha As ------------------------------------------
+    {
+      const int m = s_actn;
+      const int* off = list_off();
+      const int* prb = list_prob();
+      const int ntot = off[m];
+      for (int task = blockIdx.x; task < ntot; task += gridDim.x) {
+        const int k = act_find(off, m, task);
+        const int p = prb[k];
+        const BatchProblem& pr = P.probs[p];
+        const Geo g = pr.g;
+        const int n = __ldcg(&P.state[p].n);
+        const double alpha = __ldcg(&P.state[p].alpha);
+        const double* __restrict__ sn = pr.s[n & 1];
+        const int lt = task - off[k];
+        const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
+        double v[2] = {0.0, 0.0};
+#pragma unroll 4
+        for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
+          const int i = i0 + e % kTX, j = j0 + e / kTX;
+          if (i > g.nx || j > g.ny) continue;
+          const size_t q = g.at(i, j);
+          const double w = pr.op.W[q];
+          const double r = pr.res[q] - alpha * pr.As[q];
+          pr.sol[q] = pr.sol[q] + alpha * sn[q];
+          store_cyclic(pr.res, g, i, j, r);
+          const double wd = pr.weighted ? 1.0 / (pr.op.ax[i + 1] * pr.op.by[j + 1]) : 1.0;
+          v[0] += (wd * w * r) * r;
+          if (w != 0.0) v[1] += r * r;
+        }
+        double out[2];
+        block_reduce<2, -1, kBatchThreads>(v, out);
+        if (threadIdx.x == 0) {
+          P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
+          P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
+        }
+        tile_finished(P, p, kSweepB, &s_flag);
+      }
+    }
+    if (!barrier_rebuild(P, epoch, 1, 0u, s_act_prob, s_act_off, &s_actn)) return;
   }
-  }  // groups
 }
 
 const void* cg_batch_kernel_ptr() { return (const void*)cg_batch_kernel; }

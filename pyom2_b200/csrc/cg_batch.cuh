@@ -37,20 +37,25 @@ struct BatchState {
 };
 static_assert(sizeof(BatchState) == 88, "BatchState is moved as 11 words");
 
+// Most problems of one launch (their active list is kept in shared memory;
+// larger batches run in several launches).
+constexpr int kBatchActMax = 1024;
+
 struct BatchParams {
   const BatchProblem* probs;
   BatchState* state;     // zero on entry
   int nprob;
   int ntasks;            // total tiles of all problems
-  // problems are solved in ngroup groups, one after another, each small enough
-  // for its fields to stay in L2: group g holds problems group[g] ..
-  // group[g+1]-1 (problems and their tiles are stored group by group)
-  int ngroup;
-  const int* group;      // ngroup + 1 problem offsets
   double* part;          // per task, 4 partials
+  int* done;             // per problem, tiles finished in the current sweep (zero on entry)
+  // the problems taking part in the next sweep, rebuilt at every grid barrier:
+  // act_prob[0 .. act_n-1], their tiles at act_off[k] .. act_off[k+1]-1 of the
+  // sweep's task range (on entry: every problem, for the initial sweep)
+  int* act_n;
+  int* act_prob;         // nprob
+  int* act_off;          // nprob + 1
   SyncCtl* ctl;
-  unsigned long long* gen;  // release flag of the reducing block
-  int* any_active;
+  unsigned long long* gen;  // release flag of the block that rebuilt the list
   unsigned long long timeout_ns;
   unsigned stall_extra;  // test hook: the first barrier awaits this many blocks more than launched
 };

@@ -80,14 +80,6 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 __device__ __forceinline__ unsigned res_tag(const CGResParams& P, unsigned ep) {
   return (P.tag_gen << 20) | (ep & 0xFFFFFu);
 }
-__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -1118,55 +1110,44 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res32_kernel(const __grid_c
   if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(s_tmem, 512);
 }
 
-// Many solves in one launch: the blocks form groups (group k: blocks
-// group_base[k] .. group_base[k+1]-1) that take the solves from one queue,
-// longest first: the group's first block draws the next job with an atomic
-// and posts it as the group's s-th job (assign[k * (njobs + 1) + s], written
-// once), the others read it there.  Every block of a group runs the same
-// sequence of solves, each block in its own time: a solve has its own
-// operator, vectors, reduction slots, exchange records, error flag and
-// result, so the groups never wait on one another and a block may start its
-// group's next solve while others still finish the last one.
+// Many solves in one launch (ResMultiParams): block b runs list entries
+// list_off[b] .. list_off[b+1]-1, each a piece of one job; before a job the
+// block counts itself in at the job's join counter and waits (bounded) until
+// the whole gang is there, so the solve's own waits start with every piece
+// present.  A job has its own operator, vectors, slots, records, error flag
+// and result, so different jobs never wait on one another.
 template <int P>
 __global__ void __launch_bounds__(kResThreads, 1) cg_res_multi_kernel(const __grid_constant__ ResMultiParams M) {
   extern __shared__ __align__(16) double sm[];
   __shared__ uint32_t s_tmem;
   __shared__ ResCtl C;
   __shared__ double wred[kResThreads / 32][kResSlotWords];
-  __shared__ int s_job;
+  __shared__ int s_ok;
   if ((threadIdx.x >> 5) == 0) {
     tc::tmem_alloc(&s_tmem, 512);
     tc::tmem_relinquish();
   }
-  int grp = 0;
-  while (grp + 1 < M.ngroup && M.group_base[grp + 1] <= (int)blockIdx.x) grp++;
-  const int bid = (int)blockIdx.x - M.group_base[grp];
-  unsigned* post = M.assign + (size_t)grp * (M.njobs + 1);
-  for (int seq = 0; seq <= M.njobs; seq++) {
+  for (int e = M.list_off[blockIdx.x]; e < M.list_off[blockIdx.x + 1]; e++) {
+    const int2 ent = M.list[e];
+    const CGResParams& Pm = M.jobs[ent.x];
     if (threadIdx.x == 0) {
-      int j;
-      if (bid == 0) {
-        const unsigned q = atomicAdd(M.queue, 1u);
-        j = q < (unsigned)M.njobs ? (int)q : -1;
-        st_relaxed_u32(post + seq, j < 0 ? kResNoJob : (unsigned)j);
-      } else {
-        unsigned w = kResUnposted;
-        const unsigned long long t0 = globaltimer_ns();
-        for (unsigned spin = 1; (w = ld_relaxed_u32(post + seq)) == kResUnposted; spin++)
-          if ((spin & 63u) == 0u && globaltimer_ns() - t0 > M.timeout_ns) {
-            atomicExch(M.error, PYOMGPU_TIMEOUT);
-            break;
-          }
-        j = (w == kResUnposted || w == kResNoJob) ? -1 : (int)w;
-      }
-      s_job = j;
+      const int nb = Pm.npx * Pm.npy;
+      atomicAdd(M.join + ent.x, 1);
+      int ok = 1;
+      const unsigned long long t0 = globaltimer_ns();
+      for (unsigned spin = 1; ld_relaxed_i32(M.join + ent.x) < nb; spin++)
+        if ((spin & 63u) == 0u && (ld_relaxed_i32(M.error) != 0 || globaltimer_ns() - t0 > M.gang_timeout_ns)) {
+          atomicExch(M.error, PYOMGPU_TIMEOUT);
+          ok = 0;
+          break;
+        }
+      s_ok = ok;
     }
     __syncthreads();
-    const int j = s_job;
+    const bool ok = s_ok != 0;
     __syncthreads();
-    if (j < 0) break;
-    const CGResParams& Pm = M.jobs[j];
-    if (bid < Pm.npx * Pm.npy) res_solve<double, P, false>(Pm, bid, sm, &s_tmem, C, wred);
+    if (!ok) break;
+    res_solve<double, P, false>(Pm, ent.y, sm, &s_tmem, C, wred);
   }
   tc::fence_before_sync();
   __syncthreads();

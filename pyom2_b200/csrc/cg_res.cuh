@@ -57,21 +57,20 @@ struct CGResParams {
   float* res32;
 };
 
-// Many resident solves in one launch (cg_res_multi_kernel): equal groups of
-// blocks taking the solves from one queue.  Every job has its own CGResParams
-// with npx * npy at most the group size, its own slots, exchange records
-// (tagged), error flag and result.
-constexpr unsigned kResUnposted = 0xFFFFFFFFu;  // assign word not yet written (the host fills all-ones)
-constexpr unsigned kResNoJob = 0xFFFFFFFEu;     // the queue is empty: the group is done
+// Many resident solves in one launch (cg_res_multi_kernel), scheduled on the
+// host: every block runs its own list of (job, piece) entries in order; the
+// blocks of one job (its gang) meet at the job's join counter before they
+// start it.  Every job has its own CGResParams, slots, exchange records
+// (tagged), error flag and result.  The lists are ordered by planned start
+// time, one total order for all blocks, so no set of gangs can wait on one
+// another in a cycle.
 struct ResMultiParams {
-  const CGResParams* jobs;  // device array, longest first
-  int njobs;
-  int ngroup;
-  const int* group_base;    // ngroup + 1 block offsets
-  unsigned* queue;          // next job to hand out (zero on entry)
-  unsigned* assign;         // ngroup x (njobs + 1): job of each group's s-th draw (all-ones on entry)
-  int* error;               // PYOMGPU_TIMEOUT when a block gave up waiting for its group's draw
-  unsigned long long timeout_ns;
+  const CGResParams* jobs;
+  const int* list_off;   // gridDim.x + 1 offsets into list
+  const int2* list;      // (job, piece index within the job)
+  int* join;             // per job, blocks arrived (zero on entry)
+  int* error;            // PYOMGPU_TIMEOUT when a gang did not assemble within gang_timeout_ns
+  unsigned long long gang_timeout_ns;
 };
 
 // Phases of the trace (worker warp 1 lane 0 unless noted "ctl": warp 0 lane 0):

@@ -131,10 +131,10 @@ struct pyomgpu_ctx {
     size_t cap_tasks = 0;
     double* d_rr = nullptr;  // 2 per solve: true residual, forcing norm
     double* h_rr = nullptr;  // pinned
-    int* d_group = nullptr;  // cap_probs + 1 problem offsets of the L2-sized groups
-    int* h_group = nullptr;  // pinned
+    int* d_act = nullptr;    // act_n, act_prob (cap_probs), act_off (cap_probs + 1), done (cap_probs)
+    int* h_act = nullptr;    // pinned: the initial act_n, act_prob, act_off
     size_t l2_bytes = 0;     // L2 size of the device
-    unsigned long long* sync = nullptr;  // SyncCtl, gen, any_active
+    unsigned long long* sync = nullptr;  // SyncCtl, gen
   } batch;
 
   // many resident solves in one launch (cg_res_multi_kernel), owned by the
@@ -163,12 +163,12 @@ struct pyomgpu_ctx {
     if (batch.h_probs) cudaFreeHost(batch.h_probs);
     if (batch.h_state) cudaFreeHost(batch.h_state);
     if (batch.h_rr) cudaFreeHost(batch.h_rr);
-    if (batch.h_group) cudaFreeHost(batch.h_group);
+    if (batch.h_act) cudaFreeHost(batch.h_act);
     for (void* p : {(void*)rmulti.d_jobs, (void*)rmulti.d_idx, (void*)rmulti.d_out, (void*)rmulti.d_ctl})
       if (p) cudaFree(p);
     for (void* p : {(void*)rmulti.h_jobs, (void*)rmulti.h_idx, (void*)rmulti.h_out, (void*)rmulti.h_ctl})
       if (p) cudaFreeHost(p);
-    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace, (void*)batch.d_group, (void*)resd.hx32,
+    for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace, (void*)batch.d_act, (void*)resd.hx32,
                     (void*)resd.slots32, (void*)resd.res32})
       if (p) cudaFree(p);
     void* ptrs[] = {dxt, dxu, dyt, dyu, cost, cosu, hur, hvr, hu, hv, mT, mU, mV, sf.FX, sf.FY, sf.W, sf.ax, sf.bx,
