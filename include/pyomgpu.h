@@ -355,11 +355,10 @@ int32_t pyomgpu_congrad_streamfunction_noalloc(const pyomgpu_grid* grid, const i
  * kernel_launches describe the whole call.  The work buffers live in ctx[0]
  * and grow to the largest batch it has run.  Returns the largest status.
  * Engine (pyomgpu_set_batch_kernel on ctx[0]): where every grid fits on chip,
- * groups of SMs run on-chip-resident solves side by side (the SMs split into
- * 1, 2, 4, 8 or 16 groups; each grid in the smallest groups it fits, longest
- * solves first), else the work-queue kernel streams all solves through HBM
- * in lockstep.  The rtol stop is relative to ||forc||, or to the initial
- * residual for a zero forcing. */
+ * on-chip-resident solves run side by side in one launch, each on its own set
+ * of SMs, placed by list scheduling on the host; else the work-queue kernel
+ * streams all solves through HBM in lockstep.  The rtol stop is relative to
+ * ||forc||, or to the initial residual for a zero forcing. */
 int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t count, const double* const* forc,
                                              double* const* sol, double congr_epsilon, int32_t congr_max_iterations,
                                              double rtol, pyomgpu_solve_info* info, pyomgpu_stream stream);

@@ -830,6 +830,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   if (int rc = rmulti_reserve(o, count)) return rc;
   *used = true;
   auto& B = o->batch;
+  CK(cudaMemsetAsync(R.d_ctl, 0, sizeof(SyncCtl) * count, st));  // every solve's error flag
   // list scheduling: gangs on the blocks free earliest
   std::vector<int> order((size_t)count);
   for (int k = 0; k < count; ++k) order[k] = k;
