@@ -211,10 +211,11 @@ def c2_batch(steps, warmup, count=64):
     """Config 2: 64 closed basins (128-1024 x 128-768, 10-40 % land, 0-12
     islands), each solved to the FP64 relative residual RTOL from zero, three
     ways: congrad_streamfunction_batch on groups of SMs running on-chip
-    solves side by side (the automatic engine where every grid fits), the
-    same call on the work-queue kernel (all 64 grids streamed through HBM in
-    lockstep), and 64 sequential solve_rtol calls (each grid alone on all
-    SMs).  Device time by CUDA events."""
+    solves side by side (the automatic engine where every grid fits; its
+    schedule uses the iteration counts of the warm-up call), the same call on
+    the work-queue kernel (all 64 grids streamed through HBM in lockstep), and
+    64 sequential solve_rtol calls (each grid alone on all SMs).  Device time
+    by CUDA events."""
     import warnings
 
     import torch
@@ -262,9 +263,9 @@ def c2_batch(steps, warmup, count=64):
             "batch_launches": int(infos[0]["kernel_launches"]) - len(ws) * 5,
             "iterations_max": max(i["iterations"] for i in infos),
             "iterations_sum": int(sum(i["iterations"] for i in infos)),
-            "note": "batch: resident solves side by side on groups of SMs (one launch per group size); queue: "
-                    "one work-queue launch streaming all 64 grids; sequential: one resident launch per grid; "
-                    "FP64 Jacobi-PCG, same stop"}
+            "note": "batch: resident solves side by side in one launch, each on its own set of SMs, placed by "
+                    "list scheduling (iteration estimates from the warm-up call); queue: one work-queue launch "
+                    "streaming all 64 grids; sequential: one resident launch per grid; FP64 Jacobi-PCG, same stop"}
 
 
 def c3_learned(steps, warmup):

@@ -783,9 +783,10 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
 // with the fewest pieces at 16 points per thread: the least block-time per
 // iteration) and is placed by list scheduling on the host, largest gangs
 // first, then longest: on the pieces' count of blocks that become free
-// earliest under the estimated durations (iterations ~ the square root of the
-// point count, times the cut's iteration estimate plus ~6 us of reduction
-// latency); each block runs its entries in order of planned start.
+// earliest under the estimated durations (iterations: the grid's count in the
+// previous resident batch, else ~2 x the square root of the point count; times
+// the cut's iteration estimate plus ~6 us of reduction latency); each block
+// runs its entries in order of planned start.
 // *used = false (nothing run) when a grid does not fit on chip or the
 // resident kernel is unavailable; the caller then runs the work-queue kernel.
 int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol,
@@ -819,7 +820,18 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
       ResCut cut;
       if (res_cut(c->nx, c->ny, share, R.smem_cap, 16, false, cut)) cuts[k] = cut;
     }
-  for (int k = 0; k < count; ++k) est[k] = std::sqrt((double)v[k].c->nx * v[k].c->ny) * (cuts[k].cost + 6000.0);
+  // estimated duration: iterations (this grid's count in the previous resident batch at the
+  // same occurrence, else ~2 sqrt(points)) x the cut's iteration estimate + ~6 us of reductions
+  std::vector<int> occ((size_t)count, 0);
+  for (int k = 0; k < count; ++k)
+    for (int q = 0; q < k; ++q) occ[k] += v[q].c == v[k].c;
+  for (int k = 0; k < count; ++k) {
+    const pyomgpu_ctx* c = v[k].c;
+    const double its = occ[k] < (int)c->batch_its.size() && c->batch_its[occ[k]] > 0
+                           ? (double)c->batch_its[occ[k]]
+                           : 2.0 * std::sqrt((double)c->nx * c->ny);
+    est[k] = its * (cuts[k].cost + 6000.0);
+  }
   // workspace per solve (batch_job_words): padded sol and res, 4 record words per
   // position, the slots; the caller has reserved it before staging its inputs
   // behind it, so the pool is never reallocated here
@@ -961,6 +973,9 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   for (int k = 0; k < count; ++k) {
     const CGResult& r = R.h_out[k];
     worst = std::max(worst, r.status);
+    auto& hist = v[k].c->batch_its;
+    if ((int)hist.size() <= occ[k]) hist.resize((size_t)occ[k] + 1, 0);
+    hist[occ[k]] = r.iterations;
     if (!infos) continue;
     pyomgpu_solve_info& I = infos[k];
     I.iterations = r.iterations;

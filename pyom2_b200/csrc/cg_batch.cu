@@ -183,16 +183,19 @@ __device__ void reduce_problem(const BatchParams& P, int p, int kind) {
   }
 }
 
-// After a tile of problem p: counts it (thread 0) and, in the block that
-// finished the problem's last tile of this sweep, reduces the problem.
-__device__ __forceinline__ void tile_finished(const BatchParams& P, int p, int kind, int* s_flag) {
-  if (threadIdx.x == 0) {
-    __threadfence();  // this tile's partials before its arrival
-    const BatchProblem& pr = P.probs[p];
-    *s_flag = atom_add_acqrel_i32(&P.done[p], 1) + 1 == pr.ntx * pr.nty;
+// After a tile of problem p (its partials stored by thread 0): warp 0 counts
+// it -- the acq_rel arrival also releases those partials -- and, in the block
+// that finished the problem's last tile of this sweep, reduces the problem.
+// The other warps go on with the block's next tile.
+__device__ __forceinline__ void tile_finished(const BatchParams& P, int p, int kind) {
+  if (threadIdx.x < 32) {
+    int last = 0;
+    if (threadIdx.x == 0) {
+      const BatchProblem& pr = P.probs[p];
+      last = atom_add_acqrel_i32(&P.done[p], 1) + 1 == pr.ntx * pr.nty;
+    }
+    if (__shfl_sync(0xffffffffu, last, 0)) reduce_problem(P, p, kind);
   }
-  __syncthreads();
-  if (*s_flag && threadIdx.x < 32) reduce_problem(P, p, kind);
 }
 
 // Grid barrier after a sweep; the last block to arrive rebuilds the list of
@@ -290,7 +293,7 @@ __device__ __forceinline__ int act_find(const int* off, int m, int task) {
 __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchParams P) {
   __shared__ double b_s[kBoxN], b_FX[kBoxN], b_FY[kBoxN];
   __shared__ int s_act_prob[kBatchActMax], s_act_off[kBatchActMax + 1];
-  __shared__ int s_actn, s_flag;
+  __shared__ int s_actn;
   unsigned long long epoch = 0;
   // the active list of the initial sweep (every problem, nprob <= kBatchActMax), written by the host
   {
@@ -340,7 +343,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
       block_reduce<4, 3, kBatchThreads>(v, out);
       if (threadIdx.x == 0)
         for (int c = 0; c < 4; c++) P.part[(size_t)(pr.tile0 + lt) * 4 + c] = out[c];
-      tile_finished(P, p, kInit, &s_flag);
+      tile_finished(P, p, kInit);
     }
   }
   if (!barrier_rebuild(P, epoch, 1, P.stall_extra, s_act_prob, s_act_off, &s_actn)) return;
@@ -406,7 +409,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
           P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
           P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
         }
-        tile_finished(P, p, kSweepA, &s_flag);
+        tile_finished(P, p, kSweepA);
       }
     }
     if (!barrier_rebuild(P, epoch, 2, 0u, s_act_prob, s_act_off, &s_actn)) return;
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
           P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
           P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
         }
-        tile_finished(P, p, kSweepB, &s_flag);
+        tile_finished(P, p, kSweepB);
       }
     }
     if (!barrier_rebuild(P, epoch, 1, 0u, s_act_prob, s_act_off, &s_actn)) return;

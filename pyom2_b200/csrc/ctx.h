@@ -152,6 +152,9 @@ struct pyomgpu_ctx {
     size_t smem_cap = 0;            // dynamic shared memory reserved for the kernel (0: not yet)
   } rmulti;
   int batch_kernel = 0;  // 0 automatic, 1 work-queue kernel, 2 resident groups
+  // iterations of this context's solves in the last resident batch, by
+  // occurrence in that batch: the schedule's estimates for the next one
+  std::vector<int> batch_its;
 
   ~pyomgpu_ctx() {
     for (void* p : fast.owned)
