@@ -212,7 +212,7 @@ def c2_batch(steps, warmup, count=64):
     islands), each solved to the FP64 relative residual RTOL from zero, three
     ways: congrad_streamfunction_batch on groups of SMs running on-chip
     solves side by side (the automatic engine where every grid fits; its
-    schedule uses the iteration counts of the warm-up call), the same call on
+    schedule uses the solve durations measured in the warm-up call), the same call on
     the work-queue kernel (all 64 grids streamed through HBM in lockstep), and
     64 sequential solve_rtol calls (each grid alone on all SMs).  Device time
     by CUDA events."""
@@ -264,7 +264,7 @@ def c2_batch(steps, warmup, count=64):
             "iterations_max": max(i["iterations"] for i in infos),
             "iterations_sum": int(sum(i["iterations"] for i in infos)),
             "note": "batch: resident solves side by side in one launch, each on its own set of SMs, placed by "
-                    "list scheduling (iteration estimates from the warm-up call); queue: one work-queue launch "
+                    "list scheduling (durations measured in the warm-up call); queue: one work-queue launch "
                     "streaming all 64 grids; sequential: one resident launch per grid; FP64 Jacobi-PCG, same stop"}
 
 

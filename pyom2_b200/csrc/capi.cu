@@ -755,24 +755,27 @@ inline size_t rmulti_idx_words(int count) {
 int rmulti_reserve(pyomgpu_ctx* o, int count) {
   auto& R = o->rmulti;
   if (count <= R.cap) return 0;
-  for (void* p : {(void*)R.d_jobs, (void*)R.d_idx, (void*)R.d_out, (void*)R.d_ctl})
+  for (void* p : {(void*)R.d_jobs, (void*)R.d_idx, (void*)R.d_out, (void*)R.d_ctl, (void*)R.d_times})
     if (p) cudaFree(p);
-  for (void* p : {(void*)R.h_jobs, (void*)R.h_idx, (void*)R.h_out, (void*)R.h_ctl})
+  for (void* p : {(void*)R.h_jobs, (void*)R.h_idx, (void*)R.h_out, (void*)R.h_ctl, (void*)R.h_times})
     if (p) cudaFreeHost(p);
   R.d_jobs = nullptr;
   R.h_jobs = nullptr;
   R.d_idx = R.h_idx = nullptr;
   R.d_out = R.h_out = nullptr;
   R.d_ctl = R.h_ctl = nullptr;
+  R.d_times = R.h_times = nullptr;
   R.cap = 0;
   if (int rc = dalloc(&R.d_jobs, (size_t)count)) return rc;
   if (int rc = dalloc(&R.d_idx, rmulti_idx_words(count))) return rc;
   if (int rc = dalloc(&R.d_out, (size_t)count)) return rc;
   if (int rc = dalloc(&R.d_ctl, (size_t)count)) return rc;
+  if (int rc = dalloc(&R.d_times, (size_t)2 * count)) return rc;
   if (cudaMallocHost((void**)&R.h_jobs, sizeof(CGResParams) * count) != cudaSuccess ||
       cudaMallocHost((void**)&R.h_idx, sizeof(int) * rmulti_idx_words(count)) != cudaSuccess ||
       cudaMallocHost((void**)&R.h_out, sizeof(CGResult) * count) != cudaSuccess ||
-      cudaMallocHost((void**)&R.h_ctl, sizeof(SyncCtl) * count) != cudaSuccess)
+      cudaMallocHost((void**)&R.h_ctl, sizeof(SyncCtl) * count) != cudaSuccess ||
+      cudaMallocHost((void**)&R.h_times, sizeof(unsigned long long) * 2 * count) != cudaSuccess)
     return fail(PYOMGPU_ENOMEM, "cudaMallocHost");
   R.cap = count;
   return 0;
@@ -783,10 +786,11 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
 // with the fewest pieces at 16 points per thread: the least block-time per
 // iteration) and is placed by list scheduling on the host, largest gangs
 // first, then longest: on the pieces' count of blocks that become free
-// earliest under the estimated durations (iterations: the grid's count in the
-// previous resident batch, else ~2 x the square root of the point count; times
-// the cut's iteration estimate plus ~6 us of reduction latency); each block
-// runs its entries in order of planned start.
+// earliest under the estimated durations (the grid's device time in the
+// previous resident batch, measured with %globaltimer around its solve; else
+// ~2 x the square root of the point count iterations times the cut's
+// iteration estimate plus ~6 us of reduction latency); each block runs its
+// entries in order of planned start.
 // *used = false (nothing run) when a grid does not fit on chip or the
 // resident kernel is unavailable; the caller then runs the work-queue kernel.
 int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol,
@@ -820,17 +824,17 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
       ResCut cut;
       if (res_cut(c->nx, c->ny, share, R.smem_cap, 16, false, cut)) cuts[k] = cut;
     }
-  // estimated duration: iterations (this grid's count in the previous resident batch at the
-  // same occurrence, else ~2 sqrt(points)) x the cut's iteration estimate + ~6 us of reductions
+  // estimated duration (ns): this grid's device time in the previous resident batch at the
+  // same occurrence, else ~2 sqrt(points) iterations x (the cut's iteration estimate + ~6 us
+  // of reductions)
   std::vector<int> occ((size_t)count, 0);
   for (int k = 0; k < count; ++k)
     for (int q = 0; q < k; ++q) occ[k] += v[q].c == v[k].c;
   for (int k = 0; k < count; ++k) {
     const pyomgpu_ctx* c = v[k].c;
-    const double its = occ[k] < (int)c->batch_its.size() && c->batch_its[occ[k]] > 0
-                           ? (double)c->batch_its[occ[k]]
-                           : 2.0 * std::sqrt((double)c->nx * c->ny);
-    est[k] = its * (cuts[k].cost + 6000.0);
+    est[k] = occ[k] < (int)c->batch_ns.size() && c->batch_ns[occ[k]] > 0.0
+                 ? c->batch_ns[occ[k]]
+                 : 2.0 * std::sqrt((double)c->nx * c->ny) * (cuts[k].cost + 6000.0);
   }
   // workspace per solve (batch_job_words): padded sol and res, 4 record words per
   // position, the slots; the caller has reserved it before staging its inputs
@@ -941,6 +945,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   M.list_off = R.d_idx;
   M.list = reinterpret_cast<const int2*>(R.d_idx + lst0);
   M.join = d_err + 1;
+  M.times = R.d_times;
   M.error = d_err;
   // a block may wait for its gang while other pieces finish their previous solves
   M.gang_timeout_ns = (unsigned long long)(std::max(120.0, 64.0 * o->timeout_s) * 1e9);
@@ -951,6 +956,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   CK(cudaMemcpyAsync(R.h_out, R.d_out, sizeof(CGResult) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(R.h_ctl, R.d_ctl, sizeof(SyncCtl) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(R.h_idx, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(R.h_times, R.d_times, sizeof(unsigned long long) * 2 * count, cudaMemcpyDeviceToHost, st));
   for (int r = 0; r < count; ++r) {
     const int k = job_of_rank[r];
     const CGResParams& J = R.h_jobs[r];
@@ -973,9 +979,10 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   for (int k = 0; k < count; ++k) {
     const CGResult& r = R.h_out[k];
     worst = std::max(worst, r.status);
-    auto& hist = v[k].c->batch_its;
-    if ((int)hist.size() <= occ[k]) hist.resize((size_t)occ[k] + 1, 0);
-    hist[occ[k]] = r.iterations;
+    auto& hist = v[k].c->batch_ns;
+    if ((int)hist.size() <= occ[k]) hist.resize((size_t)occ[k] + 1, 0.0);
+    const unsigned long long t0 = R.h_times[2 * rank[k]], t1 = R.h_times[2 * rank[k] + 1];
+    hist[occ[k]] = t1 > t0 ? (double)(t1 - t0) : 0.0;
     if (!infos) continue;
     pyomgpu_solve_info& I = infos[k];
     I.iterations = r.iterations;

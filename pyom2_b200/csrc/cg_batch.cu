@@ -5,8 +5,9 @@
 // The tiles of the problems still running form one task list; every block
 // walks it with a static stride.  All problems advance in lockstep through
 // three kinds of sweep (init, A: direction + stencil, B: update) separated by
-// grid barriers.  The block that finishes a problem's last tile of a sweep
-// (a per-problem arrival counter) sums that problem's per-tile partials in a
+// grid barriers.  Every tile's arrival is counted per problem (a release
+// reduction); at the end of the sweep the block that processed a problem's
+// last task waits for the count, sums that problem's per-tile partials in a
 // fixed order and runs its stopping logic, so every problem ends with exactly
 // the iterations and status an individual solve would give; the last block
 // at the barrier rebuilds the list of problems still running and releases
@@ -129,6 +130,11 @@ __device__ void after_b(BatchState& st, const BatchProblem& pr, const double* v)
   start_iteration(st, pr, st.n + 1);
 }
 
+__device__ __forceinline__ int ld_acquire_i32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ int atom_add_acqrel_i32(int* p, int v) {
   int old;
   asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
@@ -183,19 +189,43 @@ __device__ void reduce_problem(const BatchParams& P, int p, int kind) {
   }
 }
 
-// After a tile of problem p (its partials stored by thread 0): warp 0 counts
-// it -- the acq_rel arrival also releases those partials -- and, in the block
-// that finished the problem's last tile of this sweep, reduces the problem.
-// The other warps go on with the block's next tile.
-__device__ __forceinline__ void tile_finished(const BatchParams& P, int p, int kind) {
-  if (threadIdx.x < 32) {
-    int last = 0;
-    if (threadIdx.x == 0) {
-      const BatchProblem& pr = P.probs[p];
-      last = atom_add_acqrel_i32(&P.done[p], 1) + 1 == pr.ntx * pr.nty;
+// After a tile of problem p (its partials stored by thread 0): thread 0
+// counts it with a release reduction (no return value, nothing to wait for),
+// which also releases those partials.
+__device__ __forceinline__ void tile_finished(const BatchParams& P, int p) {
+  if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(P.done + p) : "memory");
+}
+
+// End of a sweep: the block that processed a problem's last task reduces the
+// problem once all its tiles have arrived (acquire poll, bounded); the
+// block's warps take such problems in turn.  False on time-out.
+__device__ bool reduce_own(const BatchParams& P, int kind, const int* off, const int* prb, int m) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int mine = 0;  // designated problems seen so far (every warp scans the list the same way)
+  bool ok = true;
+  for (int k = 0; k < m; k++) {
+    if ((off[k + 1] - 1) % (int)gridDim.x != (int)blockIdx.x) continue;
+    if (mine++ % (kBatchThreads / 32) != warp) continue;
+    const int p = prb[k];
+    const BatchProblem& pr = P.probs[p];
+    const int nt = pr.ntx * pr.nty;
+    if (lane == 0) {
+      const unsigned long long t0 = globaltimer_ns();
+      int cnt;
+      unsigned spins = 0;
+      while ((cnt = ld_acquire_i32(P.done + p)) < nt)
+        if ((++spins & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
+          atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+          break;
+        }
+      ok = cnt >= nt;
     }
-    if (__shfl_sync(0xffffffffu, last, 0)) reduce_problem(P, p, kind);
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    __syncwarp();
+    if (!ok) break;
+    reduce_problem(P, p, kind);
   }
+  return ok;
 }
 
 // Grid barrier after a sweep; the last block to arrive rebuilds the list of
@@ -343,9 +373,10 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
       block_reduce<4, 3, kBatchThreads>(v, out);
       if (threadIdx.x == 0)
         for (int c = 0; c < 4; c++) P.part[(size_t)(pr.tile0 + lt) * 4 + c] = out[c];
-      tile_finished(P, p, kInit);
+      tile_finished(P, p);
     }
   }
+  if (!reduce_own(P, kInit, s_act_off, s_act_prob, s_actn)) return;
   if (!barrier_rebuild(P, epoch, 1, P.stall_extra, s_act_prob, s_act_off, &s_actn)) return;
 
   for (;;) {
@@ -409,9 +440,10 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
           P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
           P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
         }
-        tile_finished(P, p, kSweepA);
+        tile_finished(P, p);
       }
     }
+    if (!reduce_own(P, kSweepA, s_act_off, s_act_prob, s_actn)) return;
     if (!barrier_rebuild(P, epoch, 2, 0u, s_act_prob, s_act_off, &s_actn)) return;
     if (s_actn == 0) break;
     // ---- sweep B: sol += alpha s, res -= alpha As ------------------------------------------
@@ -450,9 +482,10 @@ __global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchP
           P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
           P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
         }
-        tile_finished(P, p, kSweepB);
+        tile_finished(P, p);
       }
     }
+    if (!reduce_own(P, kSweepB, s_act_off, s_act_prob, s_actn)) return;
     if (!barrier_rebuild(P, epoch, 1, 0u, s_act_prob, s_act_off, &s_actn)) return;
   }
 }

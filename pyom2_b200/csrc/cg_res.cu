@@ -1147,7 +1147,9 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_multi_kernel(const __gr
     const bool ok = s_ok != 0;
     __syncthreads();
     if (!ok) break;
+    if (ent.y == 0 && threadIdx.x == 0) M.times[2 * ent.x] = globaltimer_ns();
     res_solve<double, P, false>(Pm, ent.y, sm, &s_tmem, C, wred);
+    if (ent.y == 0 && threadIdx.x == 0) M.times[2 * ent.x + 1] = globaltimer_ns();
   }
   tc::fence_before_sync();
   __syncthreads();

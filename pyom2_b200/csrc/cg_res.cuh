@@ -69,6 +69,7 @@ struct ResMultiParams {
   const int* list_off;   // gridDim.x + 1 offsets into list
   const int2* list;      // (job, piece index within the job)
   int* join;             // per job, blocks arrived (zero on entry)
+  unsigned long long* times;  // per job: %globaltimer when its gang has assembled and when piece 0 ends
   int* error;            // PYOMGPU_TIMEOUT when a gang did not assemble within gang_timeout_ns
   unsigned long long gang_timeout_ns;
 };

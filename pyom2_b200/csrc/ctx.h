@@ -149,12 +149,14 @@ struct pyomgpu_ctx {
     CGResult* h_out = nullptr;      // pinned
     SyncCtl* d_ctl = nullptr;
     SyncCtl* h_ctl = nullptr;       // pinned
+    unsigned long long* d_times = nullptr;  // 2 per job: gang assembled, piece 0 done (%globaltimer)
+    unsigned long long* h_times = nullptr;  // pinned
     size_t smem_cap = 0;            // dynamic shared memory reserved for the kernel (0: not yet)
   } rmulti;
   int batch_kernel = 0;  // 0 automatic, 1 work-queue kernel, 2 resident groups
-  // iterations of this context's solves in the last resident batch, by
+  // device time (ns) of this context's solves in the last resident batch, by
   // occurrence in that batch: the schedule's estimates for the next one
-  std::vector<int> batch_its;
+  std::vector<double> batch_ns;
 
   ~pyomgpu_ctx() {
     for (void* p : fast.owned)
@@ -167,9 +169,11 @@ struct pyomgpu_ctx {
     if (batch.h_state) cudaFreeHost(batch.h_state);
     if (batch.h_rr) cudaFreeHost(batch.h_rr);
     if (batch.h_act) cudaFreeHost(batch.h_act);
-    for (void* p : {(void*)rmulti.d_jobs, (void*)rmulti.d_idx, (void*)rmulti.d_out, (void*)rmulti.d_ctl})
+    for (void* p : {(void*)rmulti.d_jobs, (void*)rmulti.d_idx, (void*)rmulti.d_out, (void*)rmulti.d_ctl,
+                    (void*)rmulti.d_times})
       if (p) cudaFree(p);
-    for (void* p : {(void*)rmulti.h_jobs, (void*)rmulti.h_idx, (void*)rmulti.h_out, (void*)rmulti.h_ctl})
+    for (void* p : {(void*)rmulti.h_jobs, (void*)rmulti.h_idx, (void*)rmulti.h_out, (void*)rmulti.h_ctl,
+                    (void*)rmulti.h_times})
       if (p) cudaFreeHost(p);
     for (void* p : {(void*)resd.hx, (void*)resd.slots, (void*)resd.trace, (void*)batch.d_act, (void*)resd.hx32,
                     (void*)resd.slots32, (void*)resd.res32})
