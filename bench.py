@@ -250,6 +250,12 @@ def c2_batch(steps, warmup, count=64):
 
     batch_ms, infos = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL,
                                                                  kernel="resident"))
+    from pyom2_b200.external import batch_schedule
+    t0, t1, nblk = batch_schedule(ems[0], len(ems))
+    span = float(t1.max())
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    sched = {"makespan_ms": span, "sm_utilisation": float((nblk * (t1 - t0)).sum() / (nsm * span)),
+             "solo_sum_ms": float((t1 - t0).sum()), "blocks_max": int(nblk.max()), "blocks_min": int(nblk.min())}
     queue_ms, qinfos = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL,
                                                                   kernel="queue"))
     seq_ms, seq = timed(lambda: [E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64)
@@ -260,7 +266,7 @@ def c2_batch(steps, warmup, count=64):
             "batch_max_rel_residual": max(i["rel_residual"] for i in infos),
             "queue_max_rel_residual": max(i["rel_residual"] for i in qinfos),
             "sequential_max_rel_residual": max(i["rel_residual"] for i in seq),
-            "batch_launches": int(infos[0]["kernel_launches"]) - len(ws) * 5,
+            "batch_launches": int(infos[0]["kernel_launches"]) - len(ws) * 5, "batch_schedule": sched,
             "iterations_max": max(i["iterations"] for i in infos),
             "iterations_sum": int(sum(i["iterations"] for i in infos)),
             "note": "batch: resident solves side by side in one launch, each on its own set of SMs, placed by "

@@ -368,6 +368,11 @@ int32_t pyomgpu_congrad_streamfunction_batch(pyomgpu_ctx* const* ctx, int32_t co
  * work-queue kernel, 2 resident groups (PYOMGPU_EINVAL from the batch call
  * when a grid does not fit).  No counterpart in the reference. */
 int32_t pyomgpu_set_batch_kernel(pyomgpu_ctx* ctx, int32_t kernel);
+/* Diagnostics of the last resident batch owned by ctx (ctx[0] of the call),
+ * per solve in call order: device start and end (ms after the earliest
+ * start, %globaltimer) and SMs used.  PYOMGPU_ESTATE when that batch had
+ * another count or none ran on the resident engine.  Any output may be NULL. */
+int32_t pyomgpu_batch_schedule(pyomgpu_ctx* ctx, int32_t count, double* start_ms, double* end_ms, int32_t* blocks);
 
 /* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
  * products.  psi is psi(:,:,taup1), in/out, host or device. */

@@ -975,6 +975,18 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, o->e0, o->e1));
   if (ms_out) *ms_out = ms;
+  {
+    unsigned long long t_min = ~0ull;
+    for (int k = 0; k < count; ++k) t_min = std::min(t_min, R.h_times[2 * rank[k]]);
+    o->sched_start.assign((size_t)count, 0.0);
+    o->sched_end.assign((size_t)count, 0.0);
+    o->sched_blocks.assign((size_t)count, 0);
+    for (int k = 0; k < count; ++k) {
+      o->sched_start[k] = (double)(R.h_times[2 * rank[k]] - t_min) * 1e-6;
+      o->sched_end[k] = (double)(R.h_times[2 * rank[k] + 1] - t_min) * 1e-6;
+      o->sched_blocks[k] = cuts[k].npx * cuts[k].npy;
+    }
+  }
   int worst = PYOMGPU_OK;
   for (int k = 0; k < count; ++k) {
     const CGResult& r = R.h_out[k];
@@ -1381,6 +1393,19 @@ int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* c, int32_t kernel) {
     if (!c->resd.ok) return fail(PYOMGPU_EINVAL, "the grid does not fit the resident kernel");
   }
   c->cg_kernel = kernel;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_batch_schedule(pyomgpu_ctx* c, int32_t count, double* start_ms, double* end_ms, int32_t* blocks) {
+  if (!c || count < 0) return fail(PYOMGPU_EINVAL, "batch_schedule: bad arguments");
+  if ((int)c->sched_start.size() != count)
+    return fail(PYOMGPU_ESTATE, "batch_schedule: the last resident batch of this context had %d solves",
+                (int)c->sched_start.size());
+  for (int k = 0; k < count; ++k) {
+    if (start_ms) start_ms[k] = c->sched_start[k];
+    if (end_ms) end_ms[k] = c->sched_end[k];
+    if (blocks) blocks[k] = c->sched_blocks[k];
+  }
   return PYOMGPU_OK;
 }
 

@@ -157,6 +157,10 @@ struct pyomgpu_ctx {
   // device time (ns) of this context's solves in the last resident batch, by
   // occurrence in that batch: the schedule's estimates for the next one
   std::vector<double> batch_ns;
+  // the last resident batch run by this (owner) context, per solve in call
+  // order: start and end (ms after the earliest start) and blocks used
+  std::vector<double> sched_start, sched_end;
+  std::vector<int> sched_blocks;
 
   ~pyomgpu_ctx() {
     for (void* p : fast.owned)

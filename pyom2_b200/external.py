@@ -490,6 +490,18 @@ def congrad_streamfunction_batch(contexts, forcs, sols, eps=1e-12, max_it=100000
     return [i.as_dict() for i in infos]
 
 
+def batch_schedule(owner, count):
+    """Diagnostics of the last resident batch whose first context was
+    ``owner``: per solve (call order) its device start and end in ms after
+    the earliest start, and the SMs it used."""
+    L = _abi.load()
+    st, en = np.zeros(count), np.zeros(count)
+    bl = np.zeros(count, dtype=np.int32)
+    _abi.check(L.pyomgpu_batch_schedule(owner._ctx, int(count), C.c_void_p(st.ctypes.data),
+                                        C.c_void_p(en.ctypes.data), C.c_void_p(bl.ctypes.data)))
+    return st, en, bl
+
+
 def island_boundaries(M, mnisle=0, maxipp=0, maxq=0, gpu=False):
     """Island labels and traced perimeters (streamfct_init.f90:35-267):
     returns (boundary, line_dir, nr_boundary) in the reference layout.  On
