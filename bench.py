@@ -317,6 +317,66 @@ def c3_learned(steps, warmup):
     return out
 
 
+def multi_rhs(steps, warmup, nrhs, peak):
+    """Many right-hand sides on one grid, the shape of the island right-hand
+    sides of streamfunction_init (streamfct_init.f90:272-287): nrhs seeded
+    smooth forcings on the 1440x720 grid, each solved from zero to the FP64
+    relative residual RTOL, three ways: one congrad_streamfunction_batch call
+    on the work-queue kernel (all solves streamed through HBM in lockstep; its
+    algorithmic bytes, 72 B per point per iteration, against the measured HBM
+    bandwidth), the same call on the resident engine (each solve on all SMs,
+    one after another in one launch), and nrhs sequential solve_rtol calls.
+    Device time by CUDA events; L2 holds ~1.5 of the 20 solves' working sets."""
+    import warnings
+
+    import torch
+    from pyom2_b200 import _abi, synth
+    from pyom2_b200.external import ExternalMode, congrad_streamfunction_batch
+
+    W = synth.config1()
+    E = ExternalMode(W.M)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        E.streamfunction_init(maxipp=10**6, maxq=10**6)
+    rng = np.random.default_rng(np.random.PCG64(4321))
+    forcs = []
+    for k in range(nrhs):
+        fpx, fpy = synth.random_fp(W.M, rng, sigma=float(rng.uniform(3.0, 12.0)), rms=1e-7)
+        f = synth.forcing_from_fp(W.M, fpx, fpy)
+        forcs.append(torch.from_numpy(np.ascontiguousarray(f.T)).cuda().T)
+    sols = [torch.zeros_like(f.T).T for f in forcs]
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        out = []
+        for k in range(warmup + steps):
+            for x in sols:
+                x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            e1.synchronize()
+            if k >= warmup:
+                out.append(e0.elapsed_time(e1))
+        return statistics.median(out), r
+
+    ems = [E] * nrhs
+    queue_ms, qi = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL, kernel="queue"))
+    res_ms, ri = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL, kernel="resident"))
+    seq_ms, si = timed(lambda: [E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64) for f, x in zip(forcs, sols)])
+    N = W.M.nx * W.M.ny
+    alg = sum(72.0 * N * i["iterations"] for i in qi)
+    achieved = alg / (queue_ms * 1e-3) / 1e9
+    return {"workload": f"c1_1440x720 x {nrhs} right-hand sides", "rtol": RTOL,
+            "queue_ms": queue_ms, "resident_ms": res_ms, "sequential_ms": seq_ms,
+            "iterations": [int(i["iterations"]) for i in qi],
+            "queue_max_rel_residual": max(i["rel_residual"] for i in qi),
+            "resident_max_rel_residual": max(i["rel_residual"] for i in ri),
+            "queue_roofline": {"kernel": "cg_batch_kernel", "algorithmic_bytes": alg, "achieved": achieved,
+                               "peak": peak, "unit": "GB/s", "frac": achieved / peak}}
+
+
 def c4_sequence(steps, spinup=10, members=8, methods=("ref", "batch_ref", "batch", "pcg64", "mixed32", "fcg")):
     """Config 4: consecutive time steps of ``members`` re-entrant channel runs
     (256x256x20, 60S-30S, one 2000 m ridge, 0.1 N/m^2 wind stress), each step
@@ -499,6 +559,7 @@ def main():
         r = c2_batch(max(1, args.steps), 1, args.c2_count)
         if rank == 0:
             print(json.dumps({"c2_batch": r}), flush=True)
+            print(json.dumps({"multi_rhs": multi_rhs(max(1, args.steps // 3), 1, 20, peaks()[0])}), flush=True)
         return
     if args.nh_only:
         r = nh_bench(args.steps, args.warmup, peaks()[0], nh_grid, max_it=args.nh_max_it,
@@ -673,6 +734,7 @@ def main():
                                           cpu=world == 1 and not args.no_cpu_baseline)
     if not args.no_c2 and rank == 0:
         out["c2_batch"] = c2_batch(max(1, args.steps // 3), 1, args.c2_count)
+        out["multi_rhs"] = multi_rhs(max(1, args.steps // 5), 1, 20, peak)
     if cpu_ref is not None:
         out["cpu_baseline"] = cpu_ref
     if rank == 0:

@@ -785,8 +785,9 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
 // cg_res_multi_kernel on all SMs.  Every solve takes its densest cut (res_cut
 // with the fewest pieces at 16 points per thread: the least block-time per
 // iteration) and is placed by list scheduling on the host, largest gangs
-// first, then longest: on the pieces' count of blocks that become free
-// earliest under the estimated durations (the grid's device time in the
+// first, then longest, improved by a seeded local search over the order: on
+// the pieces' count of blocks that become free earliest under the estimated
+// durations (the grid's device time in the
 // previous resident batch, measured with %globaltimer around its solve; else
 // ~2 x the square root of the point count iterations times the cut's
 // iteration estimate plus ~6 us of reduction latency); each block runs its
@@ -847,29 +848,65 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   *used = true;
   auto& B = o->batch;
   CK(cudaMemsetAsync(R.d_ctl, 0, sizeof(SyncCtl) * count, st));  // every solve's error flag
-  // list scheduling: gangs on the blocks free earliest
+  // list scheduling: in a given order, each job's gang on the blocks free earliest
+  std::vector<double> free_at((size_t)nsm), start((size_t)count, 0.0);
+  std::vector<std::vector<int>> gang((size_t)count);  // blocks of each job, piece order
+  std::vector<int> blk((size_t)nsm);
+  auto place = [&](const std::vector<int>& ord, bool record) {
+    std::fill(free_at.begin(), free_at.end(), 0.0);
+    double span = 0.0;
+    for (int k : ord) {
+      const int nb = cuts[k].npx * cuts[k].npy;
+      for (int b = 0; b < nsm; ++b) blk[b] = b;
+      std::nth_element(blk.begin(), blk.begin() + (nb - 1), blk.end(), [&](int a, int b) {
+        return free_at[a] != free_at[b] ? free_at[a] < free_at[b] : a < b;
+      });
+      double t = 0.0;
+      for (int q = 0; q < nb; ++q) t = std::max(t, free_at[blk[q]]);
+      for (int q = 0; q < nb; ++q) free_at[blk[q]] = t + est[k];
+      span = std::max(span, t + est[k]);
+      if (record) {
+        start[k] = t;
+        gang[k].assign(blk.begin(), blk.begin() + nb);
+        std::sort(gang[k].begin(), gang[k].end());
+      }
+    }
+    return span;
+  };
+  // order: largest gang first, then longest; then a seeded local search (swaps of
+  // nearby jobs, kept when the planned makespan drops) against gang fragmentation
   std::vector<int> order((size_t)count);
   for (int k = 0; k < count; ++k) order[k] = k;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     const int na = cuts[a].npx * cuts[a].npy, nb = cuts[b].npx * cuts[b].npy;
     return na != nb ? na > nb : est[a] > est[b];
   });
-  std::vector<double> free_at((size_t)nsm, 0.0), start((size_t)count, 0.0);
-  std::vector<std::vector<int>> gang((size_t)count);  // blocks of each job, piece order
-  std::vector<int> blk((size_t)nsm);
-  for (int k : order) {
-    const int nb = cuts[k].npx * cuts[k].npy;
-    for (int b = 0; b < nsm; ++b) blk[b] = b;
-    std::partial_sort(blk.begin(), blk.begin() + nb, blk.end(), [&](int a, int b) {
-      return free_at[a] != free_at[b] ? free_at[a] < free_at[b] : a < b;
-    });
-    double t = 0.0;
-    for (int q = 0; q < nb; ++q) t = std::max(t, free_at[blk[q]]);
-    start[k] = t;
-    gang[k].assign(blk.begin(), blk.begin() + nb);
-    std::sort(gang[k].begin(), gang[k].end());
-    for (int b : gang[k]) free_at[b] = t + est[k];
+  if (count > 2) {
+    double best = place(order, false);
+    uint64_t rng = 0x9E3779B97F4A7C15ull;
+    auto next = [&rng]() {
+      rng ^= rng << 13;
+      rng ^= rng >> 7;
+      rng ^= rng << 17;
+      return rng;
+    };
+    const int tries = std::max(20, std::min(400, 40000 / count));
+    std::vector<int> cand;
+    for (int it = 0; it < tries; ++it) {
+      cand = order;
+      for (int q = 0; q < 8; ++q) {
+        const int i = (int)(next() % (uint64_t)(count - 1));
+        const int j = std::min(count - 1, i + 1 + (int)(next() % 5));
+        std::swap(cand[i], cand[j]);
+      }
+      const double span = place(cand, false);
+      if (span < best) {
+        best = span;
+        order.swap(cand);
+      }
+    }
   }
+  place(order, true);
   // per-block lists in planned-start order (ties: job order above), one total order for all
   std::vector<int> rank((size_t)count);
   {
