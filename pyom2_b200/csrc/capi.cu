@@ -818,13 +818,28 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   }
   // fewer pieces in all than SMs: every solve gets its share of the SMs (in
   // proportion to its densest cut) and the fastest cut within it, all at once
-  if (need < nsm)
+  if (need < nsm) {
     for (int k = 0; k < count; ++k) {
       const pyomgpu_ctx* c = v[k].c;
       const int share = std::max(cuts[k].npx * cuts[k].npy, (nsm * cuts[k].npx * cuts[k].npy) / need);
       ResCut cut;
       if (res_cut(c->nx, c->ny, share, R.smem_cap, 16, false, cut)) cuts[k] = cut;
     }
+  } else {
+    // a solve beside whose densest cut no other solve of the batch fits takes the
+    // fastest cut over all SMs (the rest would idle while it runs)
+    std::vector<int> dense((size_t)count);
+    for (int k = 0; k < count; ++k) dense[k] = cuts[k].npx * cuts[k].npy;
+    for (int k = 0; k < count; ++k) {
+      int others = nsm + 1;  // the smallest densest cut among the other solves
+      for (int q = 0; q < count; ++q)
+        if (q != k) others = std::min(others, dense[q]);
+      if (others > nsm - dense[k]) {
+        ResCut cut;
+        if (res_cut(v[k].c->nx, v[k].c->ny, nsm, R.smem_cap, 16, false, cut)) cuts[k] = cut;
+      }
+    }
+  }
   // estimated duration (ns): this grid's device time in the previous resident batch at the
   // same occurrence, else ~2 sqrt(points) iterations x (the cut's iteration estimate + ~6 us
   // of reductions)
