@@ -524,6 +524,8 @@ def main():
                     help="skip config 2 (64 basins in one work-queue launch vs 64 sequential solves)")
     ap.add_argument("--c2-count", type=int, default=64, help="basins of config 2 (fewer for profiling)")
     ap.add_argument("--c2-only", action="store_true", help="time only config 2 and print its object (profiling runs)")
+    ap.add_argument("--multi-rhs-only", type=int, default=0,
+                    help="time only the many-right-hand-sides section with this many (profiling runs)")
     ap.add_argument("--no-c3", action="store_true", help="skip config 3 (learned FCG vs Jacobi-PCG on 2048x1024)")
     ap.add_argument("--no-c4", action="store_true",
                     help="skip config 4 (8-member channel ensemble, consecutive warm-started solves)")
@@ -555,6 +557,11 @@ def main():
     from pyom2_b200.external import ExternalMode, _ptr
 
     nh_grid = tuple(int(v) for v in args.nh_grid.split("x"))
+    if args.multi_rhs_only:
+        if rank == 0:
+            print(json.dumps({"multi_rhs": multi_rhs(max(1, args.steps), 1, args.multi_rhs_only, peaks()[0])}),
+                  flush=True)
+        return
     if args.c2_only:
         r = c2_batch(max(1, args.steps), 1, args.c2_count)
         if rank == 0:

@@ -863,6 +863,22 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   *used = true;
   auto& B = o->batch;
   CK(cudaMemsetAsync(R.d_ctl, 0, sizeof(SyncCtl) * count, st));  // every solve's error flag
+  // every solve's slice of the pool (call order), zeroed residual, all-ones records and
+  // slots (no tag of the solve, generation 0), packed first guess: on the stream while the
+  // host plans the schedule
+  std::vector<double*> slice((size_t)count);
+  {
+    double* cur = B.pool;
+    for (int k = 0; k < count; ++k) {
+      const pyomgpu_ctx* c = v[k].c;
+      const size_t P = align32(c->g.size());
+      slice[k] = cur;
+      CK(cudaMemsetAsync(cur + P, 0, P * sizeof(double), st));
+      CK(cudaMemsetAsync(cur + 2 * P, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
+      launch_pack(c->g, v[k].sol, cur, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
+      cur += batch_job_words(c->g.size());
+    }
+  }
   // list scheduling: in a given order, each job's gang on the blocks free earliest
   std::vector<double> free_at((size_t)nsm), start((size_t)count, 0.0);
   std::vector<std::vector<int>> gang((size_t)count);  // blocks of each job, piece order
@@ -896,6 +912,15 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     const int na = cuts[a].npx * cuts[a].npy, nb = cuts[b].npx * cuts[b].npy;
     return na != nb ? na > nb : est[a] > est[b];
   });
+  // the same solves as the owner's previous resident batch: start from its order, with
+  // fewer tries (the estimates change a little from call to call)
+  bool again = (int)o->sched_key.size() == count && (int)o->sched_order.size() == count;
+  for (int k = 0; again && k < count; ++k) again = o->sched_key[k] == v[k].c;
+  if (again) {
+    std::vector<char> seen((size_t)count, 0);
+    for (int k : o->sched_order) again = again && k >= 0 && k < count && !seen[k] && (seen[k] = 1);
+    if (again) order = o->sched_order;
+  }
   if (count > 2) {
     double best = place(order, false);
     uint64_t rng = 0x9E3779B97F4A7C15ull;
@@ -905,7 +930,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
       rng ^= rng << 17;
       return rng;
     };
-    const int tries = std::max(20, std::min(400, 40000 / count));
+    const int tries = again ? std::max(10, std::min(60, 6000 / count)) : std::max(20, std::min(400, 40000 / count));
     std::vector<int> cand;
     for (int it = 0; it < tries; ++it) {
       cand = order;
@@ -922,6 +947,9 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     }
   }
   place(order, true);
+  o->sched_key.resize((size_t)count);
+  for (int k = 0; k < count; ++k) o->sched_key[k] = v[k].c;
+  o->sched_order = order;
   // per-block lists in planned-start order (ties: job order above), one total order for all
   std::vector<int> rank((size_t)count);
   {
@@ -948,12 +976,12 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   h_off[nsm] = nent;
   // the job table in rank order (list entries name ranks)
   size_t smem = 0;
-  double* cur = B.pool;
   for (int r = 0; r < count; ++r) {
     const int k = job_of_rank[r];
     const pyomgpu_ctx* c = v[k].c;
     const ResCut& cut = cuts[k];
     const size_t P = align32(c->g.size());
+    double* cur = slice[k];
     CGResParams& J = R.h_jobs[r];
     J = CGResParams{};
     J.g = c->g;
@@ -977,11 +1005,6 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
     J.out = R.d_out + k;
     smem = std::max(smem, cut.smem);
-    CK(cudaMemsetAsync(J.res, 0, P * sizeof(double), st));
-    // records and slots all-ones: no tag of the solve (generation 0)
-    CK(cudaMemsetAsync(J.hx, 0xFF, (4 * P + (size_t)4 * (nsm + 1) * kResSlotWords) * sizeof(double), st));
-    launch_pack(c->g, v[k].sol, J.sol, true, st);  // setcyclic_xy(sol), solve_streamfct.f90:191-192
-    cur += batch_job_words(c->g.size());
   }
   o->stall_next = 0;
   const size_t list_words = (size_t)(reinterpret_cast<int*>(h_list + nent) - R.h_idx);

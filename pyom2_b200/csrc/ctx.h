@@ -161,6 +161,10 @@ struct pyomgpu_ctx {
   // order: start and end (ms after the earliest start) and blocks used
   std::vector<double> sched_start, sched_end;
   std::vector<int> sched_blocks;
+  // the solves (contexts, call order) and the schedule order of that batch: the
+  // starting point of the next batch's order search when it has the same solves
+  std::vector<const pyomgpu_ctx*> sched_key;
+  std::vector<int> sched_order;
 
   ~pyomgpu_ctx() {
     for (void* p : fast.owned)
