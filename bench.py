@@ -718,8 +718,9 @@ def main():
                      "algorithmic_bytes": R["algorithmic_bytes"], "peak_kind": peak_kind, "kernel": R["kernel"],
                      "kernel_ms": R["kernel_ms"], "bytes_per_point_iter": R["bytes_per_point_iter"],
                      **({"note": "fields stay in shared memory and TMEM for the whole solve, so DRAM moves only "
-                                 "the piece boundaries; frac is the algorithmic 72 B/point/iteration over the "
-                                 "measured HBM copy bandwidth (bandwidth-equivalent)"}
+                                 "the piece boundaries (traffic); frac is the algorithmic 72 B/point/iteration "
+                                 "over the measured HBM copy bandwidth, a bandwidth-equivalent figure that can "
+                                 "exceed 1 because the fields are read from shared memory and TMEM, not HBM"}
                         if R["kernel"].startswith("cg_res") else {})},
         "e2e": {"value": statistics.median(e2e), "unit": "ms/solve", "h2d_bytes_per_step": 2 * n2 * 8,
                 "d2h_bytes_per_step": n2 * 8},
