@@ -373,6 +373,13 @@ int32_t pyomgpu_set_batch_kernel(pyomgpu_ctx* ctx, int32_t kernel);
  * start, %globaltimer) and SMs used.  PYOMGPU_ESTATE when that batch had
  * another count or none ran on the resident engine.  Any output may be NULL. */
 int32_t pyomgpu_batch_schedule(pyomgpu_ctx* ctx, int32_t count, double* start_ms, double* end_ms, int32_t* blocks);
+/* The host planner of the resident batch on its own (no GPU work): `count`
+ * jobs, job k needing blocks[k] of nsm blocks for est[k]; `tries` local-search
+ * steps over the order.  Outputs (each may be NULL): rank (the order every
+ * block runs its jobs in), planned start, the blocks of each job (gang,
+ * count x nsm, ascending, padded with -1) and the planned makespan. */
+int32_t pyomgpu_plan_batch(int32_t nsm, int32_t count, const int32_t* blocks, const double* est, int32_t tries,
+                           int32_t* rank, double* start, int32_t* gang, double* makespan);
 
 /* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
  * products.  psi is psi(:,:,taup1), in/out, host or device. */

@@ -781,6 +781,87 @@ int rmulti_reserve(pyomgpu_ctx* o, int count) {
   return 0;
 }
 
+// List scheduling of rigid gangs on nsm blocks: job k needs nb[k] blocks for
+// est[k] (any unit).  In a given order each job takes the nb[k] blocks that
+// become free earliest (ties: lower block index) and starts when the last of
+// them is free.  The order: init (a permutation) or largest gang first, then
+// longest; then `tries` seeded local-search steps (a few swaps of nearby jobs,
+// kept when the makespan drops).  rank orders the jobs by planned start (ties:
+// the final order); a block serving several jobs runs them by rank, one total
+// order for all blocks, so gangs cannot wait on one another in a cycle.
+struct GangPlan {
+  std::vector<int> order, rank;
+  std::vector<double> start;
+  std::vector<std::vector<int>> gang;  // blocks of each job, ascending (piece q = gang[k][q])
+  double makespan = 0.0;
+};
+void plan_gangs(int nsm, const std::vector<int>& nb, const std::vector<double>& est, const std::vector<int>* init,
+                int tries, GangPlan& out) {
+  const int count = (int)nb.size();
+  std::vector<double> free_at((size_t)nsm);
+  std::vector<int> blk((size_t)nsm);
+  out.start.assign((size_t)count, 0.0);
+  out.gang.assign((size_t)count, {});
+  auto place = [&](const std::vector<int>& ord, bool record) {
+    std::fill(free_at.begin(), free_at.end(), 0.0);
+    double span = 0.0;
+    for (int k : ord) {
+      for (int b = 0; b < nsm; ++b) blk[b] = b;
+      std::nth_element(blk.begin(), blk.begin() + (nb[k] - 1), blk.end(), [&](int a, int b) {
+        return free_at[a] != free_at[b] ? free_at[a] < free_at[b] : a < b;
+      });
+      double t = 0.0;
+      for (int q = 0; q < nb[k]; ++q) t = std::max(t, free_at[blk[q]]);
+      for (int q = 0; q < nb[k]; ++q) free_at[blk[q]] = t + est[k];
+      span = std::max(span, t + est[k]);
+      if (record) {
+        out.start[k] = t;
+        out.gang[k].assign(blk.begin(), blk.begin() + nb[k]);
+        std::sort(out.gang[k].begin(), out.gang[k].end());
+      }
+    }
+    return span;
+  };
+  std::vector<int>& order = out.order;
+  order.resize((size_t)count);
+  if (init) {
+    order = *init;
+  } else {
+    for (int k = 0; k < count; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return nb[a] != nb[b] ? nb[a] > nb[b] : est[a] > est[b]; });
+  }
+  if (count > 2) {
+    double best = place(order, false);
+    uint64_t rng = 0x9E3779B97F4A7C15ull;
+    auto next = [&rng]() {
+      rng ^= rng << 13;
+      rng ^= rng >> 7;
+      rng ^= rng << 17;
+      return rng;
+    };
+    std::vector<int> cand;
+    for (int it = 0; it < tries; ++it) {
+      cand = order;
+      for (int q = 0; q < 8; ++q) {
+        const int i = (int)(next() % (uint64_t)(count - 1));
+        const int j = std::min(count - 1, i + 1 + (int)(next() % 5));
+        std::swap(cand[i], cand[j]);
+      }
+      const double span = place(cand, false);
+      if (span < best) {
+        best = span;
+        order.swap(cand);
+      }
+    }
+  }
+  out.makespan = place(order, true);
+  out.rank.assign((size_t)count, 0);
+  std::vector<int> by_start = order;
+  std::stable_sort(by_start.begin(), by_start.end(), [&](int a, int b) { return out.start[a] < out.start[b]; });
+  for (int r = 0; r < count; ++r) out.rank[by_start[r]] = r;
+}
+
 // The solves of `v` on the resident kernel, several at once, in one launch of
 // cg_res_multi_kernel on all SMs.  Every solve takes its densest cut (res_cut
 // with the fewest pieces at 16 points per thread: the least block-time per
@@ -879,84 +960,24 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
       cur += batch_job_words(c->g.size());
     }
   }
-  // list scheduling: in a given order, each job's gang on the blocks free earliest
-  std::vector<double> free_at((size_t)nsm), start((size_t)count, 0.0);
-  std::vector<std::vector<int>> gang((size_t)count);  // blocks of each job, piece order
-  std::vector<int> blk((size_t)nsm);
-  auto place = [&](const std::vector<int>& ord, bool record) {
-    std::fill(free_at.begin(), free_at.end(), 0.0);
-    double span = 0.0;
-    for (int k : ord) {
-      const int nb = cuts[k].npx * cuts[k].npy;
-      for (int b = 0; b < nsm; ++b) blk[b] = b;
-      std::nth_element(blk.begin(), blk.begin() + (nb - 1), blk.end(), [&](int a, int b) {
-        return free_at[a] != free_at[b] ? free_at[a] < free_at[b] : a < b;
-      });
-      double t = 0.0;
-      for (int q = 0; q < nb; ++q) t = std::max(t, free_at[blk[q]]);
-      for (int q = 0; q < nb; ++q) free_at[blk[q]] = t + est[k];
-      span = std::max(span, t + est[k]);
-      if (record) {
-        start[k] = t;
-        gang[k].assign(blk.begin(), blk.begin() + nb);
-        std::sort(gang[k].begin(), gang[k].end());
-      }
-    }
-    return span;
-  };
-  // order: largest gang first, then longest; then a seeded local search (swaps of
-  // nearby jobs, kept when the planned makespan drops) against gang fragmentation
-  std::vector<int> order((size_t)count);
-  for (int k = 0; k < count; ++k) order[k] = k;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-    const int na = cuts[a].npx * cuts[a].npy, nb = cuts[b].npx * cuts[b].npy;
-    return na != nb ? na > nb : est[a] > est[b];
-  });
-  // the same solves as the owner's previous resident batch: start from its order, with
-  // fewer tries (the estimates change a little from call to call)
+  // order: the owner's previous order when the batch has the same solves (the
+  // estimates change a little from call to call: fewer tries), else largest first
+  std::vector<int> nbk((size_t)count);
+  for (int k = 0; k < count; ++k) nbk[k] = cuts[k].npx * cuts[k].npy;
   bool again = (int)o->sched_key.size() == count && (int)o->sched_order.size() == count;
   for (int k = 0; again && k < count; ++k) again = o->sched_key[k] == v[k].c;
   if (again) {
     std::vector<char> seen((size_t)count, 0);
     for (int k : o->sched_order) again = again && k >= 0 && k < count && !seen[k] && (seen[k] = 1);
-    if (again) order = o->sched_order;
   }
-  if (count > 2) {
-    double best = place(order, false);
-    uint64_t rng = 0x9E3779B97F4A7C15ull;
-    auto next = [&rng]() {
-      rng ^= rng << 13;
-      rng ^= rng >> 7;
-      rng ^= rng << 17;
-      return rng;
-    };
-    const int tries = again ? std::max(10, std::min(60, 6000 / count)) : std::max(20, std::min(400, 40000 / count));
-    std::vector<int> cand;
-    for (int it = 0; it < tries; ++it) {
-      cand = order;
-      for (int q = 0; q < 8; ++q) {
-        const int i = (int)(next() % (uint64_t)(count - 1));
-        const int j = std::min(count - 1, i + 1 + (int)(next() % 5));
-        std::swap(cand[i], cand[j]);
-      }
-      const double span = place(cand, false);
-      if (span < best) {
-        best = span;
-        order.swap(cand);
-      }
-    }
-  }
-  place(order, true);
+  GangPlan plan;
+  plan_gangs(nsm, nbk, est, again ? &o->sched_order : nullptr,
+             again ? std::max(10, std::min(60, 6000 / count)) : std::max(20, std::min(400, 40000 / count)), plan);
   o->sched_key.resize((size_t)count);
   for (int k = 0; k < count; ++k) o->sched_key[k] = v[k].c;
-  o->sched_order = order;
-  // per-block lists in planned-start order (ties: job order above), one total order for all
-  std::vector<int> rank((size_t)count);
-  {
-    std::vector<int> by_start = order;
-    std::stable_sort(by_start.begin(), by_start.end(), [&](int a, int b) { return start[a] < start[b]; });
-    for (int r = 0; r < count; ++r) rank[by_start[r]] = r;
-  }
+  o->sched_order = plan.order;
+  const std::vector<int>& rank = plan.rank;
+  const std::vector<std::vector<int>>& gang = plan.gang;
   std::vector<std::vector<std::pair<int, int>>> lists((size_t)nsm);  // (rank, piece) per block
   for (int k = 0; k < count; ++k)
     for (int q = 0; q < (int)gang[k].size(); ++q) lists[gang[k][q]].push_back({rank[k], q});
@@ -1468,6 +1489,28 @@ int32_t pyomgpu_set_cg_kernel(pyomgpu_ctx* c, int32_t kernel) {
     if (!c->resd.ok) return fail(PYOMGPU_EINVAL, "the grid does not fit the resident kernel");
   }
   c->cg_kernel = kernel;
+  return PYOMGPU_OK;
+}
+
+int32_t pyomgpu_plan_batch(int32_t nsm, int32_t count, const int32_t* blocks, const double* est, int32_t tries,
+                           int32_t* rank, double* start, int32_t* gang, double* makespan) {
+  if (nsm < 1 || count < 1 || !blocks || !est || tries < 0) return fail(PYOMGPU_EINVAL, "plan_batch: bad arguments");
+  std::vector<int> nb((size_t)count);
+  std::vector<double> e((size_t)count);
+  for (int k = 0; k < count; ++k) {
+    if (blocks[k] < 1 || blocks[k] > nsm || !(est[k] >= 0.0)) return fail(PYOMGPU_EINVAL, "plan_batch: job %d", k);
+    nb[k] = blocks[k];
+    e[k] = est[k];
+  }
+  GangPlan plan;
+  plan_gangs(nsm, nb, e, nullptr, tries, plan);
+  for (int k = 0; k < count; ++k) {
+    if (rank) rank[k] = plan.rank[k];
+    if (start) start[k] = plan.start[k];
+    if (gang)
+      for (int q = 0; q < nsm; ++q) gang[(size_t)k * nsm + q] = q < nb[k] ? plan.gang[k][q] : -1;
+  }
+  if (makespan) *makespan = plan.makespan;
   return PYOMGPU_OK;
 }
 
