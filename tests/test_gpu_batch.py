@@ -174,3 +174,26 @@ def test_batch_timeout_then_usable(batch_set, engine):
     assert all(i["converged"] for i in infos)
     for s in sols[1:]:
         assert np.array_equal(s, sols[0])
+
+
+def test_batch_with_a_grid_beyond_the_resident_engine(batch_set):
+    """A batch holding a grid too large for the on-chip engine (2100 x 1000,
+    no islands): the resident engine refuses it with EINVAL, the automatic
+    engine runs the whole batch on the work-queue kernel, and every solve
+    reaches the residual."""
+    big = synth.basin(2100, 1000, 911, 0.2, 0, nz=4)
+    Eb = ExternalMode(big.M)
+    Eb.streamfunction_init(**LIMITS)
+    assert Eb.resident_layout() is None
+    W, O, E = batch_set[2]
+    ems, forcs = [Eb, E], [big.forc, W.forc]
+    sols = [np.zeros(big.M.shape2d, order="F"), np.zeros(W.M.shape2d, order="F")]
+    with pytest.raises(_abi.PyOMGPUError) as e:
+        external.congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=1e-10, kernel="resident")
+    assert e.value.code == _abi.EINVAL
+    sols = [np.zeros(big.M.shape2d, order="F"), np.zeros(W.M.shape2d, order="F")]
+    infos = external.congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=1e-10, kernel="auto")
+    assert all(i["status"] == 0 and i["rel_residual"] <= 1e-10 for i in infos), infos
+    cf = O.make_coeff_streamfunction()
+    assert O.rel_residual(cf, O.make_inv_sfc(cf), W.forc, sols[1]) <= 1.5e-10
+    Eb.close()
