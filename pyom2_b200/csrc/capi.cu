@@ -179,7 +179,8 @@ size_t res_smem_cap(pyomgpu_ctx* c) {
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess) return 0;
   size_t stat = 0;
-  std::vector<const void*> ks{cg_res_multi_kernel_ptr(), cg_res32_kernel_ptr(16), cg_res32_kernel_ptr(32)};
+  std::vector<const void*> ks{cg_res_multi_kernel_ptr(false), cg_res_multi_kernel_ptr(true), cg_res32_kernel_ptr(16),
+                              cg_res32_kernel_ptr(32)};
   for (int k = 0; k < kResNP; k++)
     for (bool single : {false, true}) ks.push_back(cg_res_kernel_ptr(kResP[k], single));
   for (const void* k : ks) {
@@ -876,16 +877,18 @@ void plan_gangs(int nsm, const std::vector<int>& nb, const std::vector<double>& 
 // *used = false (nothing run) when a grid does not fit on chip or the
 // resident kernel is unavailable; the caller then runs the work-queue kernel.
 int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, int max_it, double rtol,
-                  bool want_res, pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st, bool* used) {
+                  bool want_res, pyomgpu_solve_info* infos, float* ms_out, cudaStream_t st, bool* used,
+                  int weighted = 0) {
   *used = false;
   const int count = (int)v.size();
   auto& R = o->rmulti;
   if (R.smem_cap == 0) {
     const size_t cap = res_smem_cap(o);
     if (cap == 0) return PYOMGPU_OK;
-    if (cudaFuncSetAttribute(cg_res_multi_kernel_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) !=
-        cudaSuccess)
-      return PYOMGPU_OK;
+    for (bool w : {false, true})
+      if (cudaFuncSetAttribute(cg_res_multi_kernel_ptr(w), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap) !=
+          cudaSuccess)
+        return PYOMGPU_OK;
     R.smem_cap = cap;
   }
   const int nsm = std::min(o->nsm, kResMaxSlots - 1);
@@ -1024,6 +1027,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     J.ctl = R.d_ctl + k;
     J.timeout_ns = (unsigned long long)(o->timeout_s * 1e9);
     J.stall_extra = o->stall_next;  // test hook: every first reduction awaits a slot nobody writes
+    J.weighted = weighted;
     J.out = R.d_out + k;
     smem = std::max(smem, cut.smem);
   }
@@ -1047,7 +1051,8 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   M.gang_timeout_ns = (unsigned long long)(std::max(120.0, 64.0 * o->timeout_s) * 1e9);
   void* args[] = {&M};
   CK(cudaEventRecord(o->e0, st));
-  CK(cudaLaunchCooperativeKernel(cg_res_multi_kernel_ptr(), dim3(nsm), dim3(kResThreads), args, smem, st));
+  CK(cudaLaunchCooperativeKernel(cg_res_multi_kernel_ptr(weighted != 0), dim3(nsm), dim3(kResThreads), args, smem,
+                                 st));
   CK(cudaEventRecord(o->e1, st));
   CK(cudaMemcpyAsync(R.h_out, R.d_out, sizeof(CGResult) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(R.h_ctl, R.d_ctl, sizeof(SyncCtl) * count, cudaMemcpyDeviceToHost, st));
@@ -1233,15 +1238,15 @@ int psin_and_line_psin(pyomgpu_ctx* c, double eps, int max_it, cudaStream_t st) 
     std::vector<pyomgpu_solve_info> infos(v.size());
     const double e_k = c->psin_rtol > 0.0 ? 0.0 : eps;
     const int m_k = c->psin_rtol > 0.0 ? std::max(max_it, 1000000) : max_it;
-    // on-chip solves side by side where the grid fits (the reference's products); the
-    // work-queue kernel otherwise and for the area-weighted products
+    // on-chip solves side by side where the grid fits; the work-queue kernel otherwise
     bool resident = false;
     int rc = PYOMGPU_OK;
-    if (!c->psin_weighted && c->batch_kernel != 1) {
+    if (c->batch_kernel != 1) {
       size_t work = 0;
       for (const BatchSpec& b : v) work += batch_job_words(b.c->g.size());
       if ((rc = batch_reserve(c, (int)v.size(), work, 1))) return rc;
-      rc = run_res_multi(c, v, e_k, m_k, c->psin_rtol, false, infos.data(), nullptr, st, &resident);
+      rc = run_res_multi(c, v, e_k, m_k, c->psin_rtol, false, infos.data(), nullptr, st, &resident,
+                         c->psin_weighted);
       if (rc < 0 || rc == PYOMGPU_TIMEOUT) return rc;
     }
     if (!resident) {

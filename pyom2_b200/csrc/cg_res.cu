@@ -749,7 +749,10 @@ __device__ __forceinline__ void workers_sync() {
 // *s_tmem) and provides the dynamic shared memory sm.  Every block of the
 // group calls it for the same solve; a block returns once its share is done
 // (all threads together, after a block barrier).
-template <typename T, int P, bool TRACE>
+// WGT: the inner products (Z res, res) and (s, As) weighted by the cell area
+// D = 1/(ax by), in which A = D^-1 S is self-adjoint (the work-queue kernel's
+// option for the psin solves).
+template <typename T, int P, bool TRACE, bool WGT = false>
 __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, double* sm, const uint32_t* s_tmem_p,
                                           ResCtl& C, double (*wred)[kResSlotWords]) {
   // points per TMEM chunk (FP64: tcgen05 .x16 / .x8, .x16 at P = 16 spills; FP32: .x8)
@@ -898,7 +901,10 @@ __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, 
             w = op.W[g.at(i, j)];
             x = res_solv<T>(Pm)[g.at(i, j)];
             const T zr = w * rv;
-            v[0] += (double)zr * (double)rv;
+            if constexpr (WGT)
+              v[0] += (1.0 / ((double)axi * (double)sbx[ph + ly]) * zr) * rv;
+            else
+              v[0] += (double)zr * (double)rv;
             if (w != (T)0) {
               v[1] += (double)f * (double)f;
               v[2] += (double)rv * (double)rv;
@@ -969,7 +975,10 @@ __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, 
               const T fyn = sfy[(ly + 1) * pw + lx];
               const T a = axi * sbx[ly] * (fxe * (se - sc) + fxw * (sw - sc)) +
                           sbx[ph + ly] * (fyn * (sn - sc) + fys * (so - sc));
-              v[0] += (double)sc * (double)a;
+              if constexpr (WGT)
+                v[0] += (1.0 / ((double)axi * (double)sbx[ph + ly]) * sc) * a;
+              else
+                v[0] += (double)sc * (double)a;
               v[1] = fmax(v[1], fabs((double)sc));
               q[u] = a;
               fys = fyn;
@@ -1006,7 +1015,10 @@ __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, 
               const T w = colT_get<T>(bz, k);
               const T rv = colT_get<T>(br, k) - alpha * q[u];
               const T zr = w * rv;
-              v[0] += (double)zr * (double)rv;
+              if constexpr (WGT)
+                v[0] += (1.0 / ((double)axi * (double)sbx[ph + ly0 + u]) * zr) * rv;
+              else
+                v[0] += (double)zr * (double)rv;
               if (w != (T)0) v[1] += (double)rv * (double)rv;
               q[u] = zr;
               col_put(br, k, rv);
@@ -1116,7 +1128,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res32_kernel(const __grid_c
 // the whole gang is there, so the solve's own waits start with every piece
 // present.  A job has its own operator, vectors, slots, records, error flag
 // and result, so different jobs never wait on one another.
-template <int P>
+template <int P, bool WGT>
 __global__ void __launch_bounds__(kResThreads, 1) cg_res_multi_kernel(const __grid_constant__ ResMultiParams M) {
   extern __shared__ __align__(16) double sm[];
   __shared__ uint32_t s_tmem;
@@ -1148,7 +1160,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_multi_kernel(const __gr
     __syncthreads();
     if (!ok) break;
     if (ent.y == 0 && threadIdx.x == 0) M.times[2 * ent.x] = globaltimer_ns();
-    res_solve<double, P, false>(Pm, ent.y, sm, &s_tmem, C, wred);
+    res_solve<double, P, false, WGT>(Pm, ent.y, sm, &s_tmem, C, wred);
     if (ent.y == 0 && threadIdx.x == 0) M.times[2 * ent.x + 1] = globaltimer_ns();
   }
   tc::fence_before_sync();
@@ -1162,7 +1174,8 @@ template __global__ void cg_res_kernel<16, false>(const __grid_constant__ CGResP
 template __global__ void cg_res_kernel<4, true>(const __grid_constant__ CGResParams);
 template __global__ void cg_res_kernel<8, true>(const __grid_constant__ CGResParams);
 template __global__ void cg_res_kernel<16, true>(const __grid_constant__ CGResParams);
-template __global__ void cg_res_multi_kernel<16>(const __grid_constant__ ResMultiParams);
+template __global__ void cg_res_multi_kernel<16, false>(const __grid_constant__ ResMultiParams);
+template __global__ void cg_res_multi_kernel<16, true>(const __grid_constant__ ResMultiParams);
 template __global__ void cg_res32_kernel<16>(const __grid_constant__ CGResParams);
 template __global__ void cg_res32_kernel<32>(const __grid_constant__ CGResParams);
 
@@ -1563,7 +1576,9 @@ template __global__ void cg_res1_kernel<4>(const __grid_constant__ CGResParams);
 template __global__ void cg_res1_kernel<8>(const __grid_constant__ CGResParams);
 template __global__ void cg_res1_kernel<16>(const __grid_constant__ CGResParams);
 
-const void* cg_res_multi_kernel_ptr() { return (const void*)cg_res_multi_kernel<16>; }
+const void* cg_res_multi_kernel_ptr(bool weighted) {
+  return weighted ? (const void*)cg_res_multi_kernel<16, true> : (const void*)cg_res_multi_kernel<16, false>;
+}
 const void* cg_res32_kernel_ptr(int p) {
   return p == 16 ? (const void*)cg_res32_kernel<16> : p == 32 ? (const void*)cg_res32_kernel<32> : nullptr;
 }

@@ -39,6 +39,7 @@ struct CGResParams {
   SyncCtl* ctl;
   unsigned long long timeout_ns;
   unsigned stall_extra;  // test hook: the first reduction also awaits a slot nobody writes
+  int weighted;          // multi-solve kernel: inner products weighted by the cell area D = 1/(ax by)
   unsigned tag_gen;      // 0 .. 4094, different for consecutive solves of a context: the high bits of
                          // the epoch tags of the two-reduction kernel's slots and exchange records
   CGResult* out;
@@ -108,8 +109,9 @@ __host__ __device__ constexpr size_t res32_smem_bytes(int w, int h) {
   return 4 * (((size_t)(w + 2) * (h + 2) + (size_t)(w + 1) * h + (size_t)w * (h + 1) + 2 * (size_t)h +
                4 * (size_t)(w + h) + 3) / 4 * 4);
 }
-// The multi-solve launch of the two-reduction kernel at 16 points per thread.
-const void* cg_res_multi_kernel_ptr();
+// The multi-solve launch of the two-reduction kernel at 16 points per thread
+// (weighted: all its solves take the area-weighted products).
+const void* cg_res_multi_kernel_ptr(bool weighted = false);
 // The traced instantiation of the two-reduction kernel (same arithmetic).
 const void* cg_res_trace_kernel_ptr(int p);
 
