@@ -1,6 +1,7 @@
 """Independent solves over several GPUs: one process per GPU, each rank runs
-its share of the solves through one work-queue launch
-(``congrad_streamfunction_batch``), then every rank receives every result.
+its share of the solves through one batch call
+(``congrad_streamfunction_batch``: resident solves side by side, or the
+work-queue kernel), then every rank receives every result.
 
 A single solve does not shard (its per-iteration halo exchange and scalar
 all-reduces would be dominated by NVLink latency), but the units the
