@@ -364,12 +364,17 @@ def multi_rhs(steps, warmup, nrhs, peak):
     ems = [E] * nrhs
     queue_ms, qi = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL, kernel="queue"))
     res_ms, ri = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL, kernel="resident"))
+    from pyom2_b200.external import batch_schedule
+    t0, t1, nblk = batch_schedule(E, nrhs)
+    sched = {"makespan_ms": float(t1.max()), "solo_sum_ms": float((t1 - t0).sum()),
+             "solo_ms_per_iteration_us": float((t1 - t0).sum() * 1e3 / sum(i["iterations"] for i in ri)),
+             "blocks": int(nblk.max())}
     seq_ms, si = timed(lambda: [E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64) for f, x in zip(forcs, sols)])
     N = W.M.nx * W.M.ny
     alg = sum(72.0 * N * i["iterations"] for i in qi)
     achieved = alg / (queue_ms * 1e-3) / 1e9
     return {"workload": f"c1_1440x720 x {nrhs} right-hand sides", "rtol": RTOL,
-            "queue_ms": queue_ms, "resident_ms": res_ms, "sequential_ms": seq_ms,
+            "queue_ms": queue_ms, "resident_ms": res_ms, "sequential_ms": seq_ms, "resident_schedule": sched,
             "iterations": [int(i["iterations"]) for i in qi],
             "queue_max_rel_residual": max(i["rel_residual"] for i in qi),
             "resident_max_rel_residual": max(i["rel_residual"] for i in ri),
