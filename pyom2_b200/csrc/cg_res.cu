@@ -415,7 +415,10 @@ using Halo = HaloT<double>;
 // record until both of its values carry `tag`.  False on time-out.
 template <typename T>
 __device__ __forceinline__ bool worker_halo_load_tagged(const CGResParams& P, HaloT<T> (&hl)[2], unsigned tag) {
+  // parameters read once into registers (the polls' memory clobbers would reload them every spin)
   const unsigned long long* hx = reinterpret_cast<const unsigned long long*>(P.hx);
+  int* const err = &P.ctl->error;
+  const unsigned long long tmo = P.timeout_ns;
   const unsigned long long t0 = globaltimer_ns();
   // one record after the other (a worker rarely has two)
 #pragma unroll 1
@@ -441,8 +444,8 @@ __device__ __forceinline__ bool worker_halo_load_tagged(const CGResParams& P, Ha
         }
       }
       if (ok) break;
-      if ((spin & 63u) == 0u && (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
-        atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+      if ((spin & 63u) == 0u && (ld_relaxed_i32(err) != 0 || globaltimer_ns() - t0 > tmo)) {
+        atomicExch(err, PYOMGPU_TIMEOUT);
         return false;
       }
     }
@@ -506,7 +509,7 @@ __device__ __forceinline__ void copy_out(const CGResParams& P, double* hx, const
 template <typename T>
 __device__ __forceinline__ void copy_out_tagged(const CGResParams& P, const T* spub, int ilo, int ihi, int jlo,
                                                 int jhi, int wt, unsigned tag) {
-  const Geo& g = P.g;
+  const Geo g = P.g;
   unsigned long long* hx = reinterpret_cast<unsigned long long*>(P.hx);
   const int pw = ihi - ilo + 1, ph = jhi - jlo + 1, nent = 2 * (pw + ph);
 #pragma unroll 1
@@ -577,11 +580,16 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
                                                  unsigned long long* tr = nullptr) {
   const int lane = threadIdx.x;
   const unsigned tag = res_tag(P, ep);
+  // parameters read once into registers (the polls' memory clobbers would reload them every spin)
+  unsigned long long* const slot_base = reinterpret_cast<unsigned long long*>(P.slots);
+  const int nslot = P.nslot;
+  int* const err = &P.ctl->error;
+  const unsigned long long tmo = P.timeout_ns;
   // tagged slots: 2 buffers x nslot x 2 kResSlotWords words; a block overwrites its
   // slot of epoch ep at ep+2, when every block has published ep+1, i.e. finished
   // reading epoch ep
   auto tslot = [&](unsigned e, int b) {
-    return reinterpret_cast<unsigned long long*>(P.slots) + ((size_t)(e & 1u) * P.nslot + b) * (2 * kResSlotWords);
+    return slot_base + ((size_t)(e & 1u) * nslot + b) * (2 * kResSlotWords);
   };
   if constexpr (TAG) {
     double t[NV];
@@ -648,9 +656,8 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
         }
         if (all) have |= 1u << m;
       }
-      if (have != want && (spin & 31u) == 0u &&
-          (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
-        atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+      if (have != want && (spin & 31u) == 0u && (ld_relaxed_i32(err) != 0 || globaltimer_ns() - t0 > tmo)) {
+        atomicExch(err, PYOMGPU_TIMEOUT);
         ok = false;
         break;
       }
@@ -676,9 +683,8 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
       for (int k = 0; k < NV; k++) all = all && !is_empty(got[m][k]);
       if (all) have |= 1u << m;
     }
-    if (have != want && (spin & 31u) == 0u &&
-        (ld_relaxed_i32(&P.ctl->error) != 0 || globaltimer_ns() - t0 > P.timeout_ns)) {
-      atomicExch(&P.ctl->error, PYOMGPU_TIMEOUT);
+    if (have != want && (spin & 31u) == 0u && (ld_relaxed_i32(err) != 0 || globaltimer_ns() - t0 > tmo)) {
+      atomicExch(err, PYOMGPU_TIMEOUT);
       ok = false;
       break;
     }
