@@ -551,11 +551,7 @@ int batch_reserve(pyomgpu_ctx* o, int count, size_t pool, size_t tasks) {
   auto& B = o->batch;
   if (!B.sync) {
     int per_sm = 0;
-    if (cudaFuncSetAttribute(cg_batch_kernel_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)cg_batch_smem_bytes()) != cudaSuccess)
-      return fail(PYOMGPU_ECUDA, "cannot reserve shared memory for the batch kernel");
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_batch_kernel_ptr(), kBatchThreads,
-                                                      cg_batch_smem_bytes()) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_batch_kernel_ptr(), kBatchThreads, 0) !=
             cudaSuccess ||
         per_sm < 1)
       return fail(PYOMGPU_ECUDA, "occupancy query of the batch kernel failed");

@@ -24,19 +24,6 @@ constexpr int kBX = kOnx + 64;  // box columns: Fortran i0-1 .. i0+64
 constexpr int kTX = 64, kTY = 16;
 constexpr int kBY = kTY + 2;
 constexpr int kBoxN = kBX * kBY;
-constexpr int kBoxFields = 5;  // res, Z, s_old, FX, FY of one sweep-A box
-
-// 8-byte asynchronous global -> shared copies (zero fill when src_bytes is 0),
-// completed per thread by commit/wait groups.
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 enum : int { kInit = 0, kSweepA = 1, kSweepB = 2 };
 
@@ -331,40 +318,10 @@ __device__ __forceinline__ int act_find(const int* off, int m, int task) {
   return lo;
 }
 
-// Sweep A: the raw fields (res, Z, s_old, FX, FY) of task's box -- its tile
-// plus a one-cell halo, zero outside the padded grid -- into buf (kBoxFields x
-// kBoxN doubles) with asynchronous copies, committed as one group.
-__device__ __forceinline__ void box_prefetch(const BatchParams& P, double* buf, int task, const int* off,
-                                             const int* prb, int m) {
-  const int k = act_find(off, m, task);
-  const BatchProblem& pr = P.probs[prb[k]];
-  const Geo g = pr.g;
-  const int n = __ldcg(&P.state[prb[k]].n);
-  const double* so = pr.s[(n + 1) & 1];
-  const int lt = task - off[k];
-  const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
-  for (int e = threadIdx.x; e < kBoxN; e += kBatchThreads) {
-    const int i = i0 - 1 + e % kBX, j = j0 - 1 + e / kBX;
-    const bool in = i <= g.nx + kOnx && j <= g.ny + kOnx;
-    const size_t q = in ? g.at(i, j) : 0;
-    const int nbytes = in ? 8 : 0;
-    cp_async8(buf + e, pr.res + q, nbytes);
-    cp_async8(buf + kBoxN + e, pr.op.W + q, nbytes);
-    cp_async8(buf + 2 * kBoxN + e, so + q, nbytes);
-    cp_async8(buf + 3 * kBoxN + e, pr.op.FX + q, nbytes);
-    cp_async8(buf + 4 * kBoxN + e, pr.op.FY + q, nbytes);
-  }
-  cp_async_commit();
-}
-
 }  // namespace
 
-// Dynamic shared memory: two sweep-A boxes, so the next task's box streams in
-// while the current one is computed.
-constexpr size_t kBatchSmem = 2 * kBoxFields * kBoxN * sizeof(double);
-
-__global__ void __launch_bounds__(kBatchThreads, 2) cg_batch_kernel(const BatchParams P) {
-  extern __shared__ __align__(16) double box[];  // 2 x kBoxFields x kBoxN
+__global__ void __launch_bounds__(kBatchThreads, 4) cg_batch_kernel(const BatchParams P) {
+  __shared__ double b_s[kBoxN], b_FX[kBoxN], b_FY[kBoxN];
   __shared__ int s_act_prob[kBatchActMax], s_act_off[kBatchActMax + 1];
   __shared__ int s_actn;
   unsigned long long epoch = 0;
@@ -425,27 +382,12 @@ __global__ void __launch_bounds__(kBatchThreads, 2) cg_batch_kernel(const BatchP
   for (;;) {
     if (s_actn == 0) break;
     // ---- sweep A: s_new = Z res + bq s_old on tile + halo, As = A s_new ---------------
-    // the boxes are double-buffered: while task t is computed from one, the
-    // asynchronous copies of task t + gridDim.x fill the other
     {
       const int m = s_actn;
       const int* off = list_off();
       const int* prb = list_prob();
       const int ntot = off[m];
-      int cur = 0;
-      if ((int)blockIdx.x < ntot) box_prefetch(P, box, blockIdx.x, off, prb, m);
-      for (int task = blockIdx.x; task < ntot; task += gridDim.x, cur ^= 1) {
-        const int nxt = task + gridDim.x;
-        if (nxt < ntot) {
-          box_prefetch(P, box + (cur ^ 1) * kBoxFields * kBoxN, nxt, off, prb, m);
-          cp_async_wait<1>();
-        } else {
-          cp_async_wait<0>();
-        }
-        __syncthreads();  // every thread's copies of this task's box have landed
-        double* b = box + cur * kBoxFields * kBoxN;
-        const double* b_FX = b + 3 * kBoxN;
-        const double* b_FY = b + 4 * kBoxN;
+      for (int task = blockIdx.x; task < ntot; task += gridDim.x) {
         const int k = act_find(off, m, task);
         const int p = prb[k];
         const BatchProblem& pr = P.probs[p];
@@ -453,13 +395,29 @@ __global__ void __launch_bounds__(kBatchThreads, 2) cg_batch_kernel(const BatchP
         const OpDev<double> op = pr.op;
         const int n = __ldcg(&P.state[p].n);
         const double bq = __ldcg(&P.state[p].bq);
+        const double* __restrict__ so = pr.s[(n + 1) & 1];
         double* __restrict__ sn = pr.s[n & 1];
         const int lt = task - off[k];
         const int i0 = 1 + kTX * (lt % pr.ntx), j0 = 1 + kTY * (lt / pr.ntx);
-        // the direction on the box, in place of res: Z res + bq s_old
-        for (int e = threadIdx.x; e < kBoxN; e += kBatchThreads) b[e] = b[kBoxN + e] * b[e] + bq * b[2 * kBoxN + e];
+        __syncthreads();  // shared boxes of the previous task are free
+        // four box points per thread in flight (the loads do not depend on the shared stores)
+#pragma unroll 4
+        for (int e = threadIdx.x; e < kBoxN; e += kBatchThreads) {
+          const int i = i0 - 1 + e % kBX, j = j0 - 1 + e / kBX;
+          double r = 0.0, w = 0.0, s = 0.0, fx = 0.0, fy = 0.0;
+          if (i <= g.nx + kOnx && j <= g.ny + kOnx) {
+            const size_t q = g.at(i, j);
+            r = pr.res[q];
+            w = op.W[q];
+            s = so[q];
+            fx = op.FX[q];
+            fy = op.FY[q];
+          }
+          b_s[e] = w * r + bq * s;
+          b_FX[e] = fx;
+          b_FY[e] = fy;
+        }
         __syncthreads();
-        const double* b_s = b;
         double v[2] = {0.0, 0.0};
         for (int e = threadIdx.x; e < kTX * kTY; e += kBatchThreads) {
           const int c = e % kTX, rr = e / kTX;
@@ -477,7 +435,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) cg_batch_kernel(const BatchP
           v[1] = fmax(v[1], fabs(sc));
         }
         double out[2];
-        block_reduce<2, 1, kBatchThreads>(v, out);  // ends with a block barrier: this box is free again
+        block_reduce<2, 1, kBatchThreads>(v, out);
         if (threadIdx.x == 0) {
           P.part[(size_t)(pr.tile0 + lt) * 4] = out[0];
           P.part[(size_t)(pr.tile0 + lt) * 4 + 1] = out[1];
@@ -534,13 +492,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) cg_batch_kernel(const BatchP
 
 const void* cg_batch_kernel_ptr() { return (const void*)cg_batch_kernel; }
 
-size_t cg_batch_smem_bytes() { return kBatchSmem; }
-
 cudaError_t launch_cg_batch(const BatchParams& P, int grid, cudaStream_t st) {
   BatchParams Q = P;
   void* args[] = {&Q};
-  return cudaLaunchCooperativeKernel((const void*)cg_batch_kernel, dim3(grid), dim3(kBatchThreads), args, kBatchSmem,
-                                     st);
+  return cudaLaunchCooperativeKernel((const void*)cg_batch_kernel, dim3(grid), dim3(kBatchThreads), args, 0, st);
 }
 
 }  // namespace pyomgpu

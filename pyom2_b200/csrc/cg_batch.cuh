@@ -63,8 +63,5 @@ struct BatchParams {
 // Cooperative launch (all blocks co-resident: grid <= occupancy x SMs).
 cudaError_t launch_cg_batch(const BatchParams& P, int grid, cudaStream_t st);
 const void* cg_batch_kernel_ptr();
-// Dynamic shared memory of a launch (two sweep-A boxes; the caller sets the
-// kernel's attribute once).
-size_t cg_batch_smem_bytes();
 
 }  // namespace pyomgpu
