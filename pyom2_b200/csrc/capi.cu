@@ -799,27 +799,33 @@ struct GangPlan {
 void plan_gangs(int nsm, const std::vector<int>& nb, const std::vector<double>& est, const std::vector<int>* init,
                 int tries, GangPlan& out) {
   const int count = (int)nb.size();
-  std::vector<double> free_at((size_t)nsm);
-  std::vector<int> blk((size_t)nsm);
+  // the blocks as (free time, index), kept sorted: a job takes the first nb[k]
+  // (the earliest free, lower index first on ties), which all become free at
+  // t + est[k] and are merged back into place -- O(nsm) per job, no sort
+  std::vector<std::pair<double, int>> fr((size_t)nsm), taken, merged((size_t)nsm);
   out.start.assign((size_t)count, 0.0);
   out.gang.assign((size_t)count, {});
   auto place = [&](const std::vector<int>& ord, bool record) {
-    std::fill(free_at.begin(), free_at.end(), 0.0);
+    for (int b = 0; b < nsm; ++b) fr[b] = {0.0, b};
     double span = 0.0;
     for (int k : ord) {
-      for (int b = 0; b < nsm; ++b) blk[b] = b;
-      std::nth_element(blk.begin(), blk.begin() + (nb[k] - 1), blk.end(), [&](int a, int b) {
-        return free_at[a] != free_at[b] ? free_at[a] < free_at[b] : a < b;
-      });
-      double t = 0.0;
-      for (int q = 0; q < nb[k]; ++q) t = std::max(t, free_at[blk[q]]);
-      for (int q = 0; q < nb[k]; ++q) free_at[blk[q]] = t + est[k];
-      span = std::max(span, t + est[k]);
+      const int n = nb[k];
+      const double t = fr[n - 1].first;
+      const double done = t + est[k];
+      span = std::max(span, done);
+      taken.assign(fr.begin(), fr.begin() + n);
       if (record) {
         out.start[k] = t;
-        out.gang[k].assign(blk.begin(), blk.begin() + nb[k]);
+        out.gang[k].resize((size_t)n);
+        for (int q = 0; q < n; ++q) out.gang[k][q] = taken[q].second;
         std::sort(out.gang[k].begin(), out.gang[k].end());
       }
+      for (auto& e : taken) e.first = done;
+      std::sort(taken.begin(), taken.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+        return a.second < b.second;  // equal times: by index
+      });
+      std::merge(fr.begin() + n, fr.end(), taken.begin(), taken.end(), merged.begin());
+      fr.swap(merged);
     }
     return span;
   };
@@ -975,7 +981,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   }
   GangPlan plan;
   plan_gangs(nsm, nbk, est, again ? &o->sched_order : nullptr,
-             again ? std::max(10, std::min(60, 6000 / count)) : std::max(20, std::min(400, 40000 / count)), plan);
+             again ? std::max(20, std::min(150, 15000 / count)) : std::max(20, std::min(400, 40000 / count)), plan);
   o->sched_key.resize((size_t)count);
   for (int k = 0; k < count; ++k) o->sched_key[k] = v[k].c;
   o->sched_order = plan.order;
