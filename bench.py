@@ -255,7 +255,10 @@ def c2_batch(steps, warmup, count=64):
     span = float(t1.max())
     nsm = torch.cuda.get_device_properties(0).multi_processor_count
     sched = {"makespan_ms": span, "sm_utilisation": float((nblk * (t1 - t0)).sum() / (nsm * span)),
-             "solo_sum_ms": float((t1 - t0).sum()), "blocks_max": int(nblk.max()), "blocks_min": int(nblk.min())}
+             "solo_sum_ms": float((t1 - t0).sum()), "blocks_max": int(nblk.max()), "blocks_min": int(nblk.min()),
+             "per_grid": {"points": [int(w.M.nx * w.M.ny) for w in ws], "blocks": [int(b) for b in nblk],
+                          "ms": [round(float(x), 3) for x in (t1 - t0)],
+                          "iterations": [int(i["iterations"]) for i in infos]}}
     queue_ms, qinfos = timed(lambda: congrad_streamfunction_batch(ems, forcs, sols, eps=0.0, rtol=RTOL,
                                                                   kernel="queue"))
     seq_ms, seq = timed(lambda: [E.solve_rtol(f, x, rtol=RTOL, precision=_abi.PREC_F64)
