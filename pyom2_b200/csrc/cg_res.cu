@@ -43,6 +43,8 @@
 // PYOMGPU_TIMEOUT in the control block, frees its TMEM and returns.
 #include <math.h>
 
+#include <type_traits>
+
 #include "cg_res.cuh"
 #include "tc.cuh"
 
@@ -134,6 +136,21 @@ __device__ __forceinline__ void ld_relaxed_v4_u64(const unsigned long long* p, u
                : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3)
                : "l"(p)
                : "memory");
+}
+// The same four words read by atomic no-op read-modify-writes (OR with 0).  An
+// RMW is performed where the line is owned and reads the latest value; a gang
+// whose blocks had polled one slot for microseconds with plain loads saw its
+// new value ~2 us after the writer's fence, and with these reads mixed in it
+// left a two-group lag (half the blocks ~2.5 us behind, alternating at the two
+// reductions) less often.
+__device__ __forceinline__ void rmw_read_v4_u64(const unsigned long long* p, unsigned long long& w0,
+                                                unsigned long long& w1, unsigned long long& w2,
+                                                unsigned long long& w3) {
+  unsigned long long* q = const_cast<unsigned long long*>(p);
+  asm volatile("atom.relaxed.gpu.global.or.b64 %0, [%1], 0;" : "=l"(w0) : "l"(q) : "memory");
+  asm volatile("atom.relaxed.gpu.global.or.b64 %0, [%1], 0;" : "=l"(w1) : "l"(q + 1) : "memory");
+  asm volatile("atom.relaxed.gpu.global.or.b64 %0, [%1], 0;" : "=l"(w2) : "l"(q + 2) : "memory");
+  asm volatile("atom.relaxed.gpu.global.or.b64 %0, [%1], 0;" : "=l"(w3) : "l"(q + 3) : "memory");
 }
 
 __device__ __forceinline__ void st_relaxed_v2_u64(unsigned long long* p, unsigned long long w0, unsigned long long w1) {
@@ -574,7 +591,10 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // blocks until no word is empty; the totals are formed in a fixed order, so
 // every block obtains the same bits, and lane 0 advances the control state.
 // False on time-out.
-template <int NV, int kMaxSlot, int kStep, bool TAG = false>
+// FRESH (tagged slots only): once a poll has lasted kFreshPollNs, every 8th
+// pass reads the pending slots with rmw_read_v4_u64 instead of loads.
+constexpr unsigned long long kFreshPollNs = 1500;
+template <int NV, int kMaxSlot, int kStep, bool TAG = false, bool FRESH = false>
 __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned ep, int bid, int npoll, ResCtl& C,
                                                  const double (*wred)[kResSlotWords], unsigned* hflag = nullptr,
                                                  unsigned long long* tr = nullptr) {
@@ -602,7 +622,14 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
 #pragma unroll
     for (int k = 0; k < NV; k++)
       if ((lane >> 1) == k) mv = t[k];
-    if (lane < 2 * NV) st_relaxed_u64(tslot(ep, bid) + lane, (lane & 1) ? tag_hi(tag, mv) : tag_lo(tag, mv));
+    if (lane < 2 * NV) {
+      st_relaxed_u64(tslot(ep, bid) + lane, (lane & 1) ? tag_hi(tag, mv) : tag_lo(tag, mv));
+      // pushes the slot out before this block starts polling: without it a
+      // relaxed store stayed invisible to the other blocks for ~2-3 us at times,
+      // and dense gangs settled into two groups ~2.5 us apart (13-14 us per
+      // iteration instead of ~9.5; no cost measured on the 1440x720 solve)
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    }
     if (tr != nullptr && lane == 0) tr[0] = globaltimer_ns();
   } else {
     double t[NV];  // lane w holds worker warp w's partials; fixed shuffle tree
@@ -635,8 +662,9 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
   bool ok = true;
   const unsigned long long t0 = globaltimer_ns();
   if constexpr (TAG) {
-    // every tagged word of every slot this lane polls in one pass of relaxed loads
-    for (unsigned spin = 1; have != want; spin++) {
+    // every tagged word of every slot this lane polls in one pass of relaxed
+    // loads (RMW reads: the FRESH passes)
+    auto pass = [&](auto rmw) {
       const unsigned pend = want & ~have;
 #pragma unroll
       for (int m = 0; m < kPer; m++) {
@@ -646,7 +674,10 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
 #pragma unroll
         for (int k = 0; k < NV; k += 2) {  // two values (four words, 32 bytes) per load
           unsigned long long w0, w1, w2, w3;
-          ld_relaxed_v4_u64(sl + 2 * k, w0, w1, w2, w3);
+          if constexpr (decltype(rmw)::value)
+            rmw_read_v4_u64(sl + 2 * k, w0, w1, w2, w3);
+          else
+            ld_relaxed_v4_u64(sl + 2 * k, w0, w1, w2, w3);
           all = all && tag_ok(w0, tag) && tag_ok(w1, tag);
           got[m][k] = untag(w0, w1);  // kept only once every word of the slot is current
           if (k + 1 < NV) {
@@ -655,6 +686,16 @@ __device__ __forceinline__ bool controller_epoch(const CGResParams& P, unsigned 
           }
         }
         if (all) have |= 1u << m;
+      }
+    };
+    for (unsigned spin = 1; have != want; spin++) {
+      if constexpr (FRESH) {
+        if ((spin & 7u) == 0u && globaltimer_ns() - t0 > kFreshPollNs)
+          pass(std::true_type{});
+        else
+          pass(std::false_type{});
+      } else {
+        pass(std::false_type{});
       }
       if (have != want && (spin & 31u) == 0u && (ld_relaxed_i32(err) != 0 || globaltimer_ns() - t0 > tmo)) {
         atomicExch(err, PYOMGPU_TIMEOUT);
@@ -758,7 +799,9 @@ __device__ __forceinline__ void workers_sync() {
 // WGT: the inner products (Z res, res) and (s, As) weighted by the cell area
 // D = 1/(ax by), in which A = D^-1 S is self-adjoint (the work-queue kernel's
 // option for the psin solves).
-template <typename T, int P, bool TRACE, bool WGT = false>
+// FRESH: the reduction polls mix in atomic reads after a long wait
+// (controller_epoch), for the gangs of the multi-solve kernel.
+template <typename T, int P, bool TRACE, bool WGT = false, bool FRESH = false>
 __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, double* sm, const uint32_t* s_tmem_p,
                                           ResCtl& C, double (*wred)[kResSlotWords]) {
   // points per TMEM chunk (FP64: tcgen05 .x16 / .x8, .x16 at P = 16 spills; FP32: .x8)
@@ -809,14 +852,15 @@ __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, 
     unsigned ep = 0;
     bool stopped_after_update = false;  // the stop decided before sweep B (C stays as the workers read it)
     __syncthreads();  // S1
-    bool ok = controller_epoch<4, 3, kStepInit, true>(Pm, ep, bid, nb + (Pm.stall_extra ? 1 : 0), C, wred);
+    bool ok = controller_epoch<4, 3, kStepInit, true, FRESH>(Pm, ep, bid, nb + (Pm.stall_extra ? 1 : 0), C, wred);
     if (!__syncthreads_and(ok)) goto out;  // S2
     if (C.act == kRun) {
       for (unsigned trip = 0;; trip++) {
         unsigned long long* tr = threadIdx.x == 0 ? trace_row(trip) : nullptr;
         __syncthreads();  // S1: partials of sweep A
         if (TRACE && tr) tr[10] = globaltimer_ns();
-        ok = controller_epoch<2, 1, kStepA, true>(Pm, ++ep, bid, nb, C, wred, nullptr, TRACE && tr ? tr + 11 : nullptr);
+        ok = controller_epoch<2, 1, kStepA, true, FRESH>(Pm, ++ep, bid, nb, C, wred, nullptr,
+                                                        TRACE && tr ? tr + 11 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
         if (C.stop_after) {  // the workers finish sweep B and stop
@@ -825,7 +869,7 @@ __device__ __forceinline__ void res_solve(const CGResParams& Pm, const int bid, 
         }
         __syncthreads();  // S1: partials of sweep B
         if (TRACE && tr) tr[14] = globaltimer_ns();
-        ok = controller_epoch<2, -1, kStepB, true>(Pm, ++ep, bid, nb, C, wred, nullptr,
+        ok = controller_epoch<2, -1, kStepB, true, FRESH>(Pm, ++ep, bid, nb, C, wred, nullptr,
                                                    TRACE && tr ? tr + 15 : nullptr);
         if (!__syncthreads_and(ok)) goto out;  // S2
         if (C.act != kRun) break;
@@ -1177,7 +1221,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_res_multi_kernel(const __gr
     __syncthreads();
     if (!ok) break;
     if (ent.y == 0 && threadIdx.x == 0) M.times[2 * ent.x] = globaltimer_ns();
-    res_solve<double, P, false, WGT>(Pm, ent.y, sm, &s_tmem, C, wred);
+    res_solve<double, P, false, WGT, true>(Pm, ent.y, sm, &s_tmem, C, wred);
     if (ent.y == 0 && threadIdx.x == 0) M.times[2 * ent.x + 1] = globaltimer_ns();
   }
   tc::fence_before_sync();
