@@ -130,23 +130,40 @@ int finish_cg(pyomgpu_ctx* c, pyomgpu_solve_info* info, cudaStream_t st) {
   return c->h_result->status;
 }
 
+// Estimated iteration time (ns) of the FP64 resident kernel on a w x h piece
+// at p points per thread with nb blocks, fitted to the 1440x720 solve timed
+// under all 18 cuts that fit at 16 points per thread (8.9-10.2 us, fit within
+// ~0.2 us): a constant, the piece's points, the cache lines its exchange
+// records occupy (a west or east record on a line of its own, south and north
+// ones four to a line), the warps whose threads span two column segments
+// (e.g. 39-wide pieces: 11 of 15; 160-wide: none) and the reduction slots.
+double res_iter_ns(int w, int h, int p, int nb) {
+  const int thr = res_threads(w, h, p);
+  int straddle = 0;
+  for (int t0 = 0; t0 < thr; t0 += 32)
+    if (t0 / w != std::min(t0 + 31, thr - 1) / w) straddle++;
+  return 3480.0 + 0.49 * w * h + 1.86 * (2.0 * h + 0.5 * w) + 42.0 * straddle + 10.4 * nb;
+}
+
 // Cut of an nx x ny grid into npx x npy pieces for the resident kernel: among
 // the cuts into at most maxb pieces (pieces at least 2 x 2) whose largest piece
 // fits in `cap` bytes of dynamic shared memory and in the worker threads at p
 // points per thread (p = 0: the smallest instance that fits), the one with
-// the smallest estimated iteration time (shared-memory traffic of the largest
-// piece, ~0.27 ns per point, plus ~5 ns of reduction per block), or with
-// fewest_blocks the one with the fewest pieces.  False when none fits.
+// the smallest estimated iteration time (res_iter_ns; FP32: ~0.135 ns per
+// point plus ~5 ns per block), or with least_block_time the smallest
+// iteration time x pieces.  cost: the estimate.  False when none fits.
 struct ResCut {
   int npx = 0, npy = 0, w = 0, h = 0, p = 0;
   size_t smem = 0;
   double cost = 1e300;
 };
-bool res_cut(int nx, int ny, int maxb, size_t cap, int p_fixed, bool fewest_blocks, ResCut& out, bool f32 = false) {
+bool res_cut(int nx, int ny, int maxb, size_t cap, int p_fixed, bool least_block_time, ResCut& out,
+             bool f32 = false) {
   out = ResCut{};
   static constexpr int kP32[] = {16, 32};  // FP32 instances (cg_res32_kernel)
   const int* plist = f32 ? kP32 : kResP;
   const int np = f32 ? 2 : kResNP;
+  double best = 1e300;
   for (int npx = 1; npx <= std::min(nx / 2, maxb); npx++)
     for (int npy = 1; npy <= ny / 2 && npx * npy <= maxb; npy++) {
       const int w = (nx + npx - 1) / npx, h = (ny + npy - 1) / npy;
@@ -156,11 +173,11 @@ bool res_cut(int nx, int ny, int maxb, size_t cap, int p_fixed, bool fewest_bloc
       for (int k = 0; k < np && !pp; k++)
         if ((p_fixed == 0 || plist[k] == p_fixed) && res_threads(w, h, plist[k]) <= kResWorkers) pp = plist[k];
       if (!pp) continue;
-      const double cost = (f32 ? 0.135 : 0.27) * w * h + 5.0 * npx * npy;
-      const bool better = fewest_blocks ? (npx * npy < out.npx * out.npy || out.npx == 0 ||
-                                           (npx * npy == out.npx * out.npy && cost < out.cost))
-                                        : cost < out.cost;
-      if (better) {
+      const int nb = npx * npy;
+      const double cost = f32 ? 0.135 * w * h + 5.0 * nb : res_iter_ns(w, h, pp, nb);
+      const double key = least_block_time ? cost * nb : cost;
+      if (key < best) {
+        best = key;
         out.npx = npx;
         out.npy = npy;
         out.w = w;
@@ -871,14 +888,14 @@ void plan_gangs(int nsm, const std::vector<int>& nb, const std::vector<double>& 
 
 // The solves of `v` on the resident kernel, several at once, in one launch of
 // cg_res_multi_kernel on all SMs.  Every solve takes its densest cut (res_cut
-// with the fewest pieces at 16 points per thread: the least block-time per
-// iteration) and is placed by list scheduling on the host, largest gangs
+// with the least estimated block-time per iteration at 16 points per thread)
+// and is placed by list scheduling on the host, largest gangs
 // first, then longest, improved by a seeded local search over the order: on
 // the pieces' count of blocks that become free earliest under the estimated
 // durations (the grid's device time in the
 // previous resident batch, measured with %globaltimer around its solve; else
 // ~2 x the square root of the point count iterations times the cut's
-// iteration estimate plus ~6 us of reduction latency); each block runs its
+// iteration estimate); each block runs its
 // entries in order of planned start.
 // *used = false (nothing run) when a grid does not fit on chip or the
 // resident kernel is unavailable; the caller then runs the work-queue kernel.
@@ -931,8 +948,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     }
   }
   // estimated duration (ns): this grid's device time in the previous resident batch at the
-  // same occurrence, else ~2 sqrt(points) iterations x (the cut's iteration estimate + ~6 us
-  // of reductions)
+  // same occurrence, else ~2 sqrt(points) iterations x the cut's iteration estimate
   std::vector<int> occ((size_t)count, 0);
   for (int k = 0; k < count; ++k)
     for (int q = 0; q < k; ++q) occ[k] += v[q].c == v[k].c;
@@ -940,7 +956,7 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
     const pyomgpu_ctx* c = v[k].c;
     est[k] = occ[k] < (int)c->batch_ns.size() && c->batch_ns[occ[k]] > 0.0
                  ? c->batch_ns[occ[k]]
-                 : 2.0 * std::sqrt((double)c->nx * c->ny) * (cuts[k].cost + 6000.0);
+                 : 2.0 * std::sqrt((double)c->nx * c->ny) * cuts[k].cost;
   }
   // workspace per solve (batch_job_words): padded sol and res, 4 record words per
   // position, the slots; the caller has reserved it before staging its inputs

@@ -129,14 +129,15 @@ def test_fp32_resident_fits_twice_the_grid():
 
 
 def test_headline_grid_layout_and_kernels_agree():
-    """1440 x 720 (20 islands): 37 x 4 pieces of at most 39 x 180 points, 16
-    points per thread; the resident kernels (two reductions and one per
+    """1440 x 720 (20 islands): 9 x 16 pieces of at most 160 x 45 points, 16
+    points per thread (the cut with the least estimated iteration time); the
+    resident kernels (two reductions and one per
     iteration) and the tiled kernel reach the same solution and the same
     iteration count within one."""
     W = synth.config1()
     E = ExternalMode(W.M)
     E.streamfunction_init(maxipp=10**6, maxq=10**6)
-    assert E.resident_layout() == (37, 4, 16)
+    assert E.resident_layout() == (9, 16, 16)
     out = {}
     for kernel in ("tiled", "resident", "resident1"):
         E.set_cg_kernel(kernel)
