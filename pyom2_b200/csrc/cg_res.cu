@@ -7,8 +7,8 @@
 // block per SM (512 threads, cooperative launch).  For the whole solve a block
 // keeps
 //   shared memory: the search direction with a one-cell halo and the x- and
-//                  y-face couplings FX, FY of its piece (~182 KB for a 39 x 180
-//                  piece, i.e. 1440 x 720 over 148 SMs);
+//                  y-face couplings FX, FY of its piece (~180 KB for a 160 x 45
+//                  piece, i.e. 1440 x 720 over 144 SMs);
 //   TMEM:          the residual, the solution and the preconditioner Z of the
 //                  points a thread owns (tcgen05.ld/st of whole 32-bit columns
 //                  of the thread's lane; no MMA), 96 of the 128 columns each
