@@ -595,8 +595,9 @@ __device__ __forceinline__ void worker_partials(const double (&v)[NV], double (*
 // rmw_read_v4_u64 instead of loads -- in a gang of at most kFreshEagerSlots - 1
 // blocks on every pass after the second, in a larger one on every 8th pass
 // once the poll has lasted kFreshPollNs (there the RMWs of all lanes of ~150
-// blocks on every pass slowed each reduction).  On the 64 basins: 354 ms per
-// batch with the eager reads, 389 ms with the timed ones alone.
+// blocks on every pass slowed each reduction).  On the 64 basins: 362 ms per
+// batch with the eager reads in small gangs, 376-389 ms with the timed ones
+// alone.
 constexpr unsigned long long kFreshPollNs = 1500;
 constexpr int kFreshEagerSlots = 97;
 template <int NV, int kMaxSlot, int kStep, bool TAG = false, bool FRESH = false>
