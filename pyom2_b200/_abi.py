@@ -25,7 +25,7 @@ STATUS_NAMES = {OK: "ok", MAXITER: "max iterations exceeded", DIVERGED: "solver 
 
 # every symbol include/pyomgpu.h declares
 EXPORTS = ("pyomgpu_version", "pyomgpu_last_error", "pyomgpu_ctx_create", "pyomgpu_ctx_destroy",
-           "pyomgpu_set_sync_timeout", "pyomgpu_inject_barrier_stall", "pyomgpu_set_cg_kernel", "pyomgpu_set_batch_kernel", "pyomgpu_batch_schedule", "pyomgpu_plan_batch",
+           "pyomgpu_set_sync_timeout", "pyomgpu_inject_barrier_stall", "pyomgpu_set_cg_kernel", "pyomgpu_set_batch_kernel", "pyomgpu_batch_schedule", "pyomgpu_plan_batch", "pyomgpu_plan_cut",
            "pyomgpu_resident_layout", "pyomgpu_resident_layout32", "pyomgpu_resident_trace", "pyomgpu_set_psin_solve",
            "pyomgpu_momentum_tendencies", "pyomgpu_vertical_velocity", "pyomgpu_autotune", "pyomgpu_isleperim",
            "pyomgpu_island_boundaries", "pyomgpu_island_boundaries_gpu", "pyomgpu_streamfunction_init",
@@ -140,6 +140,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_set_batch_kernel": (i32, [vp, i32]),
         "pyomgpu_batch_schedule": (i32, [vp, i32, vp, vp, vp]),
         "pyomgpu_plan_batch": (i32, [i32, i32, vp, vp, i32, vp, vp, vp, vp]),
+        "pyomgpu_plan_cut": (i32, [i32, i32, i32, C.c_int64, i32, i32, vp, vp]),
         "pyomgpu_resident_layout": (i32, [vp, P(i32), P(i32), P(i32)]),
         "pyomgpu_resident_layout32": (i32, [vp, P(i32), P(i32), P(i32)]),
         "pyomgpu_set_psin_solve": (i32, [vp, C.c_double, i32]),

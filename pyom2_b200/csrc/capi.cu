@@ -1541,6 +1541,22 @@ int32_t pyomgpu_plan_batch(int32_t nsm, int32_t count, const int32_t* blocks, co
   return PYOMGPU_OK;
 }
 
+int32_t pyomgpu_plan_cut(int32_t nx, int32_t ny, int32_t max_blocks, int64_t smem_cap, int32_t points_per_thread,
+                         int32_t least_block_time, int32_t* out, double* est_ns) {
+  if (nx < 2 || ny < 2 || max_blocks < 1 || max_blocks >= kResMaxSlots || smem_cap < 0 || !out ||
+      (points_per_thread != 0 && points_per_thread != 4 && points_per_thread != 8 && points_per_thread != 16))
+    return fail(PYOMGPU_EINVAL, "plan_cut: bad arguments");
+  ResCut cut;
+  const bool ok = res_cut(nx, ny, max_blocks, (size_t)smem_cap, points_per_thread, least_block_time != 0, cut);
+  out[0] = ok ? cut.npx : 0;
+  out[1] = ok ? cut.npy : 0;
+  out[2] = ok ? cut.w : 0;
+  out[3] = ok ? cut.h : 0;
+  out[4] = ok ? cut.p : 0;
+  if (est_ns) *est_ns = ok ? cut.cost : 0.0;
+  return PYOMGPU_OK;
+}
+
 int32_t pyomgpu_batch_schedule(pyomgpu_ctx* c, int32_t count, double* start_ms, double* end_ms, int32_t* blocks) {
   if (!c || count < 0) return fail(PYOMGPU_EINVAL, "batch_schedule: bad arguments");
   if ((int)c->sched_start.size() != count)
