@@ -137,21 +137,28 @@ int finish_cg(pyomgpu_ctx* c, pyomgpu_solve_info* info, cudaStream_t st) {
 // records occupy (a west or east record on a line of its own, south and north
 // ones four to a line), the warps whose threads span two column segments
 // (e.g. 39-wide pieces: 11 of 15; 160-wide: none) and the reduction slots.
-double res_iter_ns(int w, int h, int p, int nb) {
+// f32: the FP32 kernel, whose pieces are counted at their thread capacity
+// (threads x points per thread): at 32 points per thread a thread's rows set
+// the sweep time, and 1440x720 on 8 x 18 pieces of 180 x 40 (360 threads x
+// 32) ran 11.6 us per iteration against 8.5 us on 16-point cuts of the same
+// piece size.  With that the same estimate ranks the FP32 cuts as measured
+// (five cuts each of 1440x720 and 2048x1024, within ~0.5 us).
+double res_iter_ns(int w, int h, int p, int nb, bool f32 = false) {
   const int thr = res_threads(w, h, p);
   int straddle = 0;
   for (int t0 = 0; t0 < thr; t0 += 32)
     if (t0 / w != std::min(t0 + 31, thr - 1) / w) straddle++;
-  return 3480.0 + 0.49 * w * h + 1.86 * (2.0 * h + 0.5 * w) + 42.0 * straddle + 10.4 * nb;
+  const double pts = f32 ? (double)thr * p : (double)w * h;
+  return 3480.0 + 0.49 * pts + 1.86 * (2.0 * h + 0.5 * w) + 42.0 * straddle + 10.4 * nb;
 }
 
 // Cut of an nx x ny grid into npx x npy pieces for the resident kernel: among
 // the cuts into at most maxb pieces (pieces at least 2 x 2) whose largest piece
 // fits in `cap` bytes of dynamic shared memory and in the worker threads at p
 // points per thread (p = 0: the smallest instance that fits), the one with
-// the smallest estimated iteration time (res_iter_ns; FP32: ~0.135 ns per
-// point plus ~5 ns per block), or with least_block_time the smallest
-// iteration time x pieces.  cost: the estimate.  False when none fits.
+// the smallest estimated iteration time (res_iter_ns), or with
+// least_block_time the smallest iteration time x pieces.  cost: the
+// estimate.  False when none fits.
 struct ResCut {
   int npx = 0, npy = 0, w = 0, h = 0, p = 0;
   size_t smem = 0;
@@ -174,7 +181,7 @@ bool res_cut(int nx, int ny, int maxb, size_t cap, int p_fixed, bool least_block
         if ((p_fixed == 0 || plist[k] == p_fixed) && res_threads(w, h, plist[k]) <= kResWorkers) pp = plist[k];
       if (!pp) continue;
       const int nb = npx * npy;
-      const double cost = f32 ? 0.135 * w * h + 5.0 * nb : res_iter_ns(w, h, pp, nb);
+      const double cost = res_iter_ns(w, h, pp, nb, f32);
       const double key = least_block_time ? cost * nb : cost;
       if (key < best) {
         best = key;
