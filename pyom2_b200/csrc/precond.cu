@@ -790,7 +790,7 @@ int32_t pyomgpu_solve_fcg(pyomgpu_ctx* c, pyomgpu_precond* P, const double* forc
   I->iterations = fcg_it;
   I->fcg_iterations = fcg_it;
   I->outer_iterations = 1;
-  // the FP64 true residual judges; Jacobi-PCG takes over on a stall, a breakdown or a miss
+  // the FP64 true residual decides; Jacobi-PCG takes over on a stall, a breakdown or a miss
   launch_fill_cyclic(c->g, c->sol, st);
   launch_residual(c->g, c->sf.dev(), f, c->sol, c->part, 1024, c->scal, st);
   cudaMemcpyAsync(c->h_scal, c->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);

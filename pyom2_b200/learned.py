@@ -3,7 +3,7 @@ flexible CG (``pyomgpu_precond_*`` / ``pyomgpu_solve_fcg`` of the C ABI).
 
 The reference has no learned component; its only preconditioner is Jacobi
 (``make_inv_sfc``, solve_streamfct.f90:381-422), which stays the fallback of
-:func:`solve_fcg` and the judge of every answer through the FP64 true
+:func:`solve_fcg`; every answer is accepted or rejected by its FP64 true
 residual.
 
 Training data are (residual, error) pairs produced by the plain solver
