@@ -1000,7 +1000,11 @@ int run_res_multi(pyomgpu_ctx* o, const std::vector<BatchSpec>& v, double eps, i
   for (int k = 0; again && k < count; ++k) again = o->sched_key[k] == v[k].c;
   if (again) {
     std::vector<char> seen((size_t)count, 0);
-    for (int k : o->sched_order) again = again && k >= 0 && k < count && !seen[k] && (seen[k] = 1);
+    for (int k : o->sched_order) {
+      again = again && k >= 0 && k < count && !seen[k];
+      if (!again) break;
+      seen[k] = 1;
+    }
   }
   GangPlan plan;
   plan_gangs(nsm, nbk, est, again ? &o->sched_order : nullptr,
