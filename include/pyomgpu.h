@@ -380,17 +380,18 @@ int32_t pyomgpu_batch_schedule(pyomgpu_ctx* ctx, int32_t count, double* start_ms
  * count x nsm, ascending, padded with -1) and the planned makespan. */
 int32_t pyomgpu_plan_batch(int32_t nsm, int32_t count, const int32_t* blocks, const double* est, int32_t tries,
                            int32_t* rank, double* start, int32_t* gang, double* makespan);
-/* The piece cut of the FP64 resident kernel on its own (no GPU work): among
- * the cuts of an nx x ny grid into at most max_blocks pieces that fit in
+/* The piece cut of the resident kernel on its own (no GPU work): among the
+ * cuts of an nx x ny grid into at most max_blocks pieces that fit in
  * smem_cap bytes of dynamic shared memory and in the worker threads at
- * points_per_thread (4, 8 or 16; 0: the smallest that fits), the one with
- * the least estimated iteration time, or with least_block_time the least
- * estimate x pieces (the densest cut of a batch gang).  out: npx, npy, the
- * largest piece's w and h, and the points per thread; est_ns: the estimate.
- * PYOMGPU_OK with out[0] = 0 when no cut fits.  No counterpart in the
- * reference. */
+ * points_per_thread (FP64: 4, 8 or 16; fp32: 16 or 32; 0: the smallest that
+ * fits), the one with the least estimated iteration time, or with
+ * least_block_time the least estimate x pieces (the densest cut of a batch
+ * gang).  fp32: the FP32 instance of the mixed-precision correction solves.
+ * out: npx, npy, the largest piece's w and h, and the points per thread;
+ * est_ns: the estimate.  PYOMGPU_OK with out[0] = 0 when no cut fits.  No
+ * counterpart in the reference. */
 int32_t pyomgpu_plan_cut(int32_t nx, int32_t ny, int32_t max_blocks, int64_t smem_cap, int32_t points_per_thread,
-                         int32_t least_block_time, int32_t* out, double* est_ns);
+                         int32_t least_block_time, int32_t fp32, int32_t* out, double* est_ns);
 
 /* congrad_surf_press (solve_pressure.f90:137-249): FP64 CG with maskT-weighted
  * products.  psi is psi(:,:,taup1), in/out, host or device. */

@@ -140,7 +140,7 @@ def load(path: str = LIB_PATH):
         "pyomgpu_set_batch_kernel": (i32, [vp, i32]),
         "pyomgpu_batch_schedule": (i32, [vp, i32, vp, vp, vp]),
         "pyomgpu_plan_batch": (i32, [i32, i32, vp, vp, i32, vp, vp, vp, vp]),
-        "pyomgpu_plan_cut": (i32, [i32, i32, i32, C.c_int64, i32, i32, vp, vp]),
+        "pyomgpu_plan_cut": (i32, [i32, i32, i32, C.c_int64, i32, i32, i32, vp, vp]),
         "pyomgpu_resident_layout": (i32, [vp, P(i32), P(i32), P(i32)]),
         "pyomgpu_resident_layout32": (i32, [vp, P(i32), P(i32), P(i32)]),
         "pyomgpu_set_psin_solve": (i32, [vp, C.c_double, i32]),

@@ -1553,12 +1553,13 @@ int32_t pyomgpu_plan_batch(int32_t nsm, int32_t count, const int32_t* blocks, co
 }
 
 int32_t pyomgpu_plan_cut(int32_t nx, int32_t ny, int32_t max_blocks, int64_t smem_cap, int32_t points_per_thread,
-                         int32_t least_block_time, int32_t* out, double* est_ns) {
-  if (nx < 2 || ny < 2 || max_blocks < 1 || max_blocks >= kResMaxSlots || smem_cap < 0 || !out ||
-      (points_per_thread != 0 && points_per_thread != 4 && points_per_thread != 8 && points_per_thread != 16))
+                         int32_t least_block_time, int32_t fp32, int32_t* out, double* est_ns) {
+  const int p = points_per_thread;
+  const bool p_ok = fp32 ? (p == 0 || p == 16 || p == 32) : (p == 0 || p == 4 || p == 8 || p == 16);
+  if (nx < 2 || ny < 2 || max_blocks < 1 || max_blocks >= kResMaxSlots || smem_cap < 0 || !out || !p_ok)
     return fail(PYOMGPU_EINVAL, "plan_cut: bad arguments");
   ResCut cut;
-  const bool ok = res_cut(nx, ny, max_blocks, (size_t)smem_cap, points_per_thread, least_block_time != 0, cut);
+  const bool ok = res_cut(nx, ny, max_blocks, (size_t)smem_cap, p, least_block_time != 0, cut, fp32 != 0);
   out[0] = ok ? cut.npx : 0;
   out[1] = ok ? cut.npy : 0;
   out[2] = ok ? cut.w : 0;
